@@ -1,0 +1,181 @@
+"""ctypes bindings of the CPU oracle (oracle/liboracle.so) and, when it was
+built here, of the reference's own hot path (oracle/_ref/libmf_ref.so).
+
+Test infrastructure only: the oracle is the checker, never the thing measured.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libmf_ref.so")
+
+P = C.c_void_p
+FP = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+U64P = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+I32P = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+U32P = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+U8P = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+VOXEL_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("r", "<f4"), ("g", "<f4"), ("b", "<f4"),
+                        ("c", "<i4"), ("fg", "<f8"), ("w", "<i4"), ("_pad", "<i4")])
+assert VOXEL_DTYPE.itemsize == 40
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _bind(lib, prefix):
+    def fn(name, res, *args):
+        f = getattr(lib, prefix + name)
+        f.restype = res
+        f.argtypes = list(args)
+        return f
+    b = {}
+    b["vol_create"] = fn("vol_create", P, C.c_int, C.c_float)
+    b["vol_destroy"] = fn("vol_destroy", None, P)
+    b["integrate"] = fn("integrate", C.c_uint, P, FP, FP, FP, C.c_int, C.c_int, FP, FP, FP,
+                        C.c_float)
+    b["alloc_update"] = fn("alloc_update", None, P, U64P, C.c_int)
+    b["block_count"] = fn("block_count", C.c_int, P)
+    b["node_count"] = fn("node_count", C.c_int, P)
+    b["root_children"] = fn("root_children", C.c_ubyte, P)
+    b["export_blocks"] = fn("export_blocks", None, P, U64P, I32P, U8P, C.c_void_p)
+    b["export_nodes"] = fn("export_nodes", None, P, U64P, U32P, U8P, C.c_void_p)
+    b["interp"] = fn("interp", C.c_float, P, FP, C.c_int)
+    b["grad"] = fn("grad", None, P, FP, FP)
+    b["raycast"] = fn("raycast", None, P, FP, FP, C.c_float, C.c_float, C.c_float, C.c_float,
+                      C.c_float, FP)
+    return b
+
+
+class VolumeHandle:
+    """One octree volume held by the oracle or by the compiled reference."""
+
+    def __init__(self, impl, size, dim):
+        self.impl, self.size, self.dim = impl, size, dim
+        self.h = impl.b["vol_create"](size, float(dim))
+
+    def __del__(self):
+        try:
+            self.impl.b["vol_destroy"](self.h)
+        except Exception:
+            pass
+
+    def integrate(self, depth, rgb3, mask, T_w_c, T_w_o, k, mu):
+        H, W = depth.shape
+        return self.impl.b["integrate"](self.h, _f32(depth), _f32(rgb3), _f32(mask), W, H,
+                                        _f32(T_w_c), _f32(T_w_o), _f32(k), float(mu))
+
+    def alloc_update(self, keys):
+        keys = np.ascontiguousarray(keys, np.uint64).copy()
+        if keys.size == 0:
+            keys = np.zeros(1, np.uint64)
+            self.impl.b["alloc_update"](self.h, keys, 0)
+        else:
+            self.impl.b["alloc_update"](self.h, keys, len(keys))
+
+    def blocks(self, with_voxels=True):
+        n = self.impl.b["block_count"](self.h)
+        keys = np.zeros(n, np.uint64)
+        coords = np.zeros((n, 3), np.int32)
+        active = np.zeros(n, np.uint8)
+        vox = np.zeros((n, 512), VOXEL_DTYPE) if with_voxels else None
+        self.impl.b["export_blocks"](self.h, keys, coords, active,
+                                     vox.ctypes.data if with_voxels else None)
+        order = np.argsort(keys, kind="stable")
+        return (keys[order], coords[order], active[order],
+                vox[order] if with_voxels else None)
+
+    def nodes(self, with_values=True):
+        n = self.impl.b["node_count"](self.h)
+        keys = np.zeros(n, np.uint64)
+        side = np.zeros(n, np.uint32)
+        cmask = np.zeros(n, np.uint8)
+        vals = np.zeros((n, 8), VOXEL_DTYPE) if with_values else None
+        self.impl.b["export_nodes"](self.h, keys, side, cmask,
+                                    vals.ctypes.data if with_values else None)
+        order = np.argsort(keys, kind="stable")
+        return (keys[order], side[order], cmask[order],
+                vals[order] if with_values else None)
+
+    def root_children(self):
+        return int(self.impl.b["root_children"](self.h))
+
+    def interp(self, pos, field=0):
+        return self.impl.b["interp"](self.h, _f32(pos), field)
+
+    def grad(self, pos):
+        out = np.zeros(3, np.float32)
+        self.impl.b["grad"](self.h, _f32(pos), out)
+        return out
+
+
+class Impl:
+    def __init__(self, path, prefix):
+        self.lib = C.CDLL(path)
+        self.prefix = prefix
+        self.b = _bind(self.lib, prefix)
+        if prefix == "or_":
+            f = self.lib.or_raycast_objects
+            f.restype = None
+            f.argtypes = [C.POINTER(P), FP, I32P, C.c_int, FP, FP, C.c_int, C.c_int, C.c_float,
+                          C.c_float, C.c_float, C.c_float, FP, FP, I32P]
+            g = self.lib.or_ray_first_block
+            g.restype = C.c_float
+            g.argtypes = [P, FP, FP, C.c_float, C.c_float, C.c_float]
+        else:
+            f = self.lib.ref_raycast_objects
+            f.restype = None
+            f.argtypes = [C.POINTER(P), FP, I32P, C.c_int, FP, FP, C.c_int, C.c_int, C.c_float,
+                          C.c_float, C.c_float, FP, FP, I32P]
+            g = self.lib.ref_ray_first_block
+            g.restype = C.c_float
+            g.argtypes = [P, FP, FP, C.c_float, C.c_float]
+            e = self.lib.ref_pin_epsilon
+            e.restype = None
+            e.argtypes = [C.c_int]
+
+    def volume(self, size, dim):
+        return VolumeHandle(self, size, dim)
+
+    def raycast_objects(self, vols, poses, labels, T_w_c, k, W, H, near=0.1, far=4.0, mu=0.1,
+                        eps_size=None, vertex=None, normal=None, label_img=None):
+        n = len(vols)
+        arr = (P * n)(*[v.h for v in vols])
+        vertex = np.zeros((H, W, 3), np.float32) if vertex is None else vertex
+        normal = np.zeros((H, W, 3), np.float32) if normal is None else normal
+        label_img = np.zeros((H, W), np.int32) if label_img is None else label_img
+        Two = _f32(np.stack(poses).reshape(n, 16))
+        labels = np.ascontiguousarray(labels, np.int32)
+        if self.prefix == "or_":
+            eps = float(np.float32(2.0 ** -np.log2(eps_size or vols[0].size)))
+            self.lib.or_raycast_objects(arr, Two, labels, n, _f32(T_w_c), _f32(k), W, H, near,
+                                        far, mu, eps, vertex, normal, label_img)
+        else:
+            self.lib.ref_raycast_objects(arr, Two, labels, n, _f32(T_w_c), _f32(k), W, H, near,
+                                         far, mu, vertex, normal, label_img)
+        return vertex, normal, label_img
+
+
+_cache = {}
+
+
+def oracle():
+    if "or" not in _cache:
+        _cache["or"] = Impl(ORACLE_SO, "or_")
+    return _cache["or"]
+
+
+def reference():
+    """The reference's own hot path, or None when oracle/_ref was not built."""
+    if not os.path.exists(REF_SO):
+        return None
+    if "ref" not in _cache:
+        _cache["ref"] = Impl(REF_SO, "ref_")
+    return _cache["ref"]
