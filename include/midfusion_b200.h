@@ -1,0 +1,143 @@
+/* MID-Fusion per-frame dense hot path on NVIDIA B200 (sm_100a): C ABI.
+ *
+ * Plain C types only: a caller written in C, C++ (the reference's Kfusion
+ * pipeline), Python (ctypes) or any FFI binds these directly.  Each entry point
+ * names the reference interface it replaces (paths relative to the reference
+ * project root).
+ *
+ * Conventions
+ *  - Every function returns MF_OK (0) or a negative MF_E_* code;
+ *    mf_last_error() gives a one-line description of the last failure.
+ *  - Matrices are 4x4 float, row-major (the reference's Matrix4:
+ *    utils/math_utils.h:47-49).  Intrinsics k = {fx, fy, cx, cy}.
+ *  - Host pointers are borrowed for the duration of the call; device state is
+ *    owned by the context.  All work is queued on the context's stream; calls
+ *    that return host data synchronise that stream.
+ *  - One context per host thread (the reference is not re-entrant either).
+ */
+#ifndef MIDFUSION_B200_H
+#define MIDFUSION_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MF_OK 0
+#define MF_E_ARG (-1)          /* invalid argument or size */
+#define MF_E_CUDA (-2)         /* CUDA runtime error (see mf_last_error) */
+#define MF_E_POOL_FULL (-3)    /* voxel-block pool exhausted */
+#define MF_E_NOT_FOUND (-4)    /* unknown instance id */
+#define MF_E_STATE (-5)        /* call made in the wrong order */
+#define MF_E_TIMEOUT (-6)      /* a bounded device wait gave up */
+
+/* Device status flags accumulated since the last mf_status() call. */
+#define MF_STATUS_POOL_FULL 1
+#define MF_STATUS_ALLOC_OVERFLOW 2  /* more keys than the reference's list holds */
+#define MF_STATUS_RAY_GUARD 4
+#define MF_STATUS_GN_FALLBACK 8     /* a 6x6 system used the truncated eigen solve */
+
+/* Robust kernels of Tracking::calc_robust_weight,
+ * apps/kfusion/src/cpp/tracking/tracking.cpp:1504-1532 (enum RobustW,
+ * tracking/tracking.h:19-24). */
+#define MF_ROBUST_NONE 0
+#define MF_ROBUST_HUBER 1
+#define MF_ROBUST_TUKEY 2
+#define MF_ROBUST_CAUCHY 3
+
+typedef struct mf_config {
+  int width, height;          /* computationSize */
+  float k[4];                 /* fx, fy, cx, cy */
+  float mu;                   /* TSDF truncation, default_parameters.h:26 (0.1) */
+  float near_plane, far_plane;/* constant_parameters.h:20-21 (0.1, 4.0) */
+  int max_weight;             /* sdf_update maxweight, object.cpp:165 (100) */
+  int pyramid_levels;         /* default_parameters.h:22-23 (3) */
+  int gn_iterations[4];       /* {10, 5, 4} */
+  int robust_kernel;          /* MF_ROBUST_* (reference default Cauchy) */
+  int use_icp, use_rgb;       /* Tracking(using_ICP, using_RGB) */
+  long long pool_blocks;      /* capacity of the shared voxel-block pool */
+  int max_instances;          /* <= 32 */
+  int batched;                /* 1: one launch per stage for all instances */
+} mf_config;
+
+typedef struct mf_context mf_context;
+
+/* Fill `cfg` with the reference defaults for a width x height frame. */
+int mf_config_default(mf_config* cfg, int width, int height);
+int mf_create(const mf_config* cfg, mf_context** out);
+int mf_destroy(mf_context* ctx);
+const char* mf_last_error(const mf_context* ctx);
+/* Pending device status flags (MF_STATUS_*), cleared by the call. */
+int mf_status(mf_context* ctx, int* flags);
+/* The cudaStream_t all work is queued on. */
+int mf_get_stream(mf_context* ctx, void** stream);
+int mf_synchronize(mf_context* ctx);
+
+/* --- instances ---------------------------------------------------------
+ * One octree volume per instance: the background (label 0) and every object.
+ * Replaces Object::Object + Volume::init (object/object.cpp:13-40,
+ * continuous/volume_template.hpp:63-67).  size: voxels per side (power of
+ * two, 32..4096); dim: metres per side; T_w_o: volume corner pose. */
+int mf_instance_add(mf_context* ctx, int size, float dim, const float T_w_o[16],
+                    int label, int* id);
+int mf_instance_count(mf_context* ctx, int* n);
+int mf_instance_set_pose(mf_context* ctx, int id, const float T_w_o[16]);
+int mf_instance_get_pose(mf_context* ctx, int id, float T_w_o[16]);
+int mf_set_camera_pose(mf_context* ctx, const float T_w_c[16]);
+int mf_get_camera_pose(mf_context* ctx, float T_w_c[16]);
+
+/* --- frame input ------------------------------------------------------
+ * depth: metres (floatDepth after mm2metersKernel, preprocessing.cpp:132-159);
+ * rgb: uint8 x 3 per pixel; masks: one generalized float mask per instance in
+ * instance order (instance_seg::generalize_label, segmentation.cpp:10-48), or
+ * NULL to keep the previous masks.  Host pointers (copied to the device). */
+int mf_frame_upload(mf_context* ctx, const float* depth, const uint8_t* rgb,
+                    const float* masks, int n_masks);
+/* Same with device pointers (no host copy). */
+int mf_frame_set_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
+                        const float* d_masks, int n_masks);
+/* Ground-truth uint16 instance labels (host) -> generalized masks on the
+ * device for every instance (fg 1, 5x5-ellipse ring 0, elsewhere -1). */
+int mf_frame_labels(mf_context* ctx, const uint16_t* labels);
+
+/* --- allocation + integration -----------------------------------------
+ * Object::integrate_volume_kernel (object/object.cpp:128-195) for each id:
+ * buildVolumeAllocationList (kfusion/alloc_impl.hpp:121-191) +
+ * Octree::alloc_update (lib/octree.hpp:761-786) + projective_functor with
+ * sdf_update (lib/functors/projective_functor.hpp:139-156,
+ * kfusion/mapping_impl.hpp:15-72), at the current camera pose. */
+int mf_integrate(mf_context* ctx, const int* ids, int n);
+/* Octree::alloc_update (lib/octree.hpp:761-786) on explicit keys. */
+int mf_alloc_update(mf_context* ctx, int id, const uint64_t* keys, int n);
+
+/* --- raycast ----------------------------------------------------------
+ * raycastObjectList (rendering/rendering.cpp:9-181) over every instance at
+ * the current camera pose: composite vertex/normal/label maps stay on the
+ * device as the tracking model. */
+int mf_raycast(mf_context* ctx);
+/* Copy the composite maps to the host (any pointer may be NULL). */
+int mf_download_raycast(mf_context* ctx, float* vertex, float* normal, int32_t* label);
+
+/* --- inspection (parity checks, debugging) -----------------------------
+ * Blocks: key (code | level), corner voxel, VoxelBlock::active_, and when
+ * `voxels` is not NULL the 512 voxels in the reference's 40-byte AoS layout
+ * (voxel_traits<SDF>::ComputeType).  Order is unspecified. */
+int mf_block_count(mf_context* ctx, int id, int* n);
+int mf_export_blocks(mf_context* ctx, int id, uint64_t* keys, int32_t* coords,
+                     uint8_t* active, void* voxels, int cap, int* n);
+/* Internal nodes (levels 1..block level - 1): key, side, children mask,
+ * and Node::value_[8] (40-byte AoS) when `values` is not NULL. */
+int mf_node_count(mf_context* ctx, int id, int* n);
+int mf_export_nodes(mf_context* ctx, int id, uint64_t* keys, uint32_t* side,
+                    uint8_t* children_mask, void* values, int cap, int* n);
+int mf_root_children(mf_context* ctx, int id, uint8_t* mask);
+/* Volume::interp (continuous/volume_template.hpp:97-104) at n points
+ * (metres, volume frame); field 0 = tsdf, 1 = foreground probability. */
+int mf_interp(mf_context* ctx, int id, const float* pos, int n, int field, float* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MIDFUSION_B200_H */

@@ -1,0 +1,69 @@
+"""Build the MID-Fusion B200 CUDA library in-tree (sm_100a).
+
+``python -m mid_fusion_b200.build`` compiles every ``csrc/*.cu`` file with nvcc
+into ``mid_fusion_b200/_lib/libmidfusion_b200.so``.  -fmad=false keeps the
+reference's IEEE single-precision evaluation order (no fused multiply-add), on
+which the bit-exact allocation parity rests.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB_DIR = os.path.join(HERE, "_lib")
+LIB = os.path.join(LIB_DIR, "libmidfusion_b200.so")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
+    "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+    "-Xptxas", "-O3",
+    "--shared",
+]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+
+
+def headers():
+    return (glob.glob(os.path.join(HERE, "csrc", "*.cuh")) +
+            glob.glob(os.path.join(HERE, "csrc", "*.h")) +
+            glob.glob(os.path.join(ROOT, "include", "*.h")))
+
+
+def up_to_date():
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(f) <= t for f in sources() + headers())
+
+
+def build(force=False, verbose=False, extra=()):
+    if not force and up_to_date():
+        return LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    nvcc = os.environ.get("NVCC", "nvcc")
+    objs = []
+    for src in sources():
+        obj = os.path.join(LIB_DIR, os.path.basename(src)[:-3] + ".o")
+        cmd = [nvcc, *NVCC_FLAGS[:-1], "-c", "-I", os.path.join(ROOT, "include"), *extra,
+               src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", *objs, "-o", LIB,
+           "-lcudart"]
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True,
+          extra=["-Xptxas", "-v"] if "--ptxas-v" in sys.argv else [])
+    print(LIB)

@@ -1,0 +1,235 @@
+"""ctypes binding of the C ABI in include/midfusion_b200.h.
+
+The CUDA library is the product; this module only loads it and converts
+numpy arrays to pointers.  Loading fails loudly when the library is missing:
+there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libmidfusion_b200.so")
+
+MF_OK = 0
+ERRORS = {-1: "MF_E_ARG", -2: "MF_E_CUDA", -3: "MF_E_POOL_FULL", -4: "MF_E_NOT_FOUND",
+          -5: "MF_E_STATE", -6: "MF_E_TIMEOUT"}
+STATUS_POOL_FULL, STATUS_ALLOC_OVERFLOW, STATUS_RAY_GUARD, STATUS_GN_FALLBACK = 1, 2, 4, 8
+ROBUST = {"none": 0, "huber": 1, "tukey": 2, "cauchy": 3}
+
+VOXEL_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("r", "<f4"), ("g", "<f4"), ("b", "<f4"),
+                        ("c", "<i4"), ("fg", "<f8"), ("w", "<i4"), ("_pad", "<i4")])
+
+# Every symbol include/midfusion_b200.h declares (checked by the CPU tests).
+EXPORTS = [
+    "mf_config_default", "mf_create", "mf_destroy", "mf_last_error", "mf_status",
+    "mf_get_stream", "mf_synchronize", "mf_instance_add", "mf_instance_count",
+    "mf_instance_set_pose", "mf_instance_get_pose", "mf_set_camera_pose", "mf_get_camera_pose",
+    "mf_frame_upload", "mf_frame_set_device", "mf_frame_labels", "mf_integrate",
+    "mf_alloc_update", "mf_raycast", "mf_download_raycast", "mf_block_count",
+    "mf_export_blocks", "mf_node_count", "mf_export_nodes", "mf_root_children", "mf_interp",
+]
+
+
+class MfConfig(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("k", C.c_float * 4),
+                ("mu", C.c_float), ("near_plane", C.c_float), ("far_plane", C.c_float),
+                ("max_weight", C.c_int), ("pyramid_levels", C.c_int),
+                ("gn_iterations", C.c_int * 4), ("robust_kernel", C.c_int),
+                ("use_icp", C.c_int), ("use_rgb", C.c_int), ("pool_blocks", C.c_longlong),
+                ("max_instances", C.c_int), ("batched", C.c_int)]
+
+
+class MfError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MfError(f"CUDA library not built: {LIB_PATH} (run python -m mid_fusion_b200.build)")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.mf_last_error.restype = C.c_char_p
+        _lib.mf_last_error.argtypes = [C.c_void_p]
+    return _lib
+
+
+def _ptr(a, dtype):
+    if a is None:
+        return None
+    assert a.dtype == dtype and a.flags.c_contiguous, (a.dtype, dtype)
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _m4(T):
+    return np.ascontiguousarray(np.asarray(T, np.float32).reshape(16))
+
+
+class Context:
+    """One mf_context: the device-side state of the whole per-frame hot path."""
+
+    def __init__(self, width, height, k=None, mu=0.1, pool_blocks=1 << 17, max_instances=16,
+                 batched=True, robust="cauchy", use_icp=True, use_rgb=True,
+                 gn_iterations=(10, 5, 4), near=0.1, far=4.0):
+        self.lib = load()
+        cfg = MfConfig()
+        self._check(self.lib.mf_config_default(C.byref(cfg), width, height))
+        if k is not None:
+            for i in range(4):
+                cfg.k[i] = float(k[i])
+        cfg.mu = mu
+        cfg.pool_blocks = int(pool_blocks)
+        cfg.max_instances = max_instances
+        cfg.batched = 1 if batched else 0
+        cfg.robust_kernel = ROBUST[robust]
+        cfg.use_icp, cfg.use_rgb = int(use_icp), int(use_rgb)
+        cfg.pyramid_levels = len(gn_iterations)
+        for i, it in enumerate(gn_iterations):
+            cfg.gn_iterations[i] = it
+        cfg.near_plane, cfg.far_plane = near, far
+        self.cfg = cfg
+        self.W, self.H = width, height
+        h = C.c_void_p()
+        self._check(self.lib.mf_create(C.byref(cfg), C.byref(h)), ctx=False)
+        self.h = h
+        self.n_instances = 0
+
+    def _check(self, rc, ctx=True):
+        if rc != MF_OK:
+            msg = ""
+            if ctx and getattr(self, "h", None):
+                msg = self.lib.mf_last_error(self.h).decode()
+            raise MfError(f"{ERRORS.get(rc, rc)} {msg}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---------------------------------------------------------------- setup
+    def add_instance(self, size, dim, T_w_o, label):
+        i = C.c_int()
+        self._check(self.lib.mf_instance_add(self.h, int(size), C.c_float(dim),
+                                             _ptr(_m4(T_w_o), np.float32), int(label),
+                                             C.byref(i)))
+        self.n_instances += 1
+        return i.value
+
+    def set_instance_pose(self, i, T):
+        self._check(self.lib.mf_instance_set_pose(self.h, i, _ptr(_m4(T), np.float32)))
+
+    def instance_pose(self, i):
+        T = np.zeros(16, np.float32)
+        self._check(self.lib.mf_instance_get_pose(self.h, i, _ptr(T, np.float32)))
+        return T.reshape(4, 4)
+
+    def set_camera_pose(self, T):
+        self._check(self.lib.mf_set_camera_pose(self.h, _ptr(_m4(T), np.float32)))
+
+    def camera_pose(self):
+        T = np.zeros(16, np.float32)
+        self._check(self.lib.mf_get_camera_pose(self.h, _ptr(T, np.float32)))
+        return T.reshape(4, 4)
+
+    # ---------------------------------------------------------------- frames
+    def upload(self, depth=None, rgb=None, masks=None):
+        d = None if depth is None else np.ascontiguousarray(depth, np.float32)
+        r = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
+        m = None if masks is None else np.ascontiguousarray(masks, np.float32)
+        n = 0 if m is None else m.shape[0]
+        self._check(self.lib.mf_frame_upload(self.h, _ptr(d, np.float32), _ptr(r, np.uint8),
+                                             _ptr(m, np.float32), n))
+
+    def upload_labels(self, labels):
+        lab = np.ascontiguousarray(labels, np.uint16)
+        self._check(self.lib.mf_frame_labels(self.h, _ptr(lab, np.uint16)))
+
+    # ---------------------------------------------------------------- stages
+    def integrate(self, ids):
+        ids = np.ascontiguousarray(ids, np.int32)
+        self._check(self.lib.mf_integrate(self.h, _ptr(ids, np.int32), len(ids)))
+
+    def alloc_update(self, i, keys):
+        keys = np.ascontiguousarray(keys, np.uint64)
+        self._check(self.lib.mf_alloc_update(self.h, i, _ptr(keys, np.uint64), len(keys)))
+
+    def raycast(self):
+        self._check(self.lib.mf_raycast(self.h))
+
+    def download_raycast(self):
+        v = np.zeros((self.H, self.W, 3), np.float32)
+        n = np.zeros((self.H, self.W, 3), np.float32)
+        lab = np.zeros((self.H, self.W), np.int32)
+        self._check(self.lib.mf_download_raycast(self.h, _ptr(v, np.float32),
+                                                 _ptr(n, np.float32), _ptr(lab, np.int32)))
+        return v, n, lab
+
+    def status(self):
+        f = C.c_int()
+        self._check(self.lib.mf_status(self.h, C.byref(f)))
+        return f.value
+
+    def synchronize(self):
+        self._check(self.lib.mf_synchronize(self.h))
+
+    def stream(self):
+        s = C.c_void_p()
+        self._check(self.lib.mf_get_stream(self.h, C.byref(s)))
+        return s.value
+
+    # ---------------------------------------------------------------- inspection
+    def blocks(self, i, with_voxels=True):
+        n = C.c_int()
+        self._check(self.lib.mf_block_count(self.h, i, C.byref(n)))
+        n = n.value
+        keys = np.zeros(n, np.uint64)
+        coords = np.zeros((n, 3), np.int32)
+        active = np.zeros(n, np.uint8)
+        vox = np.zeros((n, 512), VOXEL_DTYPE) if with_voxels else None
+        m = C.c_int()
+        self._check(self.lib.mf_export_blocks(
+            self.h, i, _ptr(keys, np.uint64), _ptr(coords, np.int32), _ptr(active, np.uint8),
+            None if vox is None else vox.ctypes.data_as(C.c_void_p), n, C.byref(m)))
+        order = np.argsort(keys, kind="stable")
+        return keys[order], coords[order], active[order], (None if vox is None else vox[order])
+
+    def nodes(self, i, with_values=True):
+        n = C.c_int()
+        self._check(self.lib.mf_node_count(self.h, i, C.byref(n)))
+        n = n.value
+        keys = np.zeros(n, np.uint64)
+        side = np.zeros(n, np.uint32)
+        cm = np.zeros(n, np.uint8)
+        vals = np.zeros((n, 8), VOXEL_DTYPE) if with_values else None
+        m = C.c_int()
+        self._check(self.lib.mf_export_nodes(
+            self.h, i, _ptr(keys, np.uint64), _ptr(side, np.uint32), _ptr(cm, np.uint8),
+            None if vals is None else vals.ctypes.data_as(C.c_void_p), n, C.byref(m)))
+        order = np.argsort(keys, kind="stable")
+        return keys[order], side[order], cm[order], (None if vals is None else vals[order])
+
+    def root_children(self, i):
+        m = C.c_uint8()
+        self._check(self.lib.mf_root_children(self.h, i, C.byref(m)))
+        return m.value
+
+    def interp(self, i, pos, field=0):
+        pos = np.ascontiguousarray(np.asarray(pos, np.float32).reshape(-1, 3))
+        out = np.zeros(len(pos), np.float32)
+        self._check(self.lib.mf_interp(self.h, i, _ptr(pos, np.float32), len(pos), field,
+                                       _ptr(out, np.float32)))
+        return out

@@ -1,0 +1,431 @@
+// C ABI of the MID-Fusion B200 library (declared in include/midfusion_b200.h).
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "mf_internal.h"
+
+using namespace mf;
+
+struct mf_context : public mf::Context {};
+
+namespace mf {
+
+// rgb2intensity, apps/kfusion/src/cpp/preprocessing/preprocessing.cpp:73-102
+// (ratio 1): float RGB in [0, 1] and grey = rgb2gs (commons.h:150-154).
+__global__ void rgb_convert_kernel(const uint8_t* __restrict__ rgb8, F3* __restrict__ rgb,
+                                   float* __restrict__ grey, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const float r = rgb8[3 * p], g = rgb8[3 * p + 1], b = rgb8[3 * p + 2];
+  rgb[p] = mk3(r / 255.0f, g / 255.0f, b / 255.0f);
+  grey[p] = (0.299f * r + 0.587f * g + 0.114f * b) / 255.f;
+}
+
+// instance_seg::generalize_label for ground-truth masks,
+// apps/kfusion/src/cpp/segmentation/segmentation.cpp:10-48: 1 on the instance,
+// 0 on the ring added by a 5x5 elliptic dilation, -1 elsewhere.
+__global__ void generalize_kernel(const uint16_t* __restrict__ labels, int W, int H,
+                                  const int* __restrict__ inst_labels, int n_inst,
+                                  float* __restrict__ masks) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y;
+  const int i = blockIdx.z;
+  if (x >= W || i >= n_inst) return;
+  const int L = inst_labels[i];
+  float v;
+  if (labels[x + y * W] == L) {
+    v = 1.f;
+  } else {
+    bool ring = false;
+    for (int dy = -2; dy <= 2 && !ring; ++dy)
+      for (int dx = -2; dx <= 2; ++dx) {
+        if ((dy == -2 || dy == 2) && dx != 0) continue;  // cv::MORPH_ELLIPSE 5x5
+        const int xx = x + dx, yy = y + dy;
+        if (xx < 0 || yy < 0 || xx >= W || yy >= H) continue;
+        if (labels[xx + yy * W] == L) { ring = true; break; }
+      }
+    v = ring ? 0.f : -1.f;
+  }
+  masks[(size_t)i * W * H + x + y * W] = v;
+}
+
+__global__ void fill_kernel(float* __restrict__ p, float v, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+}  // namespace mf
+
+static int check(mf_context* ctx) { return ctx ? MF_OK : MF_E_ARG; }
+
+static IdList all_ids(mf_context* ctx) {
+  IdList l;
+  l.n = (int)ctx->inst.size();
+  for (int i = 0; i < l.n; ++i) l.v[i] = i;
+  return l;
+}
+
+extern "C" {
+
+int mf_config_default(mf_config* c, int width, int height) {
+  if (!c || width <= 0 || height <= 0) return MF_E_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->width = width;
+  c->height = height;
+  c->k[0] = 525.f * width / 640.f;
+  c->k[1] = 525.f * width / 640.f;
+  c->k[2] = (width - 1) * 0.5f;
+  c->k[3] = (height - 1) * 0.5f;
+  c->mu = 0.1f;
+  c->near_plane = 0.1f;
+  c->far_plane = 4.0f;
+  c->max_weight = 100;
+  c->pyramid_levels = 3;
+  c->gn_iterations[0] = 10; c->gn_iterations[1] = 5; c->gn_iterations[2] = 4;
+  c->robust_kernel = MF_ROBUST_CAUCHY;
+  c->use_icp = 1;
+  c->use_rgb = 1;
+  c->pool_blocks = 1 << 17;
+  c->max_instances = 16;
+  c->batched = 1;
+  return MF_OK;
+}
+
+const char* mf_last_error(const mf_context* ctx) {
+  return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+int mf_create(const mf_config* cfg, mf_context** out) {
+  if (!cfg || !out || cfg->width <= 0 || cfg->height <= 0 || cfg->pool_blocks <= 0 ||
+      cfg->max_instances <= 0 || cfg->max_instances > MAX_INSTANCES ||
+      cfg->pool_blocks > (1LL << 30))
+    return MF_E_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MF_E_CUDA;
+  mf_context* ctx = new mf_context;
+  ctx->cfg = *cfg;
+  ctx->W = cfg->width;
+  ctx->H = cfg->height;
+  cudaGetDevice(&ctx->device);
+  auto fail = [&](int rc) { mf_destroy(ctx); return rc; };
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(MF_E_CUDA);
+  ctx->own_stream = true;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  const size_t cap = (size_t)cfg->pool_blocks;
+  Pool& P = ctx->pool;
+  P.cap = (int)cap;
+  const size_t nv = cap * 512;
+  bool ok = cudaMalloc(&P.tsdf, nv * 4) == cudaSuccess && cudaMalloc(&P.wt, nv * 4) == cudaSuccess &&
+            cudaMalloc(&P.r, nv * 4) == cudaSuccess && cudaMalloc(&P.g, nv * 4) == cudaSuccess &&
+            cudaMalloc(&P.b, nv * 4) == cudaSuccess && cudaMalloc(&P.c, nv * 4) == cudaSuccess &&
+            cudaMalloc(&P.fg, nv * 8) == cudaSuccess && cudaMalloc(&P.w, nv * 4) == cudaSuccess &&
+            cudaMalloc(&P.meta, cap * sizeof(int4)) == cudaSuccess &&
+            cudaMalloc(&P.active, cap) == cudaSuccess && cudaMalloc(&P.count, sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc(&ctx->d_vols, sizeof(Volume) * MAX_INSTANCES) == cudaSuccess &&
+       cudaMalloc(&ctx->d_Two, sizeof(float) * 16 * MAX_INSTANCES) == cudaSuccess &&
+       cudaMalloc(&ctx->d_Twc, sizeof(float) * 16) == cudaSuccess &&
+       cudaMalloc(&ctx->d_frames, sizeof(InstFrame) * MAX_INSTANCES) == cudaSuccess &&
+       cudaMalloc(&ctx->d_status, sizeof(int)) == cudaSuccess &&
+       cudaMalloc(&ctx->d_reserved, sizeof(unsigned long long) * MAX_INSTANCES) == cudaSuccess &&
+       cudaMalloc(&ctx->d_inst_label, sizeof(int) * MAX_INSTANCES) == cudaSuccess &&
+       cudaMalloc(&ctx->d_visit, sizeof(int) * cap) == cudaSuccess &&
+       cudaMalloc(&ctx->d_visit_count, sizeof(int)) == cudaSuccess &&
+       cudaMalloc(&ctx->d_depth, 4 * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_rgb8, 3 * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_rgb, sizeof(F3) * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_grey, 4 * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_masks, 4 * WH * cfg->max_instances) == cudaSuccess &&
+       cudaMalloc(&ctx->d_labels, 2 * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_vertex, sizeof(F3) * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_normal, sizeof(F3) * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_label, sizeof(int) * WH) == cudaSuccess;
+  if (!ok) {
+    ctx->last_error = "device allocation failed";
+    return fail(MF_E_CUDA);
+  }
+  // Fresh pool slots hold the reference's initial voxel {1, 0, 0, 0, 0, 0, 0, 0}
+  // (voxel_traits<SDF>::initValue, continuous/volume_traits.hpp:40); blocks are
+  // never released, so a newly acquired slot needs no further initialisation.
+  fill_kernel<<<1184, 256, 0, ctx->stream>>>(P.tsdf, 1.f, nv);
+  cudaMemsetAsync(P.wt, 0, nv * 4, ctx->stream);
+  cudaMemsetAsync(P.r, 0, nv * 4, ctx->stream);
+  cudaMemsetAsync(P.g, 0, nv * 4, ctx->stream);
+  cudaMemsetAsync(P.b, 0, nv * 4, ctx->stream);
+  cudaMemsetAsync(P.c, 0, nv * 4, ctx->stream);
+  cudaMemsetAsync(P.fg, 0, nv * 8, ctx->stream);
+  cudaMemsetAsync(P.w, 0, nv * 4, ctx->stream);
+  cudaMemsetAsync(P.active, 0, cap, ctx->stream);
+  cudaMemsetAsync(P.count, 0, sizeof(int), ctx->stream);
+  cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream);
+  cudaMemsetAsync(ctx->d_vertex, 0, sizeof(F3) * WH, ctx->stream);
+  cudaMemsetAsync(ctx->d_normal, 0, sizeof(F3) * WH, ctx->stream);
+  cudaMemsetAsync(ctx->d_label, 0, sizeof(int) * WH, ctx->stream);
+  cudaMemsetAsync(ctx->d_depth, 0, 4 * WH, ctx->stream);
+  cudaMemsetAsync(ctx->d_masks, 0, 4 * WH * cfg->max_instances, ctx->stream);
+  float I[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+  cudaMemcpyAsync(ctx->d_Twc, I, sizeof(I), cudaMemcpyHostToDevice, ctx->stream);
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    ctx->last_error = "device initialisation failed";
+    return fail(MF_E_CUDA);
+  }
+  *out = ctx;
+  return MF_OK;
+}
+
+int mf_destroy(mf_context* ctx) {
+  if (!ctx) return MF_E_ARG;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& in : ctx->inst) volume_free(in);
+  Pool& P = ctx->pool;
+  void* ps[] = {P.tsdf, P.wt, P.r, P.g, P.b, P.c, P.fg, P.w, P.meta, P.active, P.count,
+                ctx->d_vols, ctx->d_Two, ctx->d_Twc, ctx->d_frames, ctx->d_status,
+                ctx->d_reserved, ctx->d_inst_label, ctx->d_visit, ctx->d_visit_count,
+                ctx->d_depth, ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, ctx->d_masks,
+                ctx->d_labels, ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->d_export};
+  for (void* p : ps) if (p) cudaFree(p);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return MF_OK;
+}
+
+int mf_status(mf_context* ctx, int* flags) {
+  if (check(ctx) || !flags) return MF_E_ARG;
+  int v = 0;
+  MF_CUDA(cudaMemcpyAsync(&v, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  *flags = v;
+  return MF_OK;
+}
+
+int mf_get_stream(mf_context* ctx, void** stream) {
+  if (check(ctx) || !stream) return MF_E_ARG;
+  *stream = (void*)ctx->stream;
+  return MF_OK;
+}
+
+int mf_synchronize(mf_context* ctx) {
+  if (check(ctx)) return MF_E_ARG;
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_instance_add(mf_context* ctx, int size, float dim, const float T_w_o[16], int label,
+                    int* id) {
+  if (check(ctx) || !T_w_o || !(dim > 0)) return MF_E_ARG;
+  if ((int)ctx->inst.size() >= ctx->cfg.max_instances) return MF_E_ARG;
+  if (size < 16 || size > 4096 || (size & (size - 1))) return MF_E_ARG;
+  Instance in;
+  in.size = size;
+  in.dim = dim;
+  in.label = label;
+  // Object::integrate_volume_kernel, object.cpp:132-140: the allocation list holds
+  // (dim / (8 * voxelsize)) * W * H keys.
+  const float voxelsize = dim / (unsigned)size;
+  const int num_vox_per_pix = (int)(dim / (8u * voxelsize));
+  in.reserved = (size_t)num_vox_per_pix * ctx->W * ctx->H;
+  if (int rc = volume_create(ctx, in)) return rc;
+  const int i = (int)ctx->inst.size();
+  ctx->inst.push_back(in);
+  const unsigned long long res = in.reserved;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_vols + i, &ctx->inst[i].vol, sizeof(Volume),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_Two + 16 * i, T_w_o, 64, cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_reserved + i, &res, sizeof(res), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_inst_label + i, &label, sizeof(int), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (ctx->inst.size() == 1) {
+    // lib/octree.hpp:934 keeps the ray direction epsilon in a function-local
+    // static, initialised by the first ray iterator: the first volume's size.
+    ctx->ray_epsilon = exp2f((float)(-std::log2((double)size)));
+  }
+  if (id) *id = i;
+  return MF_OK;
+}
+
+int mf_instance_count(mf_context* ctx, int* n) {
+  if (check(ctx) || !n) return MF_E_ARG;
+  *n = (int)ctx->inst.size();
+  return MF_OK;
+}
+
+int mf_instance_set_pose(mf_context* ctx, int id, const float T[16]) {
+  if (check(ctx) || !T) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_Two + 16 * id, T, 64, cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_instance_get_pose(mf_context* ctx, int id, float T[16]) {
+  if (check(ctx) || !T) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  MF_CUDA(cudaMemcpyAsync(T, ctx->d_Two + 16 * id, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_set_camera_pose(mf_context* ctx, const float T[16]) {
+  if (check(ctx) || !T) return MF_E_ARG;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_Twc, T, 64, cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_get_camera_pose(mf_context* ctx, float T[16]) {
+  if (check(ctx) || !T) return MF_E_ARG;
+  MF_CUDA(cudaMemcpyAsync(T, ctx->d_Twc, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_frame_upload(mf_context* ctx, const float* depth, const uint8_t* rgb,
+                    const float* masks, int n_masks) {
+  if (check(ctx)) return MF_E_ARG;
+  if (n_masks < 0 || n_masks > ctx->cfg.max_instances || (masks && n_masks == 0)) return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  if (depth)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_depth, depth, 4 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  if (rgb) {
+    MF_CUDA(cudaMemcpyAsync(ctx->d_rgb8, rgb, 3 * WH, cudaMemcpyHostToDevice, ctx->stream));
+    rgb_convert_kernel<<<(unsigned)((WH + 255) / 256), 256, 0, ctx->stream>>>(
+        ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, (int)WH);
+    MF_CUDA(cudaGetLastError());
+  }
+  if (masks)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_masks, masks, 4 * WH * n_masks, cudaMemcpyHostToDevice,
+                            ctx->stream));
+  // the host buffers are borrowed only for the call
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_frame_set_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
+                        const float* d_masks, int n_masks) {
+  if (check(ctx)) return MF_E_ARG;
+  if (n_masks < 0 || n_masks > ctx->cfg.max_instances) return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  if (d_depth)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_depth, d_depth, 4 * WH, cudaMemcpyDeviceToDevice, ctx->stream));
+  if (d_rgb) {
+    rgb_convert_kernel<<<(unsigned)((WH + 255) / 256), 256, 0, ctx->stream>>>(
+        d_rgb, ctx->d_rgb, ctx->d_grey, (int)WH);
+    MF_CUDA(cudaGetLastError());
+  }
+  if (d_masks)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_masks, d_masks, 4 * WH * n_masks, cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+  return MF_OK;
+}
+
+int mf_frame_labels(mf_context* ctx, const uint16_t* labels) {
+  if (check(ctx) || !labels) return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_labels, labels, 2 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  const int n = (int)ctx->inst.size();
+  if (n > 0) {
+    dim3 grid((ctx->W + 127) / 128, ctx->H, n);
+    generalize_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->d_labels, ctx->W, ctx->H,
+                                                     ctx->d_inst_label, n, ctx->d_masks);
+    MF_CUDA(cudaGetLastError());
+  }
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_integrate(mf_context* ctx, const int* ids, int n) {
+  if (check(ctx) || n < 0 || (n > 0 && !ids)) return MF_E_ARG;
+  for (int i = 0; i < n; ++i)
+    if (ids[i] < 0 || ids[i] >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  if (ctx->cfg.batched) {
+    IdList l;
+    l.n = n;
+    for (int i = 0; i < n; ++i) l.v[i] = ids[i];
+    if (int rc = stage_prepare(ctx, l)) return rc;
+    if (int rc = stage_alloc(ctx, l)) return rc;
+    if (int rc = stage_integrate(ctx, l)) return rc;
+  } else {
+    for (int i = 0; i < n; ++i) {  // one instance per launch, like the reference's loop
+      IdList l;
+      l.n = 1;
+      l.v[0] = ids[i];
+      if (int rc = stage_prepare(ctx, l)) return rc;
+      if (int rc = stage_alloc(ctx, l)) return rc;
+      if (int rc = stage_integrate(ctx, l)) return rc;
+    }
+  }
+  return MF_OK;
+}
+
+int mf_alloc_update(mf_context* ctx, int id, const uint64_t* keys, int n) {
+  if (check(ctx) || n < 0 || (n > 0 && !keys)) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  uint64_t zero = 0;
+  return alloc_keys(ctx, id, n > 0 ? keys : &zero, n);
+}
+
+int mf_raycast(mf_context* ctx) {
+  if (check(ctx)) return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  const IdList l = all_ids(ctx);
+  if (int rc = stage_prepare(ctx, l)) return rc;
+  return stage_raycast(ctx, l, ctx->ray_epsilon);
+}
+
+int mf_download_raycast(mf_context* ctx, float* vertex, float* normal, int32_t* label) {
+  if (check(ctx)) return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  if (vertex)
+    MF_CUDA(cudaMemcpyAsync(vertex, ctx->d_vertex, 12 * WH, cudaMemcpyDeviceToHost, ctx->stream));
+  if (normal)
+    MF_CUDA(cudaMemcpyAsync(normal, ctx->d_normal, 12 * WH, cudaMemcpyDeviceToHost, ctx->stream));
+  if (label)
+    MF_CUDA(cudaMemcpyAsync(label, ctx->d_label, 4 * WH, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_block_count(mf_context* ctx, int id, int* n) {
+  if (check(ctx) || !n) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return export_blocks(ctx, id, nullptr, nullptr, nullptr, nullptr, 0, n);
+}
+
+int mf_export_blocks(mf_context* ctx, int id, uint64_t* keys, int32_t* coords, uint8_t* active,
+                     void* voxels, int cap, int* n) {
+  if (check(ctx)) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return export_blocks(ctx, id, keys, coords, active, voxels, cap, n);
+}
+
+int mf_node_count(mf_context* ctx, int id, int* n) {
+  if (check(ctx) || !n) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return export_nodes(ctx, id, nullptr, nullptr, nullptr, nullptr, 0, n);
+}
+
+int mf_export_nodes(mf_context* ctx, int id, uint64_t* keys, uint32_t* side,
+                    uint8_t* children_mask, void* values, int cap, int* n) {
+  if (check(ctx)) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return export_nodes(ctx, id, keys, side, children_mask, values, cap, n);
+}
+
+int mf_root_children(mf_context* ctx, int id, uint8_t* mask) {
+  if (check(ctx) || !mask) return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return root_children(ctx, id, mask);
+}
+
+int mf_interp(mf_context* ctx, int id, const float* pos, int n, int field, float* out) {
+  if (check(ctx) || n < 0 || (n > 0 && (!pos || !out)) || field < 0 || field > 1)
+    return MF_E_ARG;
+  if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return interp_points(ctx, id, pos, n, field, out);
+}
+
+}  // extern "C"

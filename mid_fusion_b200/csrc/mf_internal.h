@@ -1,0 +1,122 @@
+// Internal context of the MID-Fusion B200 library (not part of the C ABI).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/midfusion_b200.h"
+#include "mf_common.cuh"
+
+namespace mf {
+
+constexpr int MAX_INSTANCES = 32;
+constexpr int MAX_PYR = 4;
+
+// Instance ids of one stage, passed to kernels by value.
+struct IdList {
+  int n;
+  int v[32];
+};
+
+// Per-instance quantities derived on the device from the device-resident poses
+// before each stage (so a stage never waits on the host for a pose).
+struct InstFrame {
+  M4 T_w_o, inv_T_w_o;
+  // allocation (apps/kfusion/src/cpp/kfusion/alloc_impl.hpp:121-191)
+  M4 kPose;            // T_w_c * inverse(K)
+  F3 o_cam;            // camera centre in the volume frame
+  float inv_voxel;     // 1 / voxelSize
+  float band;          // 2 mu
+  int num_steps;
+  unsigned long long reserved;
+  // integration (lib/functors/projective_functor.hpp:43-166)
+  M4 Tcw;              // inverse(T_w_c) * T_w_o
+  M4 KTcw;             // K * Tcw
+  F3 delta, cam_delta;
+  // raycast (apps/kfusion/src/cpp/rendering/rendering.cpp:37-45)
+  F3 o_origin;
+  int label;
+  M4 view;             // T_w_c * inverse(K)
+  int pad[3];
+};
+
+struct Instance {
+  int size;
+  float dim;
+  int label;
+  Volume vol;          // device pointers, host copy
+  size_t reserved;     // reference allocation-list capacity
+};
+
+// One GN problem (camera or object) tracked on the device.
+struct TrackState;
+
+struct Context {
+  mf_config cfg;
+  int W = 0, H = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+  std::string last_error;
+
+  Pool pool{};                      // host copy of device pointers
+  std::vector<Instance> inst;
+  Volume* d_vols = nullptr;         // device copy of every instance's Volume
+  float* d_Two = nullptr;           // MAX_INSTANCES x 16 volume poses
+  float* d_Twc = nullptr;           // 16, camera pose
+  InstFrame* d_frames = nullptr;    // MAX_INSTANCES
+  int* d_status = nullptr;          // OR of Status flags
+  unsigned long long* d_reserved = nullptr;  // MAX_INSTANCES reference list capacities
+  int* d_inst_label = nullptr;      // MAX_INSTANCES instance labels
+  int* d_scratch_i = nullptr;       // small device scratch (export slot lists)
+  void* d_export = nullptr;         // export staging (grown on demand)
+  size_t export_bytes = 0;
+  int* d_visit = nullptr;           // integration visit list
+  int* d_visit_count = nullptr;
+
+  // frame inputs
+  float* d_depth = nullptr;         // W*H metres
+  uint8_t* d_rgb8 = nullptr;        // W*H*3
+  F3* d_rgb = nullptr;              // W*H in [0, 1]
+  float* d_grey = nullptr;          // W*H
+  float* d_masks = nullptr;         // MAX_INSTANCES x W*H generalized masks
+  uint16_t* d_labels = nullptr;     // W*H ground-truth instance labels
+
+  // raycast outputs (composite model maps)
+  F3* d_vertex = nullptr;
+  F3* d_normal = nullptr;
+  int* d_label = nullptr;
+
+  // staging
+  float* h_pinned = nullptr;        // small pinned host staging area
+  size_t h_pinned_bytes = 0;
+
+  float ray_epsilon = 0.f;          // ray iterator direction epsilon (first volume)
+  TrackState* track = nullptr;
+};
+
+#define MF_CUDA(call)                                                          \
+  do {                                                                         \
+    cudaError_t e__ = (call);                                                  \
+    if (e__ != cudaSuccess) {                                                  \
+      ctx->last_error = std::string(#call) + ": " + cudaGetErrorString(e__);   \
+      return MF_E_CUDA;                                                        \
+    }                                                                          \
+  } while (0)
+
+// kernels / stages implemented in the .cu files
+int stage_prepare(Context* ctx, const IdList& ids);
+int stage_alloc(Context* ctx, const IdList& ids);
+int stage_integrate(Context* ctx, const IdList& ids);
+int stage_raycast(Context* ctx, const IdList& ids, float epsilon);
+int alloc_keys(Context* ctx, int id, const uint64_t* keys, int n);
+int export_blocks(Context* ctx, int id, uint64_t* keys, int32_t* coords, uint8_t* active,
+                  void* voxels, int cap, int* n);
+int export_nodes(Context* ctx, int id, uint64_t* keys, uint32_t* side, uint8_t* cmask,
+                 void* values, int cap, int* n);
+int interp_points(Context* ctx, int id, const float* pos, int n, int field, float* out);
+int root_children(Context* ctx, int id, uint8_t* mask);
+int volume_create(Context* ctx, Instance& in);
+void volume_free(Instance& in);
+
+}  // namespace mf

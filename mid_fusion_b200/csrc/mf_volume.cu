@@ -1,0 +1,676 @@
+// Voxel-block allocation and projective TSDF integration on the device.
+//
+// Allocation is sort-free: each octree level is a dense table indexed by the
+// Morton code of its octants, so the reference's sort + unique_multiscale +
+// level-by-level updateLevel (lib/octree.hpp:761-863) becomes (1) every ray
+// sample of an unallocated block adds to that table entry's request count and
+// (2) one pass over the block table creates the requested blocks and flags their
+// ancestors.  The resulting key sets and topology equal the reference's; the
+// request counts also reproduce the reference's allocation-list quirks (see
+// alloc_commit_kernel).
+#include <algorithm>
+#include <cstring>
+#include "mf_internal.h"
+#include "mf_sample.cuh"
+
+namespace mf {
+
+// ------------------------------------------------------------------ prepare
+// Per-instance matrices every stage needs, computed from the device-resident
+// camera and volume poses with the reference's float operation order.
+__global__ void prepare_kernel(const float* __restrict__ Twc_p, const float* __restrict__ Two_p,
+                               const Volume* __restrict__ vols, InstFrame* __restrict__ out,
+                               F4 k, float mu, IdList ids,
+                               const unsigned long long* __restrict__ reserved,
+                               const int* __restrict__ labels) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ids.n) return;
+  const int i = ids.v[t];
+  M4 T_w_c, T_w_o;
+  memcpy(&T_w_c, Twc_p, 64);
+  memcpy(&T_w_o, Two_p + 16 * i, 64);
+  const Volume V = vols[i];
+  InstFrame f;
+  f.T_w_o = T_w_o;
+  f.inv_T_w_o = inverse(T_w_o);
+  const M4 K = camera_matrix(k);
+  f.kPose = mul(T_w_c, inverse(K));
+  f.o_cam = xform(f.inv_T_w_o, get_translation(T_w_c));
+  const float vs = V.dim / V.size;
+  f.inv_voxel = 1 / vs;
+  f.band = 2 * mu;
+  f.num_steps = (int)ceilf(f.band * f.inv_voxel);
+  f.reserved = reserved[i];
+  f.Tcw = mul(inverse(T_w_c), T_w_o);
+  f.KTcw = mul(K, f.Tcw);
+  f.delta = rotate(f.Tcw, mk3(vs, 0, 0));
+  f.cam_delta = rotate(K, f.delta);
+  const M4 view = mul(T_w_c, inverse_camera_matrix(k));
+  f.view = view;
+  f.o_origin = xform(f.inv_T_w_o, get_translation(view));
+  f.label = labels[i];
+  out[i] = f;
+}
+
+// ------------------------------------------------------------------ allocation
+// buildVolumeAllocationList, apps/kfusion/src/cpp/kfusion/alloc_impl.hpp:121-191.
+// One thread per (pixel, instance).  A sample in an allocated block marks it
+// active; a sample in an unallocated block adds to that block's request count
+// (runs of equal blocks along a ray are added at once).  The emission order of
+// the single-threaded reference (row, column, step) of the thread's last
+// emitted sample is folded into last_emit with atomicMax.
+__global__ void __launch_bounds__(256)
+alloc_mark_kernel(const float* __restrict__ depth, const float* __restrict__ masks, int W,
+                  int H, const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
+                  IdList ids, Pool pool) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= W * H) return;
+  const int inst = ids.v[blockIdx.y];
+  const float d = depth[p];
+  if (d == 0 || masks[(size_t)inst * W * H + p] < 0) return;
+  const Volume& V = vols[inst];
+  const InstFrame& F = frames[inst];
+  const unsigned x = p % W, y = p / W;
+  const float size_f = (float)(unsigned)V.size;
+  const F3 w_vertex = xform(F.kPose, mk3((x + 0.5f) * d, (y + 0.5f) * d, d));
+  const F3 o_vertex = xform(F.inv_T_w_o, w_vertex);
+  const F3 direction = normalize(F.o_cam - o_vertex);
+  const F3 origin = o_vertex - (F.band * 0.5f) * direction;
+  const F3 step = (direction * F.band) / (float)F.num_steps;
+  F3 pos = origin;
+  int run_idx = -1, run_len = 0;
+  unsigned count = 0, last_order = 0, last_idx = 0;
+  const int bshift = 3;
+  for (int i = 0; i < F.num_steps; i++) {
+    const F3 s = floor3(pos * F.inv_voxel);
+    if (s.x < size_f && s.y < size_f && s.z < size_f && s.x >= 0 && s.y >= 0 && s.z >= 0) {
+      const I3 v = to_i3(s);
+      const uint32_t bidx = (uint32_t)morton3(v.x >> bshift, v.y >> bshift, v.z >> bshift);
+      const int slot = V.block_tab[bidx];
+      if (slot >= 0) {
+        pool.active[slot] = 1;
+      } else {
+        if ((int)bidx == run_idx) {
+          ++run_len;
+        } else {
+          if (run_len) atomicAdd(&V.req[run_idx], (uint32_t)run_len);
+          run_idx = (int)bidx;
+          run_len = 1;
+        }
+        ++count;
+        last_order = (unsigned)p * (unsigned)F.num_steps + (unsigned)i;
+        last_idx = bidx;
+      }
+    }
+    pos = pos + step;
+  }
+  if (run_len) atomicAdd(&V.req[run_idx], (uint32_t)run_len);
+  if (count) {
+    atomicAdd(V.emit_total, (unsigned long long)count);
+    atomicMax(V.last_emit, ((unsigned long long)last_order << 32) | last_idx);
+  }
+}
+
+// Octree::alloc_update + updateLevel, lib/octree.hpp:761-786, :826-863.
+// One thread per (block-table entry, instance).  Reference semantics kept:
+//  - the list's slot 0 is never written (alloc_impl.hpp:175, pre-increment) and
+//    stays 0, and unique_multiscale keeps keys[0] unconditionally
+//    (lib/algorithms/unique.hpp:76-79), so the path to block (0,0,0) is
+//    allocated by every call;
+//  - [0, count) is passed on while the keys sit in slots 1..count, so the last
+//    emitted key is not allocated unless another sample requested its block.
+__global__ void __launch_bounds__(256)
+alloc_commit_kernel(const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
+                    IdList ids, Pool pool, int* __restrict__ status) {
+  const int inst = ids.v[blockIdx.y];
+  const Volume& V = vols[inst];
+  const long long n_tab = 1LL << (3 * V.block_level);
+  const long long bidx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (bidx >= n_tab) return;
+  const uint32_t r = V.req[bidx];
+  if (r == 0 && bidx != 0) return;
+  const unsigned long long total = *V.emit_total;
+  const unsigned long long last = *V.last_emit;
+  bool need = (r > 0) || (bidx == 0);
+  if (total >= frames[inst].reserved) {
+    if (bidx == 0) atomicOr(status, ST_ALLOC_OVERFLOW);
+  } else if (r == 1 && bidx != 0 && (long long)(last & 0xffffffffULL) == bidx) {
+    need = false;  // the dropped last slot was this block's only request
+  }
+  if (need && V.block_tab[bidx] < 0) {
+    const int slot = atomicAdd(pool.count, 1);
+    if (slot >= pool.cap) {
+      atomicOr(status, ST_POOL_FULL);
+    } else {
+      const int cx = (int)gather3((uint64_t)bidx) << 3;
+      const int cy = (int)gather3((uint64_t)bidx >> 1) << 3;
+      const int cz = (int)gather3((uint64_t)bidx >> 2) << 3;
+      pool.meta[slot] = make_int4(cx, cy, cz, inst);
+      pool.active[slot] = 1;
+      V.block_tab[bidx] = slot;
+      for (int l = V.block_level - 1; l >= 1; --l)
+        V.node_tab[V.node_off[l] + (bidx >> (3 * (V.block_level - l)))] = 1;
+    }
+  }
+  if (r) V.req[bidx] = 0;
+}
+
+// Octree::alloc_update on caller-supplied keys: (code, level) pairs already
+// reduced on the host to "create the octant at this level and its ancestors".
+__global__ void alloc_keys_kernel(const Volume* __restrict__ vols, int inst,
+                                  const unsigned long long* __restrict__ codes,
+                                  const int* __restrict__ levels, int n, Pool pool,
+                                  int* __restrict__ status) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const Volume& V = vols[inst];
+  const int L = levels[t];
+  const unsigned long long code = codes[t];
+  for (int l = 1; l <= L && l < V.block_level; ++l)
+    V.node_tab[V.node_off[l] + (long long)(code >> (3 * (V.max_level - l)))] = 1;
+  if (L == V.block_level) {
+    const long long bidx = (long long)(code >> (3 * (V.max_level - V.block_level)));
+    if (atomicCAS(&V.block_tab[bidx], -1, -2) == -1) {
+      const int slot = atomicAdd(pool.count, 1);
+      if (slot >= pool.cap) {
+        atomicOr(status, ST_POOL_FULL);
+        V.block_tab[bidx] = -1;
+        return;
+      }
+      pool.meta[slot] = make_int4((int)gather3(bidx) << 3, (int)gather3(bidx >> 1) << 3,
+                                  (int)gather3(bidx >> 2) << 3, inst);
+      pool.active[slot] = 1;
+      V.block_tab[bidx] = slot;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ integration
+// projective_functor::build_active_list, lib/functors/projective_functor.hpp:54-71
+// with algorithms::filter (lib/algorithms/filter.hpp:42-61, predicates ORed):
+// a block is visited when it is active or its corner projects into the frame.
+__global__ void __launch_bounds__(256)
+visit_list_kernel(Pool pool, const Volume* __restrict__ vols,
+                  const InstFrame* __restrict__ frames, uint32_t inst_mask, int W, int H,
+                  int* __restrict__ visit, int* __restrict__ visit_count) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  bool take = false;
+  if (slot < *pool.count) {
+    const int4 m = pool.meta[slot];
+    if ((inst_mask >> m.w) & 1u) {
+      if (pool.active[slot]) {
+        take = true;
+      } else {
+        const Volume& V = vols[m.w];
+        const float vs = V.dim / V.size;
+        const F3 bc = mk3((float)m.x, (float)m.y, (float)m.z) * vs;
+        const F3 vc = xform(frames[m.w].KTcw, bc);
+        const int px = (int)(vc.x / vc.z), py = (int)(vc.y / vc.z);
+        take = px >= 0 && px < W && py >= 0 && py < H;
+      }
+    }
+  }
+  // warp-aggregated append
+  const unsigned ballot = __ballot_sync(0xffffffffu, take);
+  if (!ballot) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == __ffs(ballot) - 1) base = atomicAdd(visit_count, __popc(ballot));
+  base = __shfl_sync(0xffffffffu, base, __ffs(ballot) - 1);
+  if (take) visit[base + __popc(ballot & ((1u << lane) - 1))] = slot;
+}
+
+struct SdfArgs {
+  const float* depth; const F3* rgb; const float* masks;
+  int W, H; float mu; float maxweight;
+};
+
+// sdf_update::operator(), apps/kfusion/src/cpp/kfusion/mapping_impl.hpp:17-49,
+// on one voxel held as separate field references.
+template <typename FT, typename FW, typename FC, typename FG, typename FWI>
+__device__ __forceinline__ void sdf_update(const SdfArgs& a, const float* mask, F3 pos,
+                                           float px_f, float py_f, FT& tsdf, FW& wt,
+                                           float* r, float* g, float* b, FC& c, FG& fg,
+                                           FWI& w) {
+  const unsigned px = (unsigned)px_f, py = (unsigned)py_f;
+  const float depthSample = a.depth[px + a.W * py];
+  const float m = mask[px + a.W * py];
+  if (depthSample <= 0 || m < 0) return;
+  const float diff =
+      (depthSample - pos.z) * sqrtf(1 + sq(pos.x / pos.z) + sq(pos.y / pos.z));
+  if (diff > -a.mu) {
+    const float sdf = fmn(1.f, diff / a.mu);
+    float x = tsdf, y = wt;
+    x = clampf((y * x + sdf) / (y + 1), -1.f, 1.f);
+    y = fmn(y + 1, a.maxweight);
+    tsdf = x; wt = y;
+    const F3 rgb = a.rgb[px + a.W * py];
+    const int cc = c;
+    *r = (rgb.x + *r * cc) / (cc + 1);
+    *g = (rgb.y + *g * cc) / (cc + 1);
+    *b = (rgb.z + *b * cc) / (cc + 1);
+    c = cc + 1;
+    const int ww = w;
+    fg = ((double)m + fg * ww) / (ww + 1);
+    w = ww + 1;
+  }
+}
+
+// projective_functor::update_block, lib/functors/projective_functor.hpp:73-111.
+// One CTA of 256 threads per visited block, two voxels per thread (v and
+// v + 256, i.e. z and z + 4): every field plane is read and written coalesced.
+// Field planes are only touched for voxels that pass the update test.
+__global__ void __launch_bounds__(256)
+integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
+                        const InstFrame* __restrict__ frames, SdfArgs args, F4 k,
+                        const int* __restrict__ visit, const int* __restrict__ visit_count) {
+  const int n = *visit_count;
+  const M4 K = camera_matrix(k);
+  const float wlim = args.W - 1.5f, hlim = args.H - 1.5f;
+  for (int item = blockIdx.x; item < n; item += gridDim.x) {
+    const int slot = visit[item];
+    const int4 m = pool.meta[slot];
+    const Volume& V = vols[m.w];
+    const InstFrame& F = frames[m.w];
+    const float vs = V.dim / V.size;
+    const float* mask = args.masks + (size_t)m.w * args.W * args.H;
+    bool visible = false;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int v = threadIdx.x + half * 256;
+      const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
+      const F3 start = xform(F.Tcw, mk3(m.x * vs, (m.y + y) * vs, (m.z + z) * vs));
+      const F3 camerastart = xform(K, start);
+      const F3 cv = camerastart + ((float)x * F.cam_delta);
+      const F3 pos = start + ((float)x * F.delta);
+      if (pos.z < 0.0001f) continue;
+      const float inv = 1.f / cv.z;
+      const float pxf = cv.x * inv + 0.5f, pyf = cv.y * inv + 0.5f;
+      if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) continue;
+      visible = true;
+      const size_t o = (size_t)slot * 512 + v;
+      sdf_update(args, mask, pos, pxf, pyf, pool.tsdf[o], pool.wt[o], &pool.r[o], &pool.g[o],
+                 &pool.b[o], pool.c[o], pool.fg[o], pool.w[o]);
+    }
+    const int any = __syncthreads_or(visible);
+    if (threadIdx.x == 0) pool.active[slot] = any ? 1 : 0;
+  }
+}
+
+// projective_functor::update_node, lib/functors/projective_functor.hpp:113-137,
+// over every internal node of the selected instances.  The reference takes the
+// node's voxel from unpack_morton(code) with the level bits still in the code,
+// and offsets child i by dir * rotate(Tcw, (h, h, h)) element-wise; both kept.
+__global__ void __launch_bounds__(128)
+integrate_nodes_kernel(const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
+                       SdfArgs args, F4 k, IdList ids) {
+  const int inst = ids.v[blockIdx.y];
+  const Volume& V = vols[inst];
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= V.n_nodes || !V.node_tab[e]) return;
+  int l = 1;
+  while (l + 1 < V.block_level && e >= V.node_off[l + 1]) ++l;
+  const unsigned long long mcode = (unsigned long long)(e - V.node_off[l]);
+  const unsigned long long code = (mcode << (3 * (V.max_level - l))) | (unsigned long long)l;
+  const InstFrame& F = frames[inst];
+  const M4 K = camera_matrix(k);
+  const float vs = V.dim / V.size;
+  const unsigned side = (unsigned)V.size >> l;
+  const F3 voxel = mk3((float)(int)gather3(code), (float)(int)gather3(code >> 1),
+                       (float)(int)gather3(code >> 2));
+  const F3 delta = rotate(F.Tcw, mk3(0.5f * vs * side));
+  const F3 delta_c = rotate(K, delta);
+  const F3 base_cam = xform(F.Tcw, voxel * vs);
+  const F3 basepix = xform(K, base_cam);
+  const float* mask = args.masks + (size_t)inst * args.W * args.H;
+  const float wlim = args.W - 1.5f, hlim = args.H - 1.5f;
+  for (int i = 0; i < 8; ++i) {
+    const F3 dir = mk3((float)((i & 1) > 0), (float)((i & 2) > 0), (float)((i & 4) > 0));
+    const F3 vox_cam = base_cam + dir * delta;
+    const F3 pix_hom = basepix + dir * delta_c;
+    if (vox_cam.z < 0.0001f) continue;
+    const float inv = 1.f / pix_hom.z;
+    const float pxf = pix_hom.x * inv + 0.5f, pyf = pix_hom.y * inv + 0.5f;
+    if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) continue;
+    const size_t o = (size_t)e * 8 + i;
+    sdf_update(args, mask, vox_cam, pxf, pyf, V.n_tsdf[o], V.n_wt[o], &V.n_r[o], &V.n_g[o],
+               &V.n_b[o], V.n_c[o], V.n_fg[o], V.n_w[o]);
+  }
+}
+
+__global__ void interp_points_kernel(Pool pool, const Volume* __restrict__ vols, int inst,
+                                     const float* __restrict__ pos, int n, int field,
+                                     float* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  out[t] = volume_interp(pool, vols[inst], mk3(pos[3 * t], pos[3 * t + 1], pos[3 * t + 2]),
+                         field);
+}
+
+// Gather selected blocks into the reference's 40-byte AoS voxel layout.
+__global__ void export_blocks_kernel(Pool pool, const int* __restrict__ slots, int n,
+                                     unsigned char* __restrict__ out) {
+  const int b = blockIdx.x;
+  if (b >= n) return;
+  const int slot = slots[b];
+  for (int v = threadIdx.x; v < 512; v += blockDim.x) {
+    const size_t o = (size_t)slot * 512 + v;
+    unsigned char* d = out + ((size_t)b * 512 + v) * 40;
+    *(float*)(d + 0) = pool.tsdf[o];
+    *(float*)(d + 4) = pool.wt[o];
+    *(float*)(d + 8) = pool.r[o];
+    *(float*)(d + 12) = pool.g[o];
+    *(float*)(d + 16) = pool.b[o];
+    *(int*)(d + 20) = pool.c[o];
+    *(double*)(d + 24) = pool.fg[o];
+    *(int*)(d + 32) = pool.w[o];
+    *(int*)(d + 36) = 0;
+  }
+}
+
+// ------------------------------------------------------------------ host side
+static int div_up(long long a, int b) { return (int)((a + b - 1) / b); }
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t count) {
+  return cudaMalloc((void**)p, sizeof(T) * (count ? count : 1));
+}
+
+__global__ void fill_node_values_kernel(Volume V) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= V.n_nodes * 8) return;
+  V.n_tsdf[i] = 1.f; V.n_wt[i] = 0.f; V.n_r[i] = 0.f; V.n_g[i] = 0.f; V.n_b[i] = 0.f;
+  V.n_c[i] = 0; V.n_fg[i] = 0.0; V.n_w[i] = 0;
+}
+
+int volume_create(Context* ctx, Instance& in) {
+  Volume& V = in.vol;
+  std::memset(&V, 0, sizeof(V));
+  V.size = in.size;
+  V.dim = in.dim;
+  int ml = 0;
+  while ((1 << ml) < in.size) ++ml;
+  V.max_level = ml;
+  V.block_level = ml - 3;
+  long long off = 0;
+  for (int l = 1; l < V.block_level; ++l) { V.node_off[l] = off; off += 1LL << (3 * l); }
+  V.node_off[V.block_level] = off;
+  V.n_nodes = off;
+  const long long n_tab = 1LL << (3 * V.block_level);
+  MF_CUDA(dalloc(&V.block_tab, n_tab));
+  MF_CUDA(cudaMemsetAsync(V.block_tab, 0xff, sizeof(int32_t) * n_tab, ctx->stream));
+  MF_CUDA(dalloc(&V.req, n_tab));
+  MF_CUDA(cudaMemsetAsync(V.req, 0, sizeof(uint32_t) * n_tab, ctx->stream));
+  MF_CUDA(dalloc(&V.node_tab, V.n_nodes));
+  MF_CUDA(cudaMemsetAsync(V.node_tab, 0, V.n_nodes ? V.n_nodes : 1, ctx->stream));
+  const size_t nv = (size_t)V.n_nodes * 8;
+  MF_CUDA(dalloc(&V.n_tsdf, nv)); MF_CUDA(dalloc(&V.n_wt, nv));
+  MF_CUDA(dalloc(&V.n_r, nv)); MF_CUDA(dalloc(&V.n_g, nv)); MF_CUDA(dalloc(&V.n_b, nv));
+  MF_CUDA(dalloc(&V.n_c, nv)); MF_CUDA(dalloc(&V.n_fg, nv)); MF_CUDA(dalloc(&V.n_w, nv));
+  MF_CUDA(dalloc(&V.last_emit, 1)); MF_CUDA(dalloc(&V.emit_total, 1));
+  if (nv) fill_node_values_kernel<<<div_up(nv, 256), 256, 0, ctx->stream>>>(V);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+void volume_free(Instance& in) {
+  Volume& V = in.vol;
+  void* ps[] = {V.block_tab, V.req, V.node_tab, V.n_tsdf, V.n_wt, V.n_r, V.n_g, V.n_b,
+                V.n_c, V.n_fg, V.n_w, V.last_emit, V.emit_total};
+  for (void* p : ps) if (p) cudaFree(p);
+  std::memset(&V, 0, sizeof(V));
+}
+
+
+int stage_prepare(Context* ctx, const IdList& ids) {
+  if (ids.n == 0) return MF_OK;
+  const mf_config& c = ctx->cfg;
+  prepare_kernel<<<1, 32, 0, ctx->stream>>>(ctx->d_Twc, ctx->d_Two, ctx->d_vols, ctx->d_frames,
+                                             F4{c.k[0], c.k[1], c.k[2], c.k[3]}, c.mu, ids,
+                                             ctx->d_reserved, ctx->d_inst_label);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int stage_alloc(Context* ctx, const IdList& ids) {
+  if (ids.n == 0) return MF_OK;
+  const int WH = ctx->W * ctx->H;
+  int max_tab = 0;
+  for (int i = 0; i < ids.n; ++i) {
+    const Volume& V = ctx->inst[ids.v[i]].vol;
+    MF_CUDA(cudaMemsetAsync(V.last_emit, 0, sizeof(unsigned long long), ctx->stream));
+    MF_CUDA(cudaMemsetAsync(V.emit_total, 0, sizeof(unsigned long long), ctx->stream));
+    max_tab = std::max(max_tab, 1 << (3 * V.block_level));
+  }
+  alloc_mark_kernel<<<dim3(div_up(WH, 256), ids.n), 256, 0, ctx->stream>>>(
+      ctx->d_depth, ctx->d_masks, ctx->W, ctx->H, ctx->d_vols, ctx->d_frames, ids, ctx->pool);
+  MF_CUDA(cudaGetLastError());
+  alloc_commit_kernel<<<dim3(div_up(max_tab, 256), ids.n), 256, 0, ctx->stream>>>(
+      ctx->d_vols, ctx->d_frames, ids, ctx->pool, ctx->d_status);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int stage_integrate(Context* ctx, const IdList& ids) {
+  if (ids.n == 0) return MF_OK;
+  const mf_config& c = ctx->cfg;
+  uint32_t mask = 0;
+  long long max_nodes = 0;
+  for (int i = 0; i < ids.n; ++i) {
+    mask |= 1u << ids.v[i];
+    max_nodes = std::max(max_nodes, ctx->inst[ids.v[i]].vol.n_nodes);
+  }
+  MF_CUDA(cudaMemsetAsync(ctx->d_visit_count, 0, sizeof(int), ctx->stream));
+  visit_list_kernel<<<div_up(ctx->pool.cap, 256), 256, 0, ctx->stream>>>(
+      ctx->pool, ctx->d_vols, ctx->d_frames, mask, ctx->W, ctx->H, ctx->d_visit,
+      ctx->d_visit_count);
+  MF_CUDA(cudaGetLastError());
+  SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
+  const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  integrate_blocks_kernel<<<sms * 8, 256, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
+                                                           a, k, ctx->d_visit, ctx->d_visit_count);
+  MF_CUDA(cudaGetLastError());
+  if (max_nodes > 0) {
+    integrate_nodes_kernel<<<dim3(div_up(max_nodes, 128), ids.n), 128, 0, ctx->stream>>>(
+        ctx->d_vols, ctx->d_frames, a, k, ids);
+    MF_CUDA(cudaGetLastError());
+  }
+  return MF_OK;
+}
+
+// Octree::alloc_update(keys, n), lib/octree.hpp:761-786, on explicit keys.
+// Set semantics of the reference: after sorting, every key of level L >= 1
+// creates its prefix octant at level min(L, block level) and the ancestors;
+// the smallest key is kept at every level (unique.hpp:76-79), which creates
+// its whole path down to a block.
+int alloc_keys(Context* ctx, int id, const uint64_t* keys, int n) {
+  Instance& in = ctx->inst[id];
+  const Volume& V = in.vol;
+  std::vector<unsigned long long> codes;
+  std::vector<int> levels;
+  uint64_t kmin = ~0ULL;
+  const int cnt = n < 1 ? 1 : n;  // unique_multiscale returns 1 for n < 2
+  for (int i = 0; i < cnt; ++i) kmin = std::min<uint64_t>(kmin, keys[i]);
+  for (int i = 0; i < cnt; ++i) {
+    int L = (int)(keys[i] & SCALE_MASK);
+    if (keys[i] == kmin) L = V.block_level;
+    if (L < 1) continue;
+    if (L > V.block_level) L = V.block_level;
+    codes.push_back(keys[i] & ~SCALE_MASK);
+    levels.push_back(L);
+  }
+  if (codes.empty()) return MF_OK;
+  unsigned long long* d_codes = nullptr;
+  int* d_levels = nullptr;
+  MF_CUDA(cudaMalloc(&d_codes, sizeof(unsigned long long) * codes.size()));
+  MF_CUDA(cudaMalloc(&d_levels, sizeof(int) * levels.size()));
+  MF_CUDA(cudaMemcpyAsync(d_codes, codes.data(), sizeof(unsigned long long) * codes.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(d_levels, levels.data(), sizeof(int) * levels.size(),
+                          cudaMemcpyHostToDevice, ctx->stream));
+  alloc_keys_kernel<<<div_up((long long)codes.size(), 256), 256, 0, ctx->stream>>>(
+      ctx->d_vols, id, d_codes, d_levels, (int)codes.size(), ctx->pool, ctx->d_status);
+  MF_CUDA(cudaGetLastError());
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  cudaFree(d_codes);
+  cudaFree(d_levels);
+  return MF_OK;
+}
+
+static int ensure_export(Context* ctx, size_t bytes) {
+  if (ctx->export_bytes >= bytes) return MF_OK;
+  if (ctx->d_export) cudaFree(ctx->d_export);
+  ctx->d_export = nullptr;
+  ctx->export_bytes = 0;
+  MF_CUDA(cudaMalloc(&ctx->d_export, bytes));
+  ctx->export_bytes = bytes;
+  return MF_OK;
+}
+
+int export_blocks(Context* ctx, int id, uint64_t* keys, int32_t* coords, uint8_t* active,
+                  void* voxels, int cap, int* n_out) {
+  const Volume& V = ctx->inst[id].vol;
+  const long long n_tab = 1LL << (3 * V.block_level);
+  std::vector<int32_t> tab(n_tab);
+  MF_CUDA(cudaMemcpyAsync(tab.data(), V.block_tab, sizeof(int32_t) * n_tab,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::vector<int> slots;
+  std::vector<long long> bidx;
+  for (long long b = 0; b < n_tab; ++b)
+    if (tab[b] >= 0) { slots.push_back(tab[b]); bidx.push_back(b); }
+  const int n = (int)slots.size();
+  if (n_out) *n_out = n;
+  if (!keys && !coords && !active && !voxels) return MF_OK;
+  if (n > cap) return MF_E_ARG;
+  if (n == 0) return MF_OK;
+  std::vector<uint8_t> act;
+  if (active) {
+    std::vector<uint8_t> all(ctx->pool.cap);
+    MF_CUDA(cudaMemcpy(all.data(), ctx->pool.active, ctx->pool.cap, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n; ++i) active[i] = all[slots[i]];
+  }
+  for (int i = 0; i < n; ++i) {
+    const uint64_t b = (uint64_t)bidx[i];
+    if (keys) keys[i] = (b << (3 * (V.max_level - V.block_level))) | (uint64_t)V.block_level;
+    if (coords) {
+      coords[3 * i] = (int)gather3(b) << 3;
+      coords[3 * i + 1] = (int)gather3(b >> 1) << 3;
+      coords[3 * i + 2] = (int)gather3(b >> 2) << 3;
+    }
+  }
+  if (voxels) {
+    const int chunk = 4096;
+    if (int rc = ensure_export(ctx, (size_t)chunk * 512 * 40 + sizeof(int) * chunk)) return rc;
+    int* d_slots = (int*)((char*)ctx->d_export + (size_t)chunk * 512 * 40);
+    for (int s0 = 0; s0 < n; s0 += chunk) {
+      const int m = std::min(chunk, n - s0);
+      MF_CUDA(cudaMemcpyAsync(d_slots, slots.data() + s0, sizeof(int) * m,
+                              cudaMemcpyHostToDevice, ctx->stream));
+      export_blocks_kernel<<<m, 256, 0, ctx->stream>>>(ctx->pool, d_slots, m,
+                                                       (unsigned char*)ctx->d_export);
+      MF_CUDA(cudaGetLastError());
+      MF_CUDA(cudaMemcpyAsync((char*)voxels + (size_t)s0 * 512 * 40, ctx->d_export,
+                              (size_t)m * 512 * 40, cudaMemcpyDeviceToHost, ctx->stream));
+      MF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+  }
+  return MF_OK;
+}
+
+int export_nodes(Context* ctx, int id, uint64_t* keys, uint32_t* side, uint8_t* cmask,
+                 void* values, int cap, int* n_out) {
+  const Volume& V = ctx->inst[id].vol;
+  const long long nn = V.n_nodes;
+  std::vector<uint8_t> nt(nn > 0 ? nn : 1);
+  const long long n_tab = 1LL << (3 * V.block_level);
+  std::vector<int32_t> tab(n_tab);
+  if (nn > 0)
+    MF_CUDA(cudaMemcpyAsync(nt.data(), V.node_tab, nn, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(tab.data(), V.block_tab, sizeof(int32_t) * n_tab,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  std::vector<long long> ent;
+  for (long long e = 0; e < nn; ++e) if (nt[e]) ent.push_back(e);
+  const int n = (int)ent.size();
+  if (n_out) *n_out = n;
+  if (!keys && !side && !cmask && !values) return MF_OK;
+  if (n > cap) return MF_E_ARG;
+  std::vector<float> f[5];
+  std::vector<int> ci, wi;
+  std::vector<double> fg;
+  if (values && nn > 0) {
+    float* planes[5] = {V.n_tsdf, V.n_wt, V.n_r, V.n_g, V.n_b};
+    for (int q = 0; q < 5; ++q) {
+      f[q].resize(nn * 8);
+      MF_CUDA(cudaMemcpy(f[q].data(), planes[q], sizeof(float) * nn * 8, cudaMemcpyDeviceToHost));
+    }
+    ci.resize(nn * 8); wi.resize(nn * 8); fg.resize(nn * 8);
+    MF_CUDA(cudaMemcpy(ci.data(), V.n_c, sizeof(int) * nn * 8, cudaMemcpyDeviceToHost));
+    MF_CUDA(cudaMemcpy(wi.data(), V.n_w, sizeof(int) * nn * 8, cudaMemcpyDeviceToHost));
+    MF_CUDA(cudaMemcpy(fg.data(), V.n_fg, sizeof(double) * nn * 8, cudaMemcpyDeviceToHost));
+  }
+  for (int i = 0; i < n; ++i) {
+    const long long e = ent[i];
+    int l = 1;
+    while (l + 1 < V.block_level && e >= V.node_off[l + 1]) ++l;
+    const uint64_t m = (uint64_t)(e - V.node_off[l]);
+    if (keys) keys[i] = (m << (3 * (V.max_level - l))) | (uint64_t)l;
+    if (side) side[i] = (uint32_t)(V.size >> l);
+    if (cmask) {
+      uint8_t cm = 0;
+      for (int c = 0; c < 8; ++c) {
+        const uint64_t child = m * 8 + c;
+        const bool ex = (l + 1 == V.block_level) ? tab[child] >= 0 : nt[V.node_off[l + 1] + child] != 0;
+        if (ex) cm |= (uint8_t)(1 << c);
+      }
+      cmask[i] = cm;
+    }
+    if (values) {
+      for (int c = 0; c < 8; ++c) {
+        unsigned char* d = (unsigned char*)values + ((size_t)i * 8 + c) * 40;
+        const size_t o = (size_t)e * 8 + c;
+        std::memcpy(d + 0, &f[0][o], 4); std::memcpy(d + 4, &f[1][o], 4);
+        std::memcpy(d + 8, &f[2][o], 4); std::memcpy(d + 12, &f[3][o], 4);
+        std::memcpy(d + 16, &f[4][o], 4); std::memcpy(d + 20, &ci[o], 4);
+        std::memcpy(d + 24, &fg[o], 8); std::memcpy(d + 32, &wi[o], 4);
+        std::memset(d + 36, 0, 4);
+      }
+    }
+  }
+  return MF_OK;
+}
+
+int root_children(Context* ctx, int id, uint8_t* mask) {
+  const Volume& V = ctx->inst[id].vol;
+  uint8_t cm = 0;
+  if (V.block_level == 1) {
+    int32_t tab[8];
+    MF_CUDA(cudaMemcpy(tab, V.block_tab, sizeof(tab), cudaMemcpyDeviceToHost));
+    for (int c = 0; c < 8; ++c) if (tab[c] >= 0) cm |= (uint8_t)(1 << c);
+  } else {
+    uint8_t nt[8];
+    MF_CUDA(cudaMemcpy(nt, V.node_tab + V.node_off[1], 8, cudaMemcpyDeviceToHost));
+    for (int c = 0; c < 8; ++c) if (nt[c]) cm |= (uint8_t)(1 << c);
+  }
+  *mask = cm;
+  return MF_OK;
+}
+
+int interp_points(Context* ctx, int id, const float* pos, int n, int field, float* out) {
+  if (n <= 0) return MF_OK;
+  if (int rc = ensure_export(ctx, sizeof(float) * 4 * n)) return rc;
+  float* d_pos = (float*)ctx->d_export;
+  float* d_out = d_pos + 3 * n;
+  MF_CUDA(cudaMemcpyAsync(d_pos, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  interp_points_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, id, d_pos,
+                                                                n, field, d_out);
+  MF_CUDA(cudaGetLastError());
+  MF_CUDA(cudaMemcpyAsync(out, d_out, sizeof(float) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+}  // namespace mf

@@ -432,10 +432,11 @@ float ray_first_block(const Volume& V, F3 origin, F3 direction, float nearPlane,
       if (step_mask & 4) differing |= (unsigned)(f2i(pos.z) ^ f2i(pos.z + scale_exp2));
       scale = (f2i((float)differing) >> 23) - 127;
       scale_exp2 = i2f((scale - CAST + 127) << 23);
-      if (scale < CAST) {  // the reference reads stack[23] out of bounds here
-        parent = stack[scale].parent;
-        t_max = stack[scale].t_max;
-      }
+      // scale >= 23: the ray left the root and next() returns -1 (the reference
+      // first reads stack[23], one past the array; the value is never used).
+      if (scale >= CAST) return -1.f;
+      parent = stack[scale].parent;
+      t_max = stack[scale].t_max;
       const int shx = f2i(pos.x) >> scale, shy = f2i(pos.y) >> scale, shz = f2i(pos.z) >> scale;
       pos.x = i2f(shx << scale); pos.y = i2f(shy << scale); pos.z = i2f(shz << scale);
       idx = (shx & 1) | ((shy & 1) << 1) | ((shz & 1) << 2);

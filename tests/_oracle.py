@@ -26,6 +26,19 @@ VOXEL_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("r", "<f4"), ("g", "<f4"), 
 assert VOXEL_DTYPE.itemsize == 40
 
 
+def encode(x, y, z, level, max_depth):
+    """keyops::encode, lib/octant_ops.hpp:51-55 (pure Python, for fixtures)."""
+    def spread(v):
+        r = 0
+        for i in range(21):
+            r |= ((v >> i) & 1) << (3 * i)
+        return r
+    offset = 21 - max_depth + level - 1
+    full = 0x7FFFFFFFFFFFFFFF
+    mask = (full >> (60 - 3 * offset)) << (60 - 3 * offset) & full
+    return ((spread(x) | spread(y) << 1 | spread(z) << 2) & mask) | level
+
+
 def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
 
