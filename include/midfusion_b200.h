@@ -120,6 +120,37 @@ int mf_raycast(mf_context* ctx);
 /* Copy the composite maps to the host (any pointer may be NULL). */
 int mf_download_raycast(mf_context* ctx, float* vertex, float* normal, int32_t* label);
 
+/* --- tracking ---------------------------------------------------------
+ * Tracking::set_params_frame (tracking/tracking.cpp:142-171): bilateral
+ * filter of intensity and depth, robust half-sampled pyramid, vertex, normal,
+ * gradient and ICP-covariance maps of the current frame. */
+int mf_preprocess(mf_context* ctx);
+/* Tracking::setRefImgFromCurr (tracking.cpp:1400-1413): the current frame's
+ * intensity and vertex pyramids become the photometric reference. */
+int mf_set_ref_from_current(mf_context* ctx);
+/* Tracking::trackLiveFrame (tracking.cpp:208-357, mask variant :1750-1879)
+ * against the composite model maps of the last mf_raycast: the camera pose is
+ * updated in place on the device.  Pixels whose model label has its bit set in
+ * `moving_labels` are excluded from ICP (the dynamic-object mask); 0 = none. */
+int mf_track_camera(mf_context* ctx, uint32_t moving_labels);
+/* Tracking::trackEachObject (tracking.cpp:580-708) for each id (>= 1) against
+ * its own model map; T_w_c1 is the camera pose before the last camera update
+ * (mf_track_camera or mf_set_camera_pose), T_w_c2 the current one.  The volume
+ * poses are updated on the device. */
+int mf_track_objects(mf_context* ctx, const int* ids, int n);
+/* Diagnostics of a GN problem (slot 0: camera, slot i: object i): iterations
+ * per level (int[4]), last normal-equation sums per level (double[4][32]),
+ * FP64 pose (double[16]); any pointer may be NULL. */
+int mf_track_info(mf_context* ctx, int slot, int* iterations, double* sums, double* pose);
+/* One evaluation of the normal equations (the 32 reduceKernel sums,
+ * tracking.cpp:1191-1352) of a problem at `level` and at `pose` (NULL: its
+ * current pose), without a GN step. */
+int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, double* sums);
+/* Pyramid planes of the current frame: which 0 depth, 1 intensity, 2 vertex,
+ * 3 normal, 4 x-gradient, 5 y-gradient, 6 ICP covariance, 7 camera reference
+ * vertex (float3 planes are 3 floats per pixel). */
+int mf_download_pyramid(mf_context* ctx, int level, int which, float* out);
+
 /* --- inspection (parity checks, debugging) -----------------------------
  * Blocks: key (code | level), corner voxel, VoxelBlock::active_, and when
  * `voxels` is not NULL the 512 voxels in the reference's 40-byte AoS layout

@@ -31,6 +31,8 @@ EXPORTS = [
     "mf_frame_upload", "mf_frame_set_device", "mf_frame_labels", "mf_integrate",
     "mf_alloc_update", "mf_raycast", "mf_download_raycast", "mf_block_count",
     "mf_export_blocks", "mf_node_count", "mf_export_nodes", "mf_root_children", "mf_interp",
+    "mf_preprocess", "mf_set_ref_from_current", "mf_track_camera", "mf_track_objects",
+    "mf_track_info", "mf_track_eval", "mf_download_pyramid",
 ]
 
 
@@ -190,6 +192,46 @@ class Context:
         s = C.c_void_p()
         self._check(self.lib.mf_get_stream(self.h, C.byref(s)))
         return s.value
+
+    # ---------------------------------------------------------------- tracking
+    def preprocess(self):
+        self._check(self.lib.mf_preprocess(self.h))
+
+    def set_ref_from_current(self):
+        self._check(self.lib.mf_set_ref_from_current(self.h))
+
+    def track_camera(self, moving_labels=()):
+        bits = 0
+        for l in moving_labels:
+            bits |= 1 << int(l)
+        self._check(self.lib.mf_track_camera(self.h, C.c_uint32(bits)))
+
+    def track_objects(self, ids):
+        ids = np.ascontiguousarray(ids, np.int32)
+        self._check(self.lib.mf_track_objects(self.h, _ptr(ids, np.int32), len(ids)))
+
+    def track_info(self, slot):
+        it = np.zeros(4, np.int32)
+        sums = np.zeros((4, 32), np.float64)
+        T = np.zeros(16, np.float64)
+        self._check(self.lib.mf_track_info(self.h, slot, _ptr(it, np.int32),
+                                           _ptr(sums, np.float64), _ptr(T, np.float64)))
+        return it, sums, T.reshape(4, 4)
+
+    def track_eval(self, slot, level, pose=None):
+        sums = np.zeros(32, np.float64)
+        p = None if pose is None else _m4(pose)
+        self._check(self.lib.mf_track_eval(self.h, slot, level, _ptr(p, np.float32),
+                                           _ptr(sums, np.float64)))
+        return sums
+
+    def pyramid(self, level, which):
+        w, h = self.W >> level, self.H >> level
+        out = np.zeros(w * h * 3, np.float32)
+        self._check(self.lib.mf_download_pyramid(self.h, level, which, _ptr(out, np.float32)))
+        if which in (2, 3, 6, 7):
+            return out.reshape(h, w, 3)
+        return out[:w * h].reshape(h, w)
 
     # ---------------------------------------------------------------- inspection
     def blocks(self, i, with_voxels=True):

@@ -177,6 +177,7 @@ int mf_create(const mf_config* cfg, mf_context** out) {
 int mf_destroy(mf_context* ctx) {
   if (!ctx) return MF_E_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  track_free(ctx);
   for (auto& in : ctx->inst) volume_free(in);
   Pool& P = ctx->pool;
   void* ps[] = {P.tsdf, P.wt, P.r, P.g, P.b, P.c, P.fg, P.w, P.meta, P.active, P.count,
@@ -271,6 +272,8 @@ int mf_instance_get_pose(mf_context* ctx, int id, float T[16]) {
 
 int mf_set_camera_pose(mf_context* ctx, const float T[16]) {
   if (check(ctx) || !T) return MF_E_ARG;
+  if (int rc = track_init(ctx)) return rc;
+  track_save_prev_camera(ctx);  // the replaced pose becomes T_w_c1 for object tracking
   MF_CUDA(cudaMemcpyAsync(ctx->d_Twc, T, 64, cudaMemcpyHostToDevice, ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
   return MF_OK;
@@ -426,6 +429,51 @@ int mf_interp(mf_context* ctx, int id, const float* pos, int n, int field, float
     return MF_E_ARG;
   if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
   return interp_points(ctx, id, pos, n, field, out);
+}
+
+int mf_preprocess(mf_context* ctx) {
+  if (check(ctx)) return MF_E_ARG;
+  return track_preprocess(ctx);
+}
+
+int mf_set_ref_from_current(mf_context* ctx) {
+  if (check(ctx)) return MF_E_ARG;
+  return track_set_ref(ctx);
+}
+
+int mf_track_camera(mf_context* ctx, uint32_t moving_labels) {
+  if (check(ctx)) return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  return track_camera(ctx, moving_labels);
+}
+
+int mf_track_objects(mf_context* ctx, const int* ids, int n) {
+  if (check(ctx) || n < 0 || n > 31 || (n > 0 && !ids)) return MF_E_ARG;
+  IdList l;
+  l.n = n;
+  for (int i = 0; i < n; ++i) {
+    if (ids[i] <= 0 || ids[i] >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+    l.v[i] = ids[i];
+  }
+  return track_objects(ctx, l);
+}
+
+int mf_track_info(mf_context* ctx, int slot, int* iterations, double* sums, double* pose) {
+  if (check(ctx) || slot < 0 || slot >= ctx->cfg.max_instances) return MF_E_ARG;
+  const int rc = track_info(ctx, slot, iterations, sums, pose);
+  return rc < 0 ? rc : MF_OK;
+}
+
+int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, double* sums) {
+  if (check(ctx) || !sums || slot < 0 || slot >= ctx->cfg.max_instances || level < 0 ||
+      level >= ctx->cfg.pyramid_levels)
+    return MF_E_ARG;
+  return track_eval(ctx, slot, level, pose, sums);
+}
+
+int mf_download_pyramid(mf_context* ctx, int level, int which, float* out) {
+  if (check(ctx) || !out || level < 0 || level >= ctx->cfg.pyramid_levels) return MF_E_ARG;
+  return track_download_level(ctx, level, which, out);
 }
 
 }  // extern "C"

@@ -116,6 +116,16 @@ int export_nodes(Context* ctx, int id, uint64_t* keys, uint32_t* side, uint8_t* 
                  void* values, int cap, int* n);
 int interp_points(Context* ctx, int id, const float* pos, int n, int field, float* out);
 int root_children(Context* ctx, int id, uint8_t* mask);
+int track_init(Context* ctx);
+void track_free(Context* ctx);
+int track_preprocess(Context* ctx);
+int track_set_ref(Context* ctx);
+int track_camera(Context* ctx, uint32_t moving);
+int track_objects(Context* ctx, const IdList& ids);
+int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
+int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
+int track_download_level(Context* ctx, int L, int which, float* out);
+void track_save_prev_camera(Context* ctx);
 int volume_create(Context* ctx, Instance& in);
 void volume_free(Instance& in);
 

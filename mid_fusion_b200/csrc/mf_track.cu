@@ -1,0 +1,991 @@
+// ICP + photometric Gauss-Newton tracking on the device.
+//
+// Reference: apps/kfusion/src/cpp/tracking/tracking.cpp (Tracking) and
+// apps/kfusion/src/cpp/preprocessing/*.  Per GN iteration one kernel evaluates
+// the ICP row and the photometric row of every pixel of the level for every
+// problem of the stage (the camera, or all moving objects at once), weights
+// them (IRLS), and reduces the 29 sums of the normal equations plus the three
+// outlier counts:
+//   - per thread in FP32 with Kahan-compensated accumulation,
+//   - per warp / block / grid in FP64 (block partials, fixed order),
+// and the block that finishes last for a problem runs that problem's GN step
+// on the device (cost test, step back, FP64 6x6 solve, SE(3) update,
+// convergence test).  The host only launches: the whole coarse-to-fine loop is
+// a fixed sequence of launches, and problems that stopped skip their work.
+#include <algorithm>
+#include <cmath>
+#include <cstddef>
+#include <cstring>
+#include <vector>
+#include "mf_internal.h"
+#include "mf_solve.cuh"
+
+namespace mf {
+
+constexpr float INVALIDF = -2.f;
+constexpr int GN_THREADS = 256;
+constexpr int GN_PIX = 4;  // pixels per thread per iteration
+constexpr int GN_TILE = GN_THREADS * GN_PIX;
+
+struct GNState {
+  double T[16], prevT[16];
+  double prev_err;
+  int done;
+  int kind;          // 0 camera, 1 object
+  int label;
+  int inst;
+  int iters[MAX_PYR];
+  int fallback;
+  int ticket;
+  int pad_;
+  M4 Tf, invTf;      // float pose (and inverse) seen by the per-pixel kernels
+  M4 T_w_r, inv_T_w_r, view;               // camera: reference pose, K * inverse(T_w_r)
+  M4 T_c1_o1, inv_T_c1_o1, inv_T_w_o1, T_w_c2;  // object constants
+  double sums[MAX_PYR][32];
+};
+
+struct PyrPtrs {
+  int w[MAX_PYR], h[MAX_PYR];
+  float* D[MAX_PYR];
+  float* I[2][MAX_PYR];
+  F3* V[2][MAX_PYR];
+  F3* N[MAX_PYR];
+  float* GX[MAX_PYR];
+  float* GY[MAX_PYR];
+  F3* COV[MAX_PYR];
+  uint8_t* MASK[MAX_PYR];
+};
+
+struct TrackState {
+  int levels = 0;
+  PyrPtrs pyr{};
+  int cur = 0;                      // live set; 1 - cur holds the reference frame
+  bool have_ref = false;
+  float* rD[MAX_INSTANCES][MAX_PYR] = {};
+  F3* rV[MAX_INSTANCES][MAX_PYR] = {};
+  GNState* d_state = nullptr;       // MAX_INSTANCES (slot 0: camera, slot i: object i)
+  double* d_partials = nullptr;     // MAX_INSTANCES x max_tiles x 32
+  int max_tiles = 0;
+  float* d_Twc_prev = nullptr;      // camera pose of the previous frame
+  uint8_t* d_mask0 = nullptr;       // full-resolution ICP outlier mask
+  float gaussian[5];
+  std::vector<void*> allocs;
+};
+
+// ------------------------------------------------------------------ preprocessing
+struct Gauss5 { float g[5]; };
+
+// bilateralFilterKernel, preprocessing.cpp:11-50 (e_d = 0.1, r = 2) on the
+// intensity (z = 0) and the depth (z = 1).  Neighbour coordinates clamp to the
+// image (the reference's host clamp on unsigned values goes through int min/max,
+// utils/cutil_math.h:51-57, 987-989).
+__global__ void bilateral_kernel(const float* __restrict__ grey, const float* __restrict__ depth,
+                                 float* __restrict__ out_i, float* __restrict__ out_d, int W,
+                                 int H, Gauss5 gs) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= W * H) return;
+  const float* in = blockIdx.z == 0 ? grey : depth;
+  float* out = blockIdx.z == 0 ? out_i : out_d;
+  const int x = p % W, y = p / W;
+  const float center = in[p];
+  if (center == 0) { out[p] = 0; return; }
+  const float e_d = 0.1f;
+  const float e2 = e_d * e_d * 2;
+  float sum = 0.0f, t = 0.0f;
+  for (int i = -2; i <= 2; ++i)
+    for (int j = -2; j <= 2; ++j) {
+      const int cx = imn(imx(x + i, 0), W - 1), cy = imn(imx(y + j, 0), H - 1);
+      const float cur = in[cx + cy * W];
+      if (cur > 0) {
+        const float mod = sq(cur - center);
+        const float factor = gs.g[i + 2] * gs.g[j + 2] * expf(-mod / e2);
+        t += factor * cur;
+        sum += factor;
+      }
+    }
+  out[p] = t / sum;
+}
+
+// halfSampleRobustImageKernel, preprocessing.cpp:161-196 (e_d = 0.3, r = 1).
+__global__ void half_sample_kernel(const float* __restrict__ in0, float* __restrict__ out0,
+                                   const float* __restrict__ in1, float* __restrict__ out1,
+                                   int iw, int ih, float e_d) {
+  const int ow = iw / 2, oh = ih / 2;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ow * oh) return;
+  const float* in = blockIdx.z == 0 ? in0 : in1;
+  float* out = blockIdx.z == 0 ? out0 : out1;
+  if (!in) return;
+  const int x = p % ow, y = p / ow;
+  const int cx = 2 * x, cy = 2 * y;
+  const float center = in[cx + cy * iw];
+  float sum = 0.0f, t = 0.0f;
+  for (int i = 0; i <= 1; ++i)
+    for (int j = 0; j <= 1; ++j) {
+      const int ux = imn(imx(cx + j, 0), 2 * ow - 1), uy = imn(imx(cy + i, 0), 2 * oh - 1);
+      const float cur = in[ux + uy * iw];
+      if (fabsf(cur - center) < e_d) { sum += 1.0f; t += cur; }
+    }
+  out[p] = t / sum;
+}
+
+// depth2vertexKernel, preprocessing.cpp:52-71.
+__global__ void depth2vertex_kernel(const float* __restrict__ depth, F3* __restrict__ vertex,
+                                    int w, int h, M4 invK) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w * h) return;
+  const int x = p % w, y = p / w;
+  const float d = depth[p];
+  vertex[p] = d > 0 ? d * rotate(invK, mk3((float)x, (float)y, 1.f)) : mk3(0.f);
+}
+
+// vertex2normalKernel<SDF, false> (preprocessing.h:39-81), gradientsKernel
+// (preprocessing.cpp:235-246, borders untouched) and calc_icp_cov
+// (tracking.cpp:845-871, sigma_xy = sigma_disp = 1, baseline 0.075).
+__global__ void normal_grad_cov_kernel(const F3* __restrict__ V, const float* __restrict__ I,
+                                       const float* __restrict__ D, F3* __restrict__ N,
+                                       float* __restrict__ GX, float* __restrict__ GY,
+                                       F3* __restrict__ COV, int w, int h, float focal) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w * h) return;
+  const int x = p % w, y = p / w;
+  const F3 left = V[imx(x - 1, 0) + w * y], right = V[imn(x + 1, w - 1) + w * y];
+  const F3 down = V[x + w * imx(y - 1, 0)], up = V[x + w * imn(y + 1, h - 1)];
+  if (left.z == 0 || right.z == 0 || up.z == 0 || down.z == 0) {
+    N[p].x = INVALIDF;  // the other components keep their previous values
+  } else {
+    N[p] = normalize(cross(up - down, right - left));
+  }
+  if (x >= 1 && y >= 1 && x < w - 1 && y < h - 1) {
+    GX[p] = (I[p + 1] - I[p - 1]) * 0.5f;
+    GY[p] = (I[p + w] - I[p - w]) * 0.5f;
+  }
+  const float d = D[p];
+  F3 c;
+  c.x = (d / focal) * 1.0f;
+  c.y = (d / focal) * 1.0f;
+  c.z = (d * d * 1.0f) / (focal * 0.075f);
+  c.x = c.x * c.x; c.y = c.y * c.y; c.z = c.z * c.z;
+  COV[p] = c;
+}
+
+struct SlotPtrs {
+  float* D[MAX_INSTANCES];
+  F3* V[MAX_INSTANCES];
+  const float* Din[MAX_INSTANCES];
+};
+
+// vertex2depth (preprocessing.cpp:292-309) of the model vertex map -- for an
+// object, its own map: the composite where label == object, 0 elsewhere
+// (rendering.cpp:153-178) -- seen from the reference camera (T_w_r for the
+// camera problem, T_w_c1 for an object; its inverse is kept in inv_T_w_r).
+__global__ void render_depth_kernel(const F3* __restrict__ vertex, const int* __restrict__ label,
+                                    const GNState* __restrict__ st, IdList slots, SlotPtrs sp,
+                                    int WH) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= WH) return;
+  const GNState& S = st[slots.v[blockIdx.y]];
+  F3 v = vertex[p];
+  if (S.kind == 1 && label[p] != S.label) v = mk3(0.f);
+  sp.D[blockIdx.y][p] = v.z > 0.0 ? xform(S.inv_T_w_r, v).z : 0.f;
+}
+
+__global__ void half_sample_slots_kernel(SlotPtrs sp, int iw, int ih, float e_d) {
+  const int ow = iw / 2, oh = ih / 2;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ow * oh) return;
+  const float* in = sp.Din[blockIdx.y];
+  float* out = sp.D[blockIdx.y];
+  const int x = p % ow, y = p / ow;
+  const int cx = 2 * x, cy = 2 * y;
+  const float center = in[cx + cy * iw];
+  float sum = 0.0f, t = 0.0f;
+  for (int i = 0; i <= 1; ++i)
+    for (int j = 0; j <= 1; ++j) {
+      const int ux = imn(imx(cx + j, 0), 2 * ow - 1), uy = imn(imx(cy + i, 0), 2 * oh - 1);
+      const float cur = in[ux + uy * iw];
+      if (fabsf(cur - center) < e_d) { sum += 1.0f; t += cur; }
+    }
+  out[p] = t / sum;
+}
+
+__global__ void depth2vertex_slots_kernel(SlotPtrs sp, int w, int h, M4 invK) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w * h) return;
+  const int x = p % w, y = p / w;
+  const float d = sp.D[blockIdx.y][p];
+  sp.V[blockIdx.y][p] = d > 0 ? d * rotate(invK, mk3((float)x, (float)y, 1.f)) : mk3(0.f);
+}
+
+// ------------------------------------------------------------------ GN setup
+__global__ void setup_camera_kernel(GNState* st, const float* __restrict__ Twc,
+                                    float* __restrict__ Twc_prev, F4 k) {
+  GNState& S = st[0];
+  M4 T;
+  memcpy(&T, Twc, 64);
+  memcpy(Twc_prev, Twc, 64);
+  for (int i = 0; i < 16; ++i) {
+    S.T[i] = (double)Twc[i];
+    S.prevT[i] = S.T[i];
+  }
+  S.kind = 0; S.label = 0; S.inst = 0; S.done = 0; S.ticket = 0; S.fallback = 0;
+  for (int l = 0; l < MAX_PYR; ++l) S.iters[l] = 0;
+  S.T_w_r = T;
+  S.inv_T_w_r = inverse(T);
+  S.view = mul(camera_matrix(k), S.inv_T_w_r);  // tracking.cpp:258
+  S.Tf = T;
+  S.invTf = inverse(T);
+}
+
+// trackEachObject setup, tracking.cpp:586-593: T_c1_o1 = inverse(T_w_c1) T_wo1,
+// T_c2_o2 = inverse(T_w_c2) T_wo1 with T_w_c2 the freshly tracked camera.
+__global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __restrict__ Twc2,
+                                     const float* __restrict__ Twc1, const float* __restrict__ Two,
+                                     const int* __restrict__ inst_label) {
+  const int t = threadIdx.x;
+  if (t >= slots.n) return;
+  const int s = slots.v[t];
+  GNState& S = st[s];
+  M4 T_w_c2, T_w_c1, T_wo1;
+  memcpy(&T_w_c2, Twc2, 64);
+  memcpy(&T_w_c1, Twc1, 64);
+  memcpy(&T_wo1, Two + 16 * s, 64);
+  S.kind = 1; S.inst = s; S.label = inst_label[s]; S.done = 0; S.ticket = 0; S.fallback = 0;
+  for (int l = 0; l < MAX_PYR; ++l) S.iters[l] = 0;
+  S.T_w_c2 = T_w_c2;
+  S.inv_T_w_r = inverse(T_w_c1);
+  S.T_c1_o1 = mul(S.inv_T_w_r, T_wo1);
+  S.inv_T_c1_o1 = inverse(S.T_c1_o1);
+  S.inv_T_w_o1 = inverse(T_wo1);
+  const M4 T0 = mul(inverse(T_w_c2), T_wo1);
+  for (int i = 0; i < 16; ++i) {
+    S.T[i] = (double)m_at(T0, i / 4, i % 4);
+    S.prevT[i] = S.T[i];
+  }
+  S.Tf = T0;
+  S.invTf = inverse(T0);
+}
+
+__global__ void level_start_kernel(GNState* st, IdList slots) {
+  const int t = threadIdx.x;
+  if (t >= slots.n) return;
+  GNState& S = st[slots.v[t]];
+  S.prev_err = INFINITY;
+  S.done = 0;
+  S.ticket = 0;
+}
+
+__global__ void finalize_camera_kernel(const GNState* st, float* __restrict__ Twc) {
+  const M4 T = to_m4f(st[0].T);
+  memcpy(Twc, &T, 64);
+}
+
+// volume_pose_ = T_w_c2 * T_c2_o2, tracking.cpp:695.
+__global__ void finalize_objects_kernel(const GNState* st, IdList slots, float* __restrict__ Two) {
+  const int t = threadIdx.x;
+  if (t >= slots.n) return;
+  const int s = slots.v[t];
+  const M4 P = mul(st[s].T_w_c2, to_m4f(st[s].T));
+  memcpy(Two + 16 * s, &P, 64);
+}
+
+// ------------------------------------------------------------------ GN step
+// One GN iteration's decision logic (tracking.cpp:287-335, objects :657-686):
+// cost test with step back, solve, convergence test, left-multiplied update.
+MF_HD void gn_step(GNState& S, const double* s, int level) {
+  const double err = s[0] / s[28];
+  if (S.kind == 1 && s[28] == 0) { S.done = 1; return; }
+  if (err > S.prev_err) {
+    for (int i = 0; i < 16; ++i) S.T[i] = S.prevT[i];
+    S.done = 1;
+  } else {
+    S.prev_err = err;
+    double A[6][6], b[6], x[6];
+    for (int i = 0; i < 6; ++i) b[i] = s[1 + i];
+    make_jtj(s + 7, A);
+    if (solve6(A, b, x)) S.fallback = 1;
+    double nx = 0;
+    for (int i = 0; i < 6; ++i) nx += x[i] * x[i];
+    if (sqrt(nx) < (double)1e-05f && sqrt(s[0] / s[28]) < 2e-3) {
+      S.done = 1;
+    } else {
+      double E[16], R[16];
+      se3_exp(x, E);
+      for (int i = 0; i < 16; ++i) S.prevT[i] = S.T[i];
+      mul4d(E, S.T, R);
+      for (int i = 0; i < 16; ++i) S.T[i] = R[i];
+    }
+  }
+  S.iters[level] += 1;
+  S.Tf = to_m4f(S.T);
+  S.invTf = inverse(S.Tf);
+}
+
+// ------------------------------------------------------------------ residuals
+struct GNArgs {
+  PyrPtrs pyr;
+  int cur;              // live set index
+  int W, H;             // full-resolution model maps
+  const F3* mvertex; const F3* mnormal; const int* mlabel;  // composite model maps
+  F3* rV[MAX_INSTANCES];   // rendered reference vertex of each slot at this level
+  GNState* st;
+  double* partials;
+  int max_tiles;
+  F4 kL;                // intrinsics at this level
+  F4 k0;                // full resolution
+  float inv_cov_rgb;
+  int robust;
+  int use_icp, use_rgb;
+  int device_step;      // 1: the last block runs gn_step; 0: only the sums
+};
+
+struct Row { int result; float e; float J[6]; };
+
+__device__ __forceinline__ float bil(const float* img, int w, float px, float py) {
+  const float fx0 = floorf(px), fy0 = floorf(py);
+  const int bx = (int)fx0, by = (int)fy0;
+  const float fx = px - fx0, fy = py - fy0;
+  return img[bx + by * w] * (1.f - fx) * (1.f - fy) + img[bx + 1 + by * w] * (1.f - fy) * fx +
+         img[bx + (by + 1) * w] * (1.f - fx) * fy + img[bx + 1 + (by + 1) * w] * fx * fy;
+}
+
+// Object model maps derived from the composite maps and labels.
+__device__ __forceinline__ void obj_maps(const GNArgs& a, int idx, int label, F3& v, F3& n) {
+  if (a.mlabel[idx] == label) { v = a.mvertex[idx]; n = a.mnormal[idx]; }
+  else { v = mk3(0.f); n = mk3(INVALIDF, 0.f, 0.f); }
+}
+__device__ __forceinline__ void bil_obj(const GNArgs& a, int label, float px, float py, F3& v,
+                                        F3& n) {
+  const float fx0 = floorf(px), fy0 = floorf(py);
+  const int bx = (int)fx0, by = (int)fy0;
+  const float fx = px - fx0, fy = py - fy0;
+  F3 v0, v1, v2, v3, n0, n1, n2, n3;
+  obj_maps(a, bx + by * a.W, label, v0, n0);
+  obj_maps(a, bx + 1 + by * a.W, label, v1, n1);
+  obj_maps(a, bx + (by + 1) * a.W, label, v2, n2);
+  obj_maps(a, bx + 1 + (by + 1) * a.W, label, v3, n3);
+  const float A = 1.f - fx, B = 1.f - fy;
+  v = mk3(v0.x * A * B + v1.x * B * fx + v2.x * A * fy + v3.x * fx * fy,
+          v0.y * A * B + v1.y * B * fx + v2.y * A * fy + v3.y * fx * fy,
+          v0.z * A * B + v1.z * B * fx + v2.z * A * fy + v3.z * fx * fy);
+  n = mk3(n0.x * A * B + n1.x * B * fx + n2.x * A * fy + n3.x * fx * fy,
+          n0.y * A * B + n1.y * B * fx + n2.y * A * fy + n3.y * fx * fy,
+          n0.z * A * B + n1.z * B * fx + n2.z * A * fy + n3.z * fx * fy);
+}
+
+// track_ICP_Kernel, tracking.cpp:923-1020.
+__device__ void icp_camera(const GNArgs& a, const GNState& S, int L, int p, Row& r) {
+  if (a.pyr.MASK[L][p]) { r.result = -6; return; }
+  const F3 n = a.pyr.N[L][p];
+  if (n.x == INVALIDF) { r.result = -1; return; }
+  const F3 pv = xform(S.Tf, a.pyr.V[a.cur][L][p]);
+  const F3 pp = xform(S.view, pv);
+  const float px = pp.x / pp.z, py = pp.y / pp.z;
+  if (px < 1 || px > (float)(unsigned)(a.W - 2) || py < 1 || py > (float)(unsigned)(a.H - 2) ||
+      isnan(px) || isnan(py)) { r.result = -2; return; }
+  const unsigned rx = (unsigned)px, ry = (unsigned)py;
+  const F3 rn = a.mnormal[rx + ry * a.W];
+  if (rn.x == INVALIDF) { r.result = -3; return; }
+  const F3 diff = a.mvertex[rx + ry * a.W] - pv;
+  const F3 pn = rotate(S.Tf, n);
+  if (length(diff) > 0.1f) { r.result = -4; return; }
+  if (dot(pn, rn) < 0.8f) { r.result = -5; return; }
+  r.result = 1;
+  const F3 P = a.pyr.COV[L][p];
+  const float sig = rn.x * rn.x * P.x + rn.y * rn.y * P.y + rn.z * rn.z * P.z;
+  const float ic = sqrtf((float)(1.0 / (double)sig));
+  r.e = ic * dot(rn, diff);
+  const F3 j1 = ic * cross(pv, rn);
+  r.J[0] = ic * rn.x; r.J[1] = ic * rn.y; r.J[2] = ic * rn.z;
+  r.J[3] = j1.x; r.J[4] = j1.y; r.J[5] = j1.z;
+}
+
+// track_Obj_ICP_Kernel, tracking.cpp:392-486 (object outlier mask is all zero).
+__device__ void icp_object(const GNArgs& a, const GNState& S, int L, int p, Row& r) {
+  const F3 cn = a.pyr.N[L][p];
+  if (cn.x == INVALIDF) { r.result = -1; return; }
+  const F3 cv = a.pyr.V[a.cur][L][p];
+  if (cv.x == 0 && cv.y == 0 && cv.z == 0) { r.result = -1; return; }
+  const F3 o2v = xform(S.invTf, cv);
+  const F3 c1v = xform(S.T_c1_o1, o2v);
+  const F3 pr = rotate(camera_matrix(a.k0), c1v);
+  const float px = pr.x / pr.z, py = pr.y / pr.z;
+  if (px < 1 || px > (float)(unsigned)(a.W - 2) || py < 1 || py > (float)(unsigned)(a.H - 2) ||
+      isnan(px) || isnan(py)) { r.result = -2; return; }
+  const F3 o2n = rotate(S.invTf, cn);
+  F3 wrv, wrn;
+  bil_obj(a, S.label, px, py, wrv, wrn);
+  if (wrn.x == INVALIDF) { r.result = -3; return; }
+  const F3 o1rv = xform(S.inv_T_w_o1, wrv);
+  const F3 o1rn = rotate(S.inv_T_w_o1, wrn);
+  const F3 diff = o2v - o1rv;
+  const float residual = dot(o1rn, diff);
+  if (length(diff) > 0.1f) { r.result = -4; return; }
+  if (dot(o2n, o1rn) < 0.8f) { r.result = -5; return; }
+  const F3 P = a.pyr.COV[L][p];
+  const float sig = o1rn.x * o1rn.x * P.x + o1rn.y * o1rn.y * P.y + o1rn.z * o1rn.z * P.z;
+  const float ic = sqrtf((float)(1.0 / (double)sig));
+  r.e = ic * residual;
+  const F3 Jt = rotate(S.Tf, o1rn);
+  const float c0 = -1.0f * ic * -1.0f;
+  const F3 j1 = ic * cross(cv, Jt);
+  r.J[0] = c0 * Jt.x; r.J[1] = c0 * Jt.y; r.J[2] = c0 * Jt.z;
+  r.J[3] = j1.x; r.J[4] = j1.y; r.J[5] = j1.z;
+  r.result = 1;
+}
+
+// trackRGB (tracking.cpp:1023-1111, warp :1114-1121, rgb_jacobian :1123-1150)
+// and track_obj_RGB_kernel (:491-578, obj_warp :359-367, obj_rgb_jacobian
+// :1152-1178).  The photometric outlier mask of the reference is all zero.
+__device__ void rgb_row(const GNArgs& a, const GNState& S, const F3* rV, int L, int p, int w,
+                        int h, Row& r) {
+  const F3 rv = rV[p];
+  const F3 rl = a.pyr.V[1 - a.cur][L][p];
+  if (rv.z <= 0.f || rv.z == INVALIDF) { r.result = -1; return; }
+  if (length(rv - rl) > 0.1f && rl.z > 0.f) { r.result = -3; return; }
+  const M4 KL = camera_matrix(a.kL);
+  F3 lv, wv;
+  if (S.kind == 0) {
+    wv = xform(S.T_w_r, rv);
+    lv = xform(S.invTf, wv);
+  } else {
+    const F3 o1v = xform(S.inv_T_c1_o1, rv);
+    lv = xform(S.Tf, o1v);
+  }
+  const F3 pr = rotate(KL, lv);
+  const float px = pr.x / pr.z, py = pr.y / pr.z;
+  if (px < 1 || px > (float)(unsigned)(w - 2) || py < 1 || py > (float)(unsigned)(h - 2) ||
+      isnan(px) || isnan(py)) { r.result = -2; return; }
+  const float residual = a.pyr.I[1 - a.cur][L][p] - bil(a.pyr.I[a.cur][L], w, px, py);
+  const float gx = bil(a.pyr.GX[L], w, px, py), gy = bil(a.pyr.GY[L], w, px, py);
+  const float fx = KL.r[0].x, fy = KL.r[1].y;
+  F3 Jt = (1.f / lv.z) * mk3(gx * fx, gy * fy, -(gx * lv.x * fx + gy * lv.y * fy) / lv.z);
+  F3 Jr;
+  if (S.kind == 0) {
+    Jt = -1.f * rotate(S.Tf, Jt);  // rotate(Jtrans, transpose(T_w_l))
+    Jr = cross(wv, Jt);
+  } else {
+    Jr = cross(lv, Jt);
+  }
+  const float ic = a.inv_cov_rgb;
+  r.J[0] = ic * Jt.x; r.J[1] = ic * Jt.y; r.J[2] = ic * Jt.z;
+  r.J[3] = ic * Jr.x; r.J[4] = ic * Jr.y; r.J[5] = ic * Jr.z;
+  r.e = ic * residual;
+  r.result = 1;
+}
+
+// calc_robust_weight / calc_robust_residual, tracking.cpp:1474-1532: evaluated
+// in double, used as float.
+__device__ __forceinline__ void robust(float e, int kind, float& w, float& loss) {
+  const double r = e;
+  double wd = 1.0, l;
+  switch (kind) {
+    case 1: {
+      const double a = fabs(r);
+      if (a <= 1.345) { wd = 1.0; l = 0.5 * r * r; }
+      else { wd = 1.345 / a; l = 1.345 * (a - 0.5 * 1.345); }
+      break;
+    }
+    case 2: {
+      const double b = 4.6851, a = fabs(r);
+      if (a <= b) {
+        const double u = 1.0 - r * r / (b * b);
+        wd = u * u;
+        const double v = 1.0 - (r / b) * (r / b);
+        l = b * b / 6.0 * (1.0 - v * v * v);
+      } else { wd = 0; l = b * b / 6.0; }
+      break;
+    }
+    case 3: {
+      const double q = (r / 2.3849) * (r / 2.3849);
+      wd = 1 / (1 + q);
+      l = 0.5 * 2.3849 * 2.3849 * log(1.0 + q);
+      break;
+    }
+    default: l = 0.5 * r * r;
+  }
+  w = (float)wd;
+  loss = (float)l;
+}
+
+struct Kahan {
+  float s, c;
+  __device__ __forceinline__ void add(float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
+
+__device__ __forceinline__ void accumulate(Kahan* acc, int* cnt, const Row& r, int kind) {
+  if (r.result < 1) {
+    cnt[0] += r.result == -4;
+    cnt[1] += r.result == -5;
+    cnt[2] += r.result > -4;
+    return;
+  }
+  float w, loss;
+  robust(r.e, kind, w, loss);
+  acc[0].add(loss);
+  const float we = w * r.e;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) acc[1 + i].add(we * r.J[i]);
+  int q = 7;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    const float wj = w * r.J[i];
+#pragma unroll
+    for (int j = i; j < 6; ++j) acc[q++].add(wj * r.J[j]);
+  }
+  acc[28].add(1.f);
+}
+
+__global__ void __launch_bounds__(GN_THREADS)
+gn_iter_kernel(GNArgs a, IdList slots, int L) {
+  const int s = slots.v[blockIdx.y];
+  GNState& S = a.st[s];
+  if (S.done) return;
+  const int w = a.pyr.w[L], h = a.pyr.h[L];
+  const int n = w * h;
+  Kahan acc[29];
+#pragma unroll
+  for (int i = 0; i < 29; ++i) { acc[i].s = 0.f; acc[i].c = 0.f; }
+  int cnt[3] = {0, 0, 0};
+  const F3* rV = a.rV[s];
+  for (int k = 0; k < GN_PIX; ++k) {
+    const int p = blockIdx.x * GN_TILE + k * GN_THREADS + threadIdx.x;
+    if (p >= n) break;
+    Row r;
+    if (a.use_icp) {
+      r.result = 0;
+      if (S.kind == 0) icp_camera(a, S, L, p, r);
+      else icp_object(a, S, L, p, r);
+      accumulate(acc, cnt, r, a.robust);
+    }
+    if (a.use_rgb) {
+      r.result = 0;
+      rgb_row(a, S, rV, L, p, w, h, r);
+      accumulate(acc, cnt, r, a.robust);
+    }
+  }
+  // FP64 from the warp level up
+  __shared__ double sh[GN_THREADS / 32][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = 0; i < 32; ++i) {
+    double v = i < 29 ? (double)acc[i].s - (double)acc[i].c : (double)cnt[i - 29];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[warp][i] = v;
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x < 32) {
+    double v = 0;
+    for (int wi = 0; wi < GN_THREADS / 32; ++wi) v += sh[wi][threadIdx.x];
+    a.partials[((size_t)s * a.max_tiles + blockIdx.x) * 32 + threadIdx.x] = v;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int t = atomicAdd(&S.ticket, 1);
+    last = (t == (int)gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ double tot[32];
+  if (threadIdx.x < 32) {
+    double v = 0;
+    for (int b = 0; b < (int)gridDim.x; ++b)
+      v += __ldcg(&a.partials[((size_t)s * a.max_tiles + b) * 32 + threadIdx.x]);
+    tot[threadIdx.x] = v;
+    S.sums[L][threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    S.ticket = 0;
+    if (a.device_step) gn_step(S, tot, L);
+  }
+}
+
+// ------------------------------------------------------------------ host side
+static int div_up(long long a, int b) { return (int)((a + b - 1) / b); }
+
+template <typename T>
+static int talloc(Context* ctx, T** p, size_t n) {
+  if (cudaMalloc((void**)p, sizeof(T) * (n ? n : 1)) != cudaSuccess) {
+    ctx->last_error = "tracking buffer allocation failed";
+    return MF_E_CUDA;
+  }
+  ctx->track->allocs.push_back(*p);
+  MF_CUDA(cudaMemsetAsync(*p, 0, sizeof(T) * (n ? n : 1), ctx->stream));
+  return MF_OK;
+}
+
+int track_init(Context* ctx) {
+  if (ctx->track) return MF_OK;
+  TrackState* ts = new TrackState;
+  ctx->track = ts;
+  ts->levels = std::max(1, std::min(ctx->cfg.pyramid_levels, MAX_PYR));
+  PyrPtrs& P = ts->pyr;
+  for (int l = 0; l < ts->levels; ++l) {
+    P.w[l] = ctx->W >> l;
+    P.h[l] = ctx->H >> l;
+    const size_t n = (size_t)P.w[l] * P.h[l];
+    int rc = 0;
+    rc |= talloc(ctx, &P.D[l], n);
+    rc |= talloc(ctx, &P.I[0][l], n);
+    rc |= talloc(ctx, &P.I[1][l], n);
+    rc |= talloc(ctx, &P.V[0][l], n);
+    rc |= talloc(ctx, &P.V[1][l], n);
+    rc |= talloc(ctx, &P.N[l], n);
+    rc |= talloc(ctx, &P.GX[l], n);
+    rc |= talloc(ctx, &P.GY[l], n);
+    rc |= talloc(ctx, &P.COV[l], n);
+    rc |= talloc(ctx, &P.MASK[l], n);
+    for (int s = 0; s < ctx->cfg.max_instances; ++s) {
+      rc |= talloc(ctx, &ts->rD[s][l], n);
+      rc |= talloc(ctx, &ts->rV[s][l], n);
+    }
+    if (rc) return MF_E_CUDA;
+  }
+  ts->max_tiles = div_up((long long)ctx->W * ctx->H, GN_TILE);
+  if (talloc(ctx, &ts->d_state, MAX_INSTANCES)) return MF_E_CUDA;
+  if (talloc(ctx, &ts->d_partials, (size_t)MAX_INSTANCES * ts->max_tiles * 32)) return MF_E_CUDA;
+  if (talloc(ctx, &ts->d_Twc_prev, 16)) return MF_E_CUDA;
+  if (talloc(ctx, &ts->d_mask0, (size_t)ctx->W * ctx->H)) return MF_E_CUDA;
+  // Tracking::Tracking, tracking.cpp:77-84: gaussian[i] = expf(-(x*x) / (2 delta^2)),
+  // x = i - 2, delta = 4 (computed on the host exactly as the reference does).
+  for (int i = 0; i < 5; ++i) {
+    const int x = i - 2;
+    ts->gaussian[i] = expf(-(x * x) / (2 * 4.0f * 4.0f));
+  }
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+void track_free(Context* ctx) {
+  if (!ctx->track) return;
+  for (void* p : ctx->track->allocs) cudaFree(p);
+  delete ctx->track;
+  ctx->track = nullptr;
+}
+
+static F4 kdiv(const mf_config& c, int l) {
+  const float d = float(1 << l);
+  return F4{c.k[0] / d, c.k[1] / d, c.k[2] / d, c.k[3] / d};
+}
+
+// Tracking::set_params_frame, tracking.cpp:142-171 (buildPyramid :776-818).
+int track_preprocess(Context* ctx) {
+  if (int rc = track_init(ctx)) return rc;
+  TrackState& T = *ctx->track;
+  PyrPtrs& P = T.pyr;
+  const int W = ctx->W, H = ctx->H;
+  Gauss5 g;
+  for (int i = 0; i < 5; ++i) g.g[i] = T.gaussian[i];
+  bilateral_kernel<<<dim3(div_up((long long)W * H, 256), 1, 2), 256, 0, ctx->stream>>>(
+      ctx->d_grey, ctx->d_depth, P.I[T.cur][0], P.D[0], W, H, g);
+  MF_CUDA(cudaGetLastError());
+  const float e_d = 0.1f * 3;
+  for (int l = 1; l < T.levels; ++l) {
+    half_sample_kernel<<<dim3(div_up((long long)P.w[l] * P.h[l], 256), 1, 2), 256, 0, ctx->stream>>>(
+        P.D[l - 1], P.D[l], P.I[T.cur][l - 1], P.I[T.cur][l], P.w[l - 1], P.h[l - 1], e_d);
+    MF_CUDA(cudaGetLastError());
+  }
+  for (int l = 0; l < T.levels; ++l) {
+    const F4 kl = kdiv(ctx->cfg, l);
+    const int n = P.w[l] * P.h[l];
+    depth2vertex_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(P.D[l], P.V[T.cur][l], P.w[l],
+                                                                  P.h[l], inverse_camera_matrix(kl));
+    normal_grad_cov_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(
+        P.V[T.cur][l], P.I[T.cur][l], P.D[l], P.N[l], P.GX[l], P.GY[l], P.COV[l], P.w[l], P.h[l],
+        kl.x);
+    MF_CUDA(cudaGetLastError());
+    MF_CUDA(cudaMemsetAsync(P.MASK[l], 0, n, ctx->stream));
+  }
+  return MF_OK;
+}
+
+// Tracking::setRefImgFromCurr, tracking.cpp:1400-1413: the live intensity and
+// vertex pyramids become the reference (a buffer swap instead of a copy).
+int track_set_ref(Context* ctx) {
+  if (int rc = track_init(ctx)) return rc;
+  ctx->track->cur = 1 - ctx->track->cur;
+  ctx->track->have_ref = true;
+  return MF_OK;
+}
+
+// The camera's ICP outlier mask, trackLiveFrame(..., mask): cv::resize to each
+// level: 2x (INTER_AREA) keeps any nonzero of a 2x2 cell, 4x (INTER_LINEAR)
+// samples taps 4x+1 and 4x+2 per axis.
+__global__ void mask_pyramid_kernel(const uint8_t* __restrict__ m0, uint8_t* __restrict__ out,
+                                    int W, int w, int h, int l) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= w * h) return;
+  const int x = p % w, y = p / w;
+  uint8_t v;
+  if (l == 0) {
+    v = m0[p];
+  } else {
+    const int o = l == 1 ? 0 : (1 << (l - 1)) - 1, s = 1 << l;
+    v = 0;
+    for (int dy = 0; dy < 2; ++dy)
+      for (int dx = 0; dx < 2; ++dx) v |= m0[(s * x + o + dx) + (s * y + o + dy) * W];
+  }
+  out[p] = v ? 1 : 0;
+}
+
+// Mask of the pixels whose composite label belongs to a moving object
+// (the dynamic-object mask of Kfusion::tracking, kfusion.cpp:358-393).
+__global__ void label_mask_kernel(const int* __restrict__ label, uint32_t moving,
+                                  uint8_t* __restrict__ out, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int l = label[p];
+  out[p] = (l >= 0 && l < 32 && ((moving >> l) & 1u)) ? 255 : 0;
+}
+
+int track_set_mask(Context* ctx, const uint8_t* d_mask0) {
+  TrackState& T = *ctx->track;
+  PyrPtrs& P = T.pyr;
+  for (int l = 0; l < T.levels; ++l) {
+    const int n = P.w[l] * P.h[l];
+    mask_pyramid_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(d_mask0, P.MASK[l], ctx->W,
+                                                                  P.w[l], P.h[l], l);
+    MF_CUDA(cudaGetLastError());
+  }
+  return MF_OK;
+}
+
+static int render_reference(Context* ctx, const IdList& slots) {
+  TrackState& T = *ctx->track;
+  PyrPtrs& P = T.pyr;
+  const int WH = ctx->W * ctx->H;
+  SlotPtrs sp{};
+  for (int i = 0; i < slots.n; ++i) sp.D[i] = T.rD[slots.v[i]][0];
+  render_depth_kernel<<<dim3(div_up(WH, 256), slots.n), 256, 0, ctx->stream>>>(
+      ctx->d_vertex, ctx->d_label, T.d_state, slots, sp, WH);
+  MF_CUDA(cudaGetLastError());
+  for (int l = 0; l < T.levels; ++l) {
+    SlotPtrs q{};
+    for (int i = 0; i < slots.n; ++i) {
+      q.D[i] = T.rD[slots.v[i]][l];
+      q.V[i] = T.rV[slots.v[i]][l];
+      q.Din[i] = l > 0 ? T.rD[slots.v[i]][l - 1] : nullptr;
+    }
+    const int n = P.w[l] * P.h[l];
+    if (l > 0) {
+      half_sample_slots_kernel<<<dim3(div_up(n, 256), slots.n), 256, 0, ctx->stream>>>(
+          q, P.w[l - 1], P.h[l - 1], 0.1f * 3);
+      MF_CUDA(cudaGetLastError());
+    }
+    depth2vertex_slots_kernel<<<dim3(div_up(n, 256), slots.n), 256, 0, ctx->stream>>>(
+        q, P.w[l], P.h[l], inverse_camera_matrix(kdiv(ctx->cfg, l)));
+    MF_CUDA(cudaGetLastError());
+  }
+  return MF_OK;
+}
+
+static const void* sums_ptr(const TrackState& T, int slot, int L) {
+  return (const char*)(T.d_state + slot) + offsetof(GNState, sums) + sizeof(double) * 32 * L;
+}
+
+static GNArgs make_args(Context* ctx, int L, int device_step) {
+  TrackState& T = *ctx->track;
+  GNArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.pyr = T.pyr;
+  a.cur = T.cur;
+  a.W = ctx->W; a.H = ctx->H;
+  a.mvertex = ctx->d_vertex; a.mnormal = ctx->d_normal; a.mlabel = ctx->d_label;
+  for (int s = 0; s < ctx->cfg.max_instances; ++s) a.rV[s] = T.rV[s][L];
+  a.st = T.d_state;
+  a.partials = T.d_partials;
+  a.max_tiles = T.max_tiles;
+  a.kL = kdiv(ctx->cfg, L);
+  a.k0 = kdiv(ctx->cfg, 0);
+  // obtainErrorParameters (TUM branch, tracking.cpp:766-772) keeps sigma_bright
+  // in a float member; trackRGB uses 1.0 / sigma_bright (double) as a float.
+  const float sigma_bright = (float)(sqrtf(100.0f) / 255.0);
+  a.inv_cov_rgb = (float)(1.0 / (double)sigma_bright);
+  a.robust = ctx->cfg.robust_kernel;
+  a.use_icp = ctx->cfg.use_icp;
+  a.use_rgb = ctx->cfg.use_rgb;
+  a.device_step = device_step;
+  return a;
+}
+
+// Coarse-to-fine GN of every problem in `slots`, all on the device
+// (trackLiveFrame :240-335 / trackEachObject :629-694).
+static int gn_device(Context* ctx, const IdList& slots) {
+  TrackState& T = *ctx->track;
+  for (int L = T.levels - 1; L >= 0; --L) {
+    level_start_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, slots);
+    const GNArgs a = make_args(ctx, L, 1);
+    const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_TILE);
+    for (int it = 0; it < ctx->cfg.gn_iterations[L]; ++it)
+      gn_iter_kernel<<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
+    MF_CUDA(cudaGetLastError());
+  }
+  return MF_OK;
+}
+
+// Host-driven GN of one problem: the sums come back to the host every
+// iteration and the step runs there (the reference's structure on a GPU).
+static int gn_host(Context* ctx, int slot) {
+  TrackState& T = *ctx->track;
+  IdList one;
+  one.n = 1;
+  one.v[0] = slot;
+  GNState S;
+  MF_CUDA(cudaMemcpyAsync(&S, T.d_state + slot, sizeof(GNState), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int L = T.levels - 1; L >= 0; --L) {
+    S.prev_err = INFINITY;
+    S.done = 0;
+    S.ticket = 0;
+    const GNArgs a = make_args(ctx, L, 0);
+    const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_TILE);
+    for (int it = 0; it < ctx->cfg.gn_iterations[L] && !S.done; ++it) {
+      MF_CUDA(cudaMemcpyAsync(T.d_state + slot, &S, sizeof(GNState), cudaMemcpyHostToDevice,
+                              ctx->stream));
+      gn_iter_kernel<<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
+      MF_CUDA(cudaGetLastError());
+      MF_CUDA(cudaMemcpyAsync(S.sums[L], sums_ptr(T, slot, L), sizeof(double) * 32,
+                              cudaMemcpyDeviceToHost, ctx->stream));
+      MF_CUDA(cudaStreamSynchronize(ctx->stream));
+      gn_step(S, S.sums[L], L);
+    }
+  }
+  MF_CUDA(cudaMemcpyAsync(T.d_state + slot, &S, sizeof(GNState), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  return MF_OK;
+}
+
+// Tracking::trackLiveFrame with the current model maps; the camera pose is read
+// from and written back to the device.  `moving` (bit per label) selects the
+// pixels excluded from ICP (trackLiveFrame(..., mask)); 0 = no mask.
+int track_camera(Context* ctx, uint32_t moving) {
+  if (int rc = track_init(ctx)) return rc;
+  TrackState& T = *ctx->track;
+  const mf_config& c = ctx->cfg;
+  setup_camera_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc, T.d_Twc_prev,
+                                                F4{c.k[0], c.k[1], c.k[2], c.k[3]});
+  MF_CUDA(cudaGetLastError());
+  if (moving) {
+    label_mask_kernel<<<div_up((long long)ctx->W * ctx->H, 256), 256, 0, ctx->stream>>>(
+        ctx->d_label, moving, T.d_mask0, ctx->W * ctx->H);
+    if (int rc = track_set_mask(ctx, T.d_mask0)) return rc;
+  }
+  IdList cam;
+  cam.n = 1;
+  cam.v[0] = 0;
+  if (int rc = render_reference(ctx, cam)) return rc;
+  if (c.batched) {
+    if (int rc = gn_device(ctx, cam)) return rc;
+  } else {
+    if (int rc = gn_host(ctx, 0)) return rc;
+  }
+  finalize_camera_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Tracking::trackEachObject for every id (instance ids >= 1), against the
+// model maps of the last raycast, from the previous camera pose (saved by
+// track_camera) to the current one.
+int track_objects(Context* ctx, const IdList& ids) {
+  if (int rc = track_init(ctx)) return rc;
+  if (ids.n == 0) return MF_OK;
+  TrackState& T = *ctx->track;
+  setup_objects_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, ids, ctx->d_Twc, T.d_Twc_prev,
+                                                  ctx->d_Two, ctx->d_inst_label);
+  MF_CUDA(cudaGetLastError());
+  if (int rc = render_reference(ctx, ids)) return rc;
+  if (ctx->cfg.batched) {
+    if (int rc = gn_device(ctx, ids)) return rc;
+  } else {
+    for (int i = 0; i < ids.n; ++i)
+      if (int rc = gn_host(ctx, ids.v[i])) return rc;
+  }
+  finalize_objects_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, ids, ctx->d_Two);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+void track_save_prev_camera(Context* ctx) {
+  cudaMemcpyAsync(ctx->track->d_Twc_prev, ctx->d_Twc, 64, cudaMemcpyDeviceToDevice, ctx->stream);
+}
+
+int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64) {
+  if (!ctx->track) return MF_E_STATE;
+  GNState S;
+  MF_CUDA(cudaMemcpyAsync(&S, ctx->track->d_state + slot, sizeof(GNState),
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int l = 0; l < MAX_PYR; ++l) {
+    if (iters) iters[l] = S.iters[l];
+    if (sums) for (int i = 0; i < 32; ++i) sums[32 * l + i] = S.sums[l][i];
+  }
+  if (T64) for (int i = 0; i < 16; ++i) T64[i] = S.T[i];
+  return S.fallback ? 1 : 0;
+}
+
+// One evaluation of the normal equations at a given level for one problem at
+// its current pose, without a step (parity checks of residuals + reduction).
+int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums) {
+  if (!ctx->track) return MF_E_STATE;
+  TrackState& T = *ctx->track;
+  GNState S;
+  MF_CUDA(cudaMemcpyAsync(&S, T.d_state + slot, sizeof(GNState), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (pose16) {
+    std::memcpy(&S.Tf, pose16, 64);
+    S.invTf = inverse(S.Tf);
+    for (int i = 0; i < 16; ++i) S.T[i] = pose16[i];
+  }
+  S.done = 0;
+  S.ticket = 0;
+  MF_CUDA(cudaMemcpyAsync(T.d_state + slot, &S, sizeof(GNState), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  IdList one;
+  one.n = 1;
+  one.v[0] = slot;
+  const GNArgs a = make_args(ctx, L, 0);
+  const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_TILE);
+  gn_iter_kernel<<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
+  MF_CUDA(cudaGetLastError());
+  MF_CUDA(cudaMemcpyAsync(sums, sums_ptr(T, slot, L), sizeof(double) * 32,
+                          cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int track_download_level(Context* ctx, int L, int which, float* out) {
+  if (!ctx->track) return MF_E_STATE;
+  TrackState& T = *ctx->track;
+  const PyrPtrs& P = T.pyr;
+  const size_t n = (size_t)P.w[L] * P.h[L];
+  const void* src = nullptr;
+  size_t bytes = 4 * n;
+  switch (which) {
+    case 0: src = P.D[L]; break;
+    case 1: src = P.I[T.cur][L]; break;
+    case 2: src = P.V[T.cur][L]; bytes = 12 * n; break;
+    case 3: src = P.N[L]; bytes = 12 * n; break;
+    case 4: src = P.GX[L]; break;
+    case 5: src = P.GY[L]; break;
+    case 6: src = P.COV[L]; bytes = 12 * n; break;
+    case 7: src = T.rV[0][L]; bytes = 12 * n; break;
+    default: return MF_E_ARG;
+  }
+  MF_CUDA(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+}  // namespace mf

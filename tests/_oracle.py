@@ -192,3 +192,92 @@ def reference():
     if "ref" not in _cache:
         _cache["ref"] = Impl(REF_SO, "ref_")
     return _cache["ref"]
+
+
+class Tracker:
+    """The tracking oracle (fp64=True: all-FP64; False: the reference's FP32 order)."""
+
+    def __init__(self, W, H, k, iters=(10, 5, 4), robust=1, use_icp=True, use_rgb=True,
+                 fp64=True):
+        lib = oracle().lib
+        self.lib = lib
+        self.W, self.H = W, H
+        I32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        U8 = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+        F64 = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        lib.ot_create.restype = P
+        lib.ot_create.argtypes = [C.c_int, C.c_int, FP, C.c_int, I32, C.c_int, C.c_int, C.c_int,
+                                  C.c_int]
+        lib.ot_destroy.argtypes = [P]
+        lib.ot_set_frame.argtypes = [P, U8, FP]
+        lib.ot_set_ref_from_current.argtypes = [P]
+        lib.ot_set_outlier_mask.argtypes = [P, U8]
+        lib.ot_track_camera.argtypes = [P, FP, FP, FP, FP, FP, C.c_void_p]
+        lib.ot_track_object.argtypes = [P, FP, FP, FP, FP, FP, I32, C.c_int, FP, C.c_void_p]
+        lib.ot_camera_sums.argtypes = [P, C.c_int, FP, FP, FP, FP, F64]
+        lib.ot_object_sums.argtypes = [P, C.c_int, FP, FP, FP, FP, FP, I32, C.c_int, F64]
+        lib.ot_last_sums.argtypes = [P, C.c_int, F64]
+        lib.ot_last_iterations.restype = C.c_int
+        lib.ot_last_iterations.argtypes = [P, C.c_int]
+        lib.ot_get_level.restype = C.c_int
+        lib.ot_get_level.argtypes = [P, C.c_int, C.c_int, FP]
+        it = np.zeros(4, np.int32)
+        it[:len(iters)] = iters
+        self.levels = len(iters)
+        self.h = lib.ot_create(W, H, _f32(k), len(iters), it, robust, int(use_icp), int(use_rgb),
+                               int(fp64))
+
+    def __del__(self):
+        try:
+            self.lib.ot_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_frame(self, rgb, depth):
+        self.lib.ot_set_frame(self.h, np.ascontiguousarray(rgb, np.uint8), _f32(depth))
+
+    def set_ref(self):
+        self.lib.ot_set_ref_from_current(self.h)
+
+    def set_mask(self, mask):
+        self.lib.ot_set_outlier_mask(self.h, np.ascontiguousarray(mask, np.uint8))
+
+    def track_camera(self, T_in, T_w_r, vertex, normal):
+        out = np.zeros(16, np.float32)
+        out64 = np.zeros(16, np.float64)
+        self.lib.ot_track_camera(self.h, _f32(T_in).reshape(16), _f32(T_w_r).reshape(16),
+                                 _f32(vertex), _f32(normal), out, out64.ctypes.data)
+        return out64.reshape(4, 4)
+
+    def track_object(self, T_wo1, T_w_c2, T_w_c1, vertex, normal, labels, label):
+        out = np.zeros(16, np.float32)
+        out64 = np.zeros(16, np.float64)
+        self.lib.ot_track_object(self.h, _f32(T_wo1).reshape(16), _f32(T_w_c2).reshape(16),
+                                 _f32(T_w_c1).reshape(16), _f32(vertex), _f32(normal),
+                                 np.ascontiguousarray(labels, np.int32), int(label), out,
+                                 out64.ctypes.data)
+        return out64.reshape(4, 4)
+
+    def camera_sums(self, level, T_w_l, T_w_r, vertex, normal):
+        out = np.zeros(32, np.float64)
+        self.lib.ot_camera_sums(self.h, level, _f32(T_w_l).reshape(16), _f32(T_w_r).reshape(16),
+                                _f32(vertex), _f32(normal), out)
+        return out
+
+    def object_sums(self, level, T_c2_o2, T_wo1, T_w_c1, vertex, normal, labels, label):
+        out = np.zeros(32, np.float64)
+        self.lib.ot_object_sums(self.h, level, _f32(T_c2_o2).reshape(16), _f32(T_wo1).reshape(16),
+                                _f32(T_w_c1).reshape(16), _f32(vertex), _f32(normal),
+                                np.ascontiguousarray(labels, np.int32), int(label), out)
+        return out
+
+    def iterations(self):
+        return [self.lib.ot_last_iterations(self.h, l) for l in range(self.levels)]
+
+    def level(self, l, which):
+        n = (self.W >> l) * (self.H >> l)
+        out = np.zeros(n * 3, np.float32)
+        self.lib.ot_get_level(self.h, l, which, out)
+        if which in (2, 3, 6, 7):
+            return out.reshape(self.H >> l, self.W >> l, 3)
+        return out[:n].reshape(self.H >> l, self.W >> l)
