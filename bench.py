@@ -1,0 +1,409 @@
+"""Frames/s of the MID-Fusion per-frame dense hot path on B200.
+
+One step = one frame of the pipeline (mf_process_frame): preprocessing, camera
++ object Gauss-Newton tracking, allocation + integration of every instance,
+multi-instance raycast.  Workload: 640x480 frames, background octree 512^3 @
+1 cm plus three rigid objects (sphere r 0.12 m, box 0.2x0.1x0.3 m, cylinder
+r 0.06 m h 0.25 m) with 256^3 @ 2 mm octrees, each object moving with its own
+seeded twist; seeded synthetic frames stand in for the reference's datasets.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value: batched frames/s with the frames already in device memory (device
+time, CUDA events on the library's stream, L2 flushed between frames);
+plain: the one-instance-per-launch path with host-driven GN on the same
+frames; e2e: the batched path through the C ABI from pinned host buffers,
+host->device copies and the pose read-back inside the timed region.
+Multi-GPU runs one independent sequence per rank (weak scaling, no collective
+on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H = 640, 480
+METRIC = "640x480 frames/s, K objects: batched vs plain GPU at <=1e-5 pose err; HBM GB/s"
+WORKLOAD = "640x480 RGB-D, background 512^3@1cm + 3 objects 256^3@2mm (sphere, box, cylinder)"
+
+
+def scene_for(rank, n_frames):
+    from mid_fusion_b200.scene import make_scene
+    return make_scene("multi", W, H, n_frames=n_frames, seed=11 + rank, n_objects=3,
+                      bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512)
+
+
+def _render(args):
+    rank, n_frames, f = args
+    s = scene_for(rank, n_frames)
+    d, rgb, lab = s.render(f)
+    return f, d, rgb, lab
+
+
+def render_frames(rank, n_frames, workers):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(workers) as pool:
+        out = pool.map(_render, [(rank, n_frames, f) for f in range(n_frames)])
+    out.sort(key=lambda t: t[0])
+    return [o[1:] for o in out]
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.idx, self.samples, self.proc = gpu_index, [], None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=2)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(s[1]) for s in self.samples if len(s) > 2 and s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if len(s) > 2 and s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for s in self.samples:
+            for n, v in zip(names, s[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from mid_fusion_b200 import build
+    from mid_fusion_b200.capi import Context
+
+    n_frames = 1 + args.warmup + args.steps
+    frames = render_frames(rank, n_frames, args.workers)  # before the first CUDA call
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    build.build()
+    s = scene_for(rank, n_frames)
+
+    def make_ctx(batched):
+        ctx = Context(W, H, k=s.k, pool_blocks=args.pool_blocks, batched=batched, robust="huber")
+        for inst, T in zip(s.instances, s.volume_poses(0)):
+            ctx.add_instance(inst.size, inst.dim, T, inst.label)
+        ctx.set_camera_pose(s.cam_poses[0])
+        return ctx
+
+    # device-resident inputs
+    d_depth = [torch.from_numpy(f[0]).to(dev) for f in frames]
+    d_rgb = [torch.from_numpy(np.ascontiguousarray(f[1])).to(dev) for f in frames]
+    d_lab = [torch.from_numpy(f[2].astype(np.int16)).to(dev) for f in frames]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def run(batched, record_poses=True):
+        ctx = make_ctx(batched)
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+        lib = ctx.lib
+        times, poses = [], []
+        for f in range(n_frames):
+            flush.fill_(f & 0xff)
+            torch.cuda.synchronize(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.mf_process_frame_device(ctx.h, ctx_ptr(d_depth[f]), ctx_ptr(d_rgb[f]),
+                                             ctx_ptr(d_lab[f]))
+            if rc != 0:
+                raise RuntimeError(f"mf_process_frame_device failed: {rc}")
+            e1.record(stream)
+            e1.synchronize()
+            if f >= 1 + args.warmup:
+                times.append(e0.elapsed_time(e1) * 1e-3)
+            if record_poses:
+                poses.append(ctx_poses(ctx))
+        st = ctx.status()
+        if batched:
+            stats.update(ctx.frame_stats())
+        return ctx, times, poses, st
+
+    def ctx_ptr(t):
+        import ctypes
+        return ctypes.c_void_p(t.data_ptr())
+
+    def ctx_poses(ctx):
+        import ctypes
+        Tc = np.zeros(16, np.float32)
+        To = np.zeros(16 * len(s.instances), np.float32)
+        ctx.lib.mf_get_poses(ctx.h, Tc.ctypes.data_as(ctypes.c_void_p),
+                             To.ctypes.data_as(ctypes.c_void_p))
+        return Tc.reshape(4, 4), To.reshape(-1, 4, 4)
+
+    stats = {}
+    sampler = ClockSampler(local_rank)
+    # ---- batched, device-resident
+    with sampler:
+        ctx_b, t_b, poses_b, st_b = run(True)
+    total_b = sum(t_b)
+    prof = ctx_b.profile(reps=20)  # after the timed frames (re-integrates the last one)
+    if args.profile:  # the batched device path only (for profiler launch lists)
+        return dict(total_b=total_b, total_p=total_b, total_e=total_b, dpos=0.0, gt_err=0.0,
+                    status=(st_b, 0), clocks=sampler.summary(), h2d=0, d2h=0,
+                    ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, n_inst=len(s.instances))
+    # ---- plain (one instance per launch, host-driven GN)
+    ctx_p, t_p, poses_p, st_p = run(False)
+    total_p = sum(t_p)
+    # pose agreement between the two paths over the whole sequence
+    dpos = 0.0
+    for (cb, ob), (cp, op) in zip(poses_b, poses_p):
+        dpos = max(dpos, float(np.abs(cb[:3, 3] - cp[:3, 3]).max()),
+                   float(np.abs(ob[:, :3, 3] - op[:, :3, 3]).max()))
+    # pose error against ground truth (last frame), informative
+    gt_err = float(np.linalg.norm(poses_b[-1][0][:3, 3] - s.cam_poses[n_frames - 1][:3, 3]))
+
+    # ---- e2e through the C ABI from pinned host buffers
+    import ctypes
+    ctx_e = make_ctx(True)
+    stream_e = torch.cuda.ExternalStream(ctx_e.stream(), device=dev)
+    h_depth = [torch.from_numpy(f[0]).pin_memory() for f in frames]
+    h_rgb = [torch.from_numpy(np.ascontiguousarray(f[1])).pin_memory() for f in frames]
+    h_lab = [torch.from_numpy(f[2].astype(np.int16)).pin_memory() for f in frames]
+    Tc = torch.zeros(16, dtype=torch.float32).pin_memory()
+    To = torch.zeros(16 * len(s.instances), dtype=torch.float32).pin_memory()
+    t_e = []
+    for f in range(n_frames):
+        flush.fill_(f & 0xff)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream_e)
+        rc = ctx_e.lib.mf_process_frame(ctx_e.h, ctypes.c_void_p(h_depth[f].data_ptr()),
+                                        ctypes.c_void_p(h_rgb[f].data_ptr()),
+                                        ctypes.c_void_p(h_lab[f].data_ptr()))
+        rc |= ctx_e.lib.mf_get_poses(ctx_e.h, ctypes.c_void_p(Tc.data_ptr()),
+                                     ctypes.c_void_p(To.data_ptr()))
+        e1.record(stream_e)
+        e1.synchronize()
+        if rc != 0:
+            raise RuntimeError("mf_process_frame failed")
+        if f >= 1 + args.warmup:
+            t_e.append(e0.elapsed_time(e1) * 1e-3)
+    total_e = sum(t_e)
+    h2d = W * H * (4 + 3 + 2)
+    d2h = 64 * (1 + len(s.instances))
+    # ---- CPU baseline: rank 0 at N=1, a bounded sample of the same sequence
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import cpu_baseline as CB
+        n_cpu = min(3, n_frames - 1)
+        sec, kind = CB.time_frames(s, frames, 1, n_cpu, use_reference=True)
+        cpu = {"value": round(1.0 / sec, 4), "unit": "frames/s", "cores": CB.threads(),
+               "kind": kind,
+               "sample": f"frames 1..{n_cpu} of the same sequence (frame 0 untimed), full "
+                         f"640x480 frames, OpenMP on every host thread"}
+    return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
+                status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
+                ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
+                n_inst=len(s.instances))
+
+
+def run_reference(args):
+    """The reference's CPU implementation of the path on the host cores: one step
+    = one frame of the same workload (oracle/cpu_baseline.py: the reference's own
+    allocation / integration / raycast code built with OpenMP, the tracking
+    restated where the reference needs TooN)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import cpu_baseline as CB
+    n_frames = 1 + args.warmup + args.steps
+    frames = render_frames(0, n_frames, args.workers)
+    s = scene_for(0, n_frames)
+    p = CB.CpuPipeline(s, use_reference=True)
+    t = []
+    for f in range(n_frames):
+        d, rgb, lab = frames[f]
+        t0 = time.perf_counter()
+        p.step(d, rgb, lab)
+        if f >= 1 + args.warmup:
+            t.append(time.perf_counter() - t0)
+    total = sum(t)
+    value = len(t) / total
+    return {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "frames/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total / len(t), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4},
+        "cpu_baseline": {"value": round(value, 4), "unit": "frames/s", "cores": CB.threads(),
+                         "kind": p.kind,
+                         "sample": f"{len(t)} frames after {1 + args.warmup} untimed, full "
+                                   "640x480 frames, OpenMP on every host thread"},
+        "e2e": {"value": round(value, 4), "unit": "frames/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def traffic_from_profiles(name):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/<name>."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        for line in open(p):
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1].strip()))
+    except OSError:
+        pass
+    return None
+
+
+def reduce_max(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workers", type=int, default=min(32, os.cpu_count() or 4))
+    ap.add_argument("--pool-blocks", type=int, default=1 << 18)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile", action="store_true",
+                    help="run only the batched device-resident path (profiler runs)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    r = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    total_b = reduce_max(r["total_b"], world)
+    total_p = reduce_max(r["total_p"], world)
+    total_e = reduce_max(r["total_e"], world)
+    frames = args.steps * world
+    value = frames / total_b
+    hbm, peak_kind = measured_peaks()
+    prof = r["prof"]
+    gbs = lambda nbytes, us: nbytes / (us * 1e-6) / 1e9
+    # dominant kernel by device time: the Gauss-Newton evaluation (residuals +
+    # Jacobians + normal-equation reduction), timed live at level 0 of the camera
+    ach = gbs(prof["gn_l0_bytes"], prof["gn_l0_us"])
+    roofline = {"kernel": "gn_iter_kernel (camera, level 0, 640x480)", "bound": "hbm",
+                "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(ach / hbm, 4), "peak_kind": peak_kind,
+                "us_per_launch": round(prof["gn_l0_us"], 2),
+                "algorithmic_bytes_per_launch": int(prof["gn_l0_bytes"]),
+                "traffic": traffic_from_profiles("gn_iter_kernel_l0_640x480.md")}
+    ai = gbs(prof["integrate_bytes"], prof["integrate_us"])
+    others = {
+        "integrate_blocks_kernel": {"achieved": round(ai, 1), "unit": "GB/s",
+                                    "frac": round(ai / hbm, 4),
+                                    "us_per_launch": round(prof["integrate_us"], 2),
+                                    "algorithmic_bytes_per_launch": int(prof["integrate_bytes"]),
+                                    "traffic": traffic_from_profiles(
+                                        "integrate_blocks_kernel_640x480.md")},
+        "raycast_objects_kernel": {"us_per_launch": round(prof["raycast_us"], 2)},
+    }
+    per_frame = (r["stats"] or {}).get("graph_kernels", 0) + 1  # graph + rgb conversion
+    launches = per_frame * args.steps
+    out = {
+        "metric": METRIC,
+        "value": round(value, 2),
+        "unit": "frames/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(1e3 * total_b / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "precision": "f32 per-pixel arithmetic, f64 reductions, 6x6 solve and SE(3) update",
+        "data": "synthetic (seeded analytic RGB-D scenes)",
+        "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4,
+                   "l2": "flushed between steps (256 MiB write)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "plain": {"value": round(frames / total_p, 2), "unit": "frames/s",
+                  "ms_per_step": round(1e3 * total_p / args.steps, 4)},
+        "batched_over_plain": round(total_p / total_b, 3),
+        "pose_diff_batched_vs_plain_m": r["dpos"],
+        "camera_err_vs_gt_m": r["gt_err"],
+        "e2e": {"value": round(frames / total_e, 2), "unit": "frames/s",
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
+        "roofline": roofline,
+        "rooflines_other": others,
+        "cpu_baseline": r.get("cpu"),
+        "gpu_launches": launches,
+        "clocks": r["clocks"],
+        "status_flags": r["status"],
+        "last_frame_stats": r.get("stats"),
+        "peak_hbm_gbs": hbm, "peak_kind": peak_kind,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -151,6 +151,36 @@ int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, doubl
  * vertex (float3 planes are 3 floats per pixel). */
 int mf_download_pyramid(mf_context* ctx, int level, int which, float* out);
 
+/* --- whole frame -------------------------------------------------------
+ * One frame of Kfusion in the reference's order (mainQt.cpp:262-291,
+ * benchmark.cpp:113-159): preprocessing; from the second frame on, camera
+ * tracking against the last raycast (moving-object pixels excluded from ICP)
+ * and trackEachObject for every object instance; generalized masks from the
+ * uint16 ground-truth labels (NULL: keep the current masks); allocation +
+ * integration of every instance; raycastObjectList; setRefImgFromCurr.
+ * Host pointers (copied in; nothing is read back -- see mf_get_poses). */
+int mf_process_frame(mf_context* ctx, const float* depth, const uint8_t* rgb,
+                     const uint16_t* labels);
+/* Same with device pointers. */
+int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
+                            const uint16_t* d_labels);
+/* Camera pose (16 floats) and every instance's volume pose (16 floats each,
+ * instance order); either pointer may be NULL.  Synchronises. */
+int mf_get_poses(mf_context* ctx, float* T_w_c, float* T_w_o);
+/* Work counters of the last frame: out[0] voxel blocks in the pool, out[1]
+ * blocks visited by the last integration, out[2 + i] ray samples instance i
+ * emitted into its allocation list, out[2 + n_instances] kernel launches in one
+ * replay of the batched frame graph (0 before capture).  Synchronises. */
+int mf_frame_stats(mf_context* ctx, long long* out, int n);
+/* Kernel timing on the current frame (CUDA events on the context's stream,
+ * `reps` launches each): out[0] us per camera GN evaluation at level 0 and
+ * out[1] its algorithmic bytes; out[2] us per integration launch and out[3] its
+ * algorithmic bytes (counted); out[4] us per raycast launch.  Re-integrates
+ * the current frame, so call it only after the frames that matter. */
+int mf_profile(mf_context* ctx, int reps, double* out, int n);
+/* Batched mode replays the frame as a CUDA graph once captured (default 1). */
+int mf_set_graphs(mf_context* ctx, int enable);
+
 /* --- inspection (parity checks, debugging) -----------------------------
  * Blocks: key (code | level), corner voxel, VoxelBlock::active_, and when
  * `voxels` is not NULL the 512 voxels in the reference's 40-byte AoS layout

@@ -32,7 +32,9 @@ EXPORTS = [
     "mf_alloc_update", "mf_raycast", "mf_download_raycast", "mf_block_count",
     "mf_export_blocks", "mf_node_count", "mf_export_nodes", "mf_root_children", "mf_interp",
     "mf_preprocess", "mf_set_ref_from_current", "mf_track_camera", "mf_track_objects",
-    "mf_track_info", "mf_track_eval", "mf_download_pyramid",
+    "mf_track_info", "mf_track_eval", "mf_download_pyramid", "mf_process_frame",
+    "mf_process_frame_device", "mf_get_poses", "mf_frame_stats", "mf_set_graphs",
+    "mf_profile",
 ]
 
 
@@ -179,6 +181,19 @@ class Context:
         self._check(self.lib.mf_download_raycast(self.h, _ptr(v, np.float32),
                                                  _ptr(n, np.float32), _ptr(lab, np.int32)))
         return v, n, lab
+
+    def frame_stats(self):
+        out = np.zeros(3 + self.n_instances, np.int64)
+        self._check(self.lib.mf_frame_stats(self.h, _ptr(out, np.int64), len(out)))
+        return {"pool_blocks": int(out[0]), "visited_blocks": int(out[1]),
+                "emitted": [int(v) for v in out[2:2 + self.n_instances]],
+                "graph_kernels": int(out[2 + self.n_instances])}
+
+    def profile(self, reps=20):
+        out = np.zeros(6, np.float64)
+        self._check(self.lib.mf_profile(self.h, int(reps), _ptr(out, np.float64), len(out)))
+        return {"gn_l0_us": out[0], "gn_l0_bytes": out[1], "integrate_us": out[2],
+                "integrate_bytes": out[3], "raycast_us": out[4]}
 
     def status(self):
         f = C.c_int()

@@ -55,6 +55,16 @@ __global__ void fill_kernel(float* __restrict__ p, float v, size_t n) {
     p[i] = v;
 }
 
+int launch_generalize(Context* ctx) {
+  const int n = (int)ctx->inst.size();
+  if (n == 0) return MF_OK;
+  dim3 grid((ctx->W + 127) / 128, ctx->H, n);
+  generalize_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->d_labels, ctx->W, ctx->H,
+                                                   ctx->d_inst_label, n, ctx->d_masks);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
 }  // namespace mf
 
 static int check(mf_context* ctx) { return ctx ? MF_OK : MF_E_ARG; }
@@ -177,6 +187,7 @@ int mf_create(const mf_config* cfg, mf_context** out) {
 int mf_destroy(mf_context* ctx) {
   if (!ctx) return MF_E_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  pipeline_free(ctx);
   track_free(ctx);
   for (auto& in : ctx->inst) volume_free(in);
   Pool& P = ctx->pool;
@@ -329,13 +340,7 @@ int mf_frame_labels(mf_context* ctx, const uint16_t* labels) {
   if (check(ctx) || !labels) return MF_E_ARG;
   const size_t WH = (size_t)ctx->W * ctx->H;
   MF_CUDA(cudaMemcpyAsync(ctx->d_labels, labels, 2 * WH, cudaMemcpyHostToDevice, ctx->stream));
-  const int n = (int)ctx->inst.size();
-  if (n > 0) {
-    dim3 grid((ctx->W + 127) / 128, ctx->H, n);
-    generalize_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->d_labels, ctx->W, ctx->H,
-                                                     ctx->d_inst_label, n, ctx->d_masks);
-    MF_CUDA(cudaGetLastError());
-  }
+  if (int rc = launch_generalize(ctx)) return rc;
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
   return MF_OK;
 }
@@ -429,6 +434,77 @@ int mf_interp(mf_context* ctx, int id, const float* pos, int n, int field, float
     return MF_E_ARG;
   if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
   return interp_points(ctx, id, pos, n, field, out);
+}
+
+int mf_process_frame(mf_context* ctx, const float* depth, const uint8_t* rgb,
+                     const uint16_t* labels) {
+  if (check(ctx) || !depth || !rgb) return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_depth, depth, 4 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_rgb8, rgb, 3 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  rgb_convert_kernel<<<(unsigned)((WH + 255) / 256), 256, 0, ctx->stream>>>(
+      ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, (int)WH);
+  MF_CUDA(cudaGetLastError());
+  if (labels)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_labels, labels, 2 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  return process_frame(ctx, labels != nullptr);
+}
+
+int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
+                            const uint16_t* d_labels) {
+  if (check(ctx) || !d_depth || !d_rgb) return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_depth, d_depth, 4 * WH, cudaMemcpyDeviceToDevice, ctx->stream));
+  rgb_convert_kernel<<<(unsigned)((WH + 255) / 256), 256, 0, ctx->stream>>>(
+      d_rgb, ctx->d_rgb, ctx->d_grey, (int)WH);
+  MF_CUDA(cudaGetLastError());
+  if (d_labels)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_labels, d_labels, 2 * WH, cudaMemcpyDeviceToDevice,
+                            ctx->stream));
+  return process_frame(ctx, d_labels != nullptr);
+}
+
+int mf_get_poses(mf_context* ctx, float* T_w_c, float* T_w_o) {
+  if (check(ctx)) return MF_E_ARG;
+  if (T_w_c)
+    MF_CUDA(cudaMemcpyAsync(T_w_c, ctx->d_Twc, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  if (T_w_o)
+    MF_CUDA(cudaMemcpyAsync(T_w_o, ctx->d_Two, 64 * ctx->inst.size(), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_frame_stats(mf_context* ctx, long long* out, int n) {
+  if (check(ctx) || !out || n < 2) return MF_E_ARG;
+  int pc = 0, vc = 0;
+  MF_CUDA(cudaMemcpyAsync(&pc, ctx->pool.count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(&vc, ctx->d_visit_count, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  std::vector<unsigned long long> em(ctx->inst.size(), 0);
+  for (size_t i = 0; i < ctx->inst.size(); ++i)
+    MF_CUDA(cudaMemcpyAsync(&em[i], ctx->inst[i].vol.emit_total, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  out[0] = pc;
+  out[1] = vc;
+  for (size_t i = 0; i < ctx->inst.size() && (int)i + 2 < n; ++i) out[2 + i] = (long long)em[i];
+  if ((int)ctx->inst.size() + 2 < n) out[2 + ctx->inst.size()] = (long long)graph_kernel_nodes(ctx);
+  return MF_OK;
+}
+
+int mf_profile(mf_context* ctx, int reps, double* out, int n) {
+  if (check(ctx) || !out || n < 6 || reps < 1) return MF_E_ARG;
+  if (int rc = profile_gn(ctx, reps, &out[0], &out[1])) return rc;
+  if (int rc = profile_integrate(ctx, reps, &out[2], &out[3])) return rc;
+  out[5] = 0;
+  return profile_raycast(ctx, reps, &out[4]);
+}
+
+int mf_set_graphs(mf_context* ctx, int enable) {
+  if (check(ctx)) return MF_E_ARG;
+  ctx->use_graphs = enable != 0;
+  return MF_OK;
 }
 
 int mf_preprocess(mf_context* ctx) {

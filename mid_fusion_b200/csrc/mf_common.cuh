@@ -74,9 +74,12 @@ MF_HD void m_set(M4& m, int i, int j, float v) {
 // 4x4 float product accumulated k = 0..3 (commons.h:657-662 via TooN).
 MF_HD M4 mul(const M4& A, const M4& B) {
   M4 R;
+#pragma unroll
   for (int i = 0; i < 4; ++i)
+#pragma unroll
     for (int j = 0; j < 4; ++j) {
       float s = m_at(A, i, 0) * m_at(B, 0, j);
+#pragma unroll
       for (int k = 1; k < 4; ++k) s += m_at(A, i, k) * m_at(B, k, j);
       m_set(R, i, j, s);
     }
@@ -85,31 +88,68 @@ MF_HD M4 mul(const M4& A, const M4& B) {
 // commons.h:649-655 (TooN gaussian_elimination, not vendored): Gaussian
 // elimination with partial pivoting on [A | I], then back substitution, float.
 MF_HD M4 inverse(const M4& A) {
+  // Fully unrolled so every index is a compile-time constant (registers, no
+  // local memory); the pivot swap is a predicated exchange of whole rows, so the
+  // arithmetic is exactly that of the plain partial-pivoting elimination.
   float a[4][4], b[4][4];
+#pragma unroll
   for (int i = 0; i < 4; ++i)
+#pragma unroll
     for (int j = 0; j < 4; ++j) { a[i][j] = m_at(A, i, j); b[i][j] = (i == j) ? 1.f : 0.f; }
+#pragma unroll
   for (int c = 0; c < 4; ++c) {
-    int p = c; float best = fabsf(a[c][c]);
-    for (int r = c + 1; r < 4; ++r) if (fabsf(a[r][c]) > best) { best = fabsf(a[r][c]); p = r; }
-    if (p != c)
-      for (int j = 0; j < 4; ++j) {
-        float t = a[c][j]; a[c][j] = a[p][j]; a[p][j] = t;
-        t = b[c][j]; b[c][j] = b[p][j]; b[p][j] = t;
+    int p = c;
+    float best = fabsf(a[c][c]);
+#pragma unroll
+    for (int r = c + 1; r < 4; ++r)
+      if (fabsf(a[r][c]) > best) { best = fabsf(a[r][c]); p = r; }
+#pragma unroll
+    for (int r = c + 1; r < 4; ++r) {
+      if (p == r) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          float t = a[c][j]; a[c][j] = a[r][j]; a[r][j] = t;
+          t = b[c][j]; b[c][j] = b[r][j]; b[r][j] = t;
+        }
       }
+    }
+#pragma unroll
     for (int r = c + 1; r < 4; ++r) {
       const float f = a[r][c] / a[c][c];
+#pragma unroll
       for (int j = c; j < 4; ++j) a[r][j] -= f * a[c][j];
+#pragma unroll
       for (int j = 0; j < 4; ++j) b[r][j] -= f * b[c][j];
     }
   }
-  M4 R;
+  float R[4][4];
+#pragma unroll
   for (int j = 0; j < 4; ++j)
+#pragma unroll
     for (int r = 3; r >= 0; --r) {
       float s = b[r][j];
-      for (int k = r + 1; k < 4; ++k) s -= a[r][k] * m_at(R, k, j);
-      m_set(R, r, j, s / a[r][r]);
+#pragma unroll
+      for (int k = r + 1; k < 4; ++k) s -= a[r][k] * R[k][j];
+      R[r][j] = s / a[r][r];
     }
-  return R;
+  M4 out;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) out.r[i] = F4{R[i][0], R[i][1], R[i][2], R[i][3]};
+  return out;
+}
+// 16 floats (row-major Matrix4) from / to memory, four 4-float loads/stores
+// when the pointer is 16-byte aligned.
+MF_HD M4 load_m4(const float* p) {
+  M4 m;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) m.r[i] = F4{p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]};
+  return m;
+}
+MF_HD void store_m4(float* p, const M4& m) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    p[4 * i] = m.r[i].x; p[4 * i + 1] = m.r[i].y; p[4 * i + 2] = m.r[i].z; p[4 * i + 3] = m.r[i].w;
+  }
 }
 MF_HD M4 camera_matrix(F4 k) {  // commons.h:631-638
   M4 K;

@@ -92,6 +92,8 @@ struct Context {
   size_t h_pinned_bytes = 0;
 
   float ray_epsilon = 0.f;          // ray iterator direction epsilon (first volume)
+  void* graphs = nullptr;           // captured frame graphs (mf_pipeline.cu)
+  bool use_graphs = true;
   TrackState* track = nullptr;
 };
 
@@ -126,6 +128,16 @@ int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int track_download_level(Context* ctx, int L, int which, float* out);
 void track_save_prev_camera(Context* ctx);
+bool track_has_ref(Context* ctx);
+int track_parity(Context* ctx);
+void track_set_parity(Context* ctx, int parity);
+int launch_generalize(Context* ctx);
+int process_frame(Context* ctx, bool labels);
+int profile_integrate(Context* ctx, int reps, double* us, double* bytes);
+int profile_gn(Context* ctx, int reps, double* us, double* bytes);
+int profile_raycast(Context* ctx, int reps, double* us);
+void pipeline_free(Context* ctx);
+size_t graph_kernel_nodes(Context* ctx);
 int volume_create(Context* ctx, Instance& in);
 void volume_free(Instance& in);
 

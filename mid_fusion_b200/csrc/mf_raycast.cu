@@ -18,7 +18,8 @@ namespace mf {
 // the traversal stack holds one entry per level.  The loop carries an
 // iteration guard (never reached by a valid traversal; it only protects the
 // GPU from a corrupted table).
-__device__ float ray_first_block(const Volume& V, F3 origin, F3 direction, float nearPlane,
+__device__ __noinline__ float ray_first_block(const Volume& V, F3 origin, F3 direction,
+                                              float nearPlane,
                                  float farPlane, float epsilon, int* status) {
   int st_m[MAX_LEVELS];
   float st_t[MAX_LEVELS];
@@ -122,7 +123,8 @@ __device__ float ray_first_block(const Volume& V, F3 origin, F3 direction, float
 
 // raycast(const Volume<SDF>&, origin, direction, ...),
 // apps/kfusion/src/cpp/kfusion/rendering_impl.hpp:80-140.
-__device__ F4 raycast_volume(const Pool& P, const Volume& V, F3 origin, F3 direction,
+__device__ __noinline__ F4 raycast_volume(const Pool& P, const Volume& V, F3 origin,
+                                          F3 direction,
                              float nearPlane, float farPlane, float mu, float step,
                              float largestep) {
   const F3 invR = mk3(1.0f / direction.x, 1.0f / direction.y, 1.0f / direction.z);
@@ -136,18 +138,19 @@ __device__ F4 raycast_volume(const Pool& P, const Volume& V, F3 origin, F3 direc
   const float tfar = fmn(smallest_tmax, farPlane);
   const float inv = V.size / V.dim;
   if (tnear < tfar) {
+    BlockMemo memo;
     float t = tnear, stepsize = largestep;
     F3 position = origin + direction * t;
-    float f_t = volume_interp(P, V, position, 0), f_tt = 0;
+    float f_t = volume_interp_m<0>(P, V, position, memo), f_tt = 0;
     if (f_t > 0) {
       // (guarded: a valid march takes at most (far - near) / step steps)
       for (int guard = 0; t < tfar && guard < (1 << 20); t += stepsize, ++guard) {
         // Volume::get -> get_fine at the truncated voxel (volume_template.hpp:83-88);
         // the weight test data.y < 0 can never hold for SDF voxels.
         const I3 s = to_i3(mk3(position.x * inv, position.y * inv, position.z * inv));
-        f_tt = tsdf_at(P, V, s.x, s.y, s.z);
+        f_tt = tsdf_at_m(P, V, memo, s.x, s.y, s.z);
         // f_tt <= 0.1 compares in double; for a float that is f_tt < 0.1f.
-        if (f_tt < 0.1f && f_tt >= -0.5f) f_tt = volume_interp(P, V, position, 0);
+        if (f_tt < 0.1f && f_tt >= -0.5f) f_tt = volume_interp_m<0>(P, V, position, memo);
         if (f_tt < 0) break;
         stepsize = fmx(f_tt * mu, step);
         position = position + stepsize * direction;
@@ -222,6 +225,27 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
     a.normal[p] = mk3(INVALID, 0, 0);
     a.label[p] = (int)INVALID;
   }
+}
+
+int profile_raycast(Context* ctx, int reps, double* us) {
+  IdList all;
+  all.n = (int)ctx->inst.size();
+  for (int i = 0; i < all.n; ++i) all.v[i] = i;
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, ctx->stream);
+  for (int r = 0; r < reps; ++r)
+    if (int rc = stage_raycast(ctx, all, ctx->ray_epsilon)) return rc;
+  cudaEventRecord(e1, ctx->stream);
+  MF_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *us = 1e3 * ms / reps;
+  return MF_OK;
 }
 
 int stage_raycast(Context* ctx, const IdList& ids, float epsilon) {

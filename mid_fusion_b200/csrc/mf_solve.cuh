@@ -16,13 +16,20 @@ namespace mf {
 
 // makeJTJ, commons.h:673-687: 21 upper-triangle terms (row-major) -> 6x6.
 MF_HD void make_jtj(const double* v21, double A[6][6]) {
-  int q = 0;
+#pragma unroll
   for (int i = 0; i < 6; ++i)
-    for (int j = i; j < 6; ++j) { A[i][j] = v21[q]; A[j][i] = v21[q]; ++q; }
+#pragma unroll
+    for (int j = i; j < 6; ++j) {
+      const int q = i * 6 - i * (i - 1) / 2 + (j - i);
+      A[i][j] = v21[q];
+      A[j][i] = v21[q];
+    }
 }
 
-MF_HD void solve6_eigen(const double Ain[6][6], const double b[6], double condition,
-                        double x[6]) {
+// Not inlined: the rare ill-conditioned path.
+__host__ __device__ __noinline__ inline void solve6_eigen(const double Ain[6][6],
+                                                          const double b[6], double condition,
+                                                          double x[6]) {
   double A[6][6], V[6][6];
   for (int i = 0; i < 6; ++i)
     for (int j = 0; j < 6; ++j) { A[i][j] = Ain[i][j]; V[i][j] = i == j ? 1.0 : 0.0; }
@@ -64,39 +71,49 @@ MF_HD void solve6_eigen(const double Ain[6][6], const double b[6], double condit
   }
 }
 
-// Returns true when the truncated eigen solve was needed.
+// Returns true when the truncated eigen solve was needed.  All loops have
+// compile-time bounds and are unrolled, so the factorisation stays in registers.
 MF_HD bool solve6(const double A[6][6], const double b[6], double x[6]) {
   double L[6][6], d[6];
   double dmax = 0;
   bool ok = true;
-  for (int j = 0; j < 6 && ok; ++j) {
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
     double dj = A[j][j];
+#pragma unroll
     for (int k = 0; k < j; ++k) dj -= L[j][k] * L[j][k] * d[k];
     d[j] = dj;
     dmax = fmax(dmax, dj);
-    if (!(dj > 1e-5 * dmax) || !(dj > 0)) { ok = false; break; }
+    ok = ok && (dj > 0);
+    const double inv = 1.0 / dj;
+#pragma unroll
     for (int i = j + 1; i < 6; ++i) {
       double v = A[i][j];
+#pragma unroll
       for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k] * d[k];
-      L[i][j] = v / dj;
+      L[i][j] = v * inv;
     }
   }
-  if (ok) {
-    for (int j = 0; j < 6; ++j) if (!(d[j] > 1e-5 * dmax)) ok = false;
-  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) ok = ok && (d[j] > 1e-5 * dmax);
   if (!ok) {
     solve6_eigen(A, b, 1e6, x);
     return true;
   }
   double y[6];
+#pragma unroll
   for (int i = 0; i < 6; ++i) {
     double v = b[i];
+#pragma unroll
     for (int k = 0; k < i; ++k) v -= L[i][k] * y[k];
     y[i] = v;
   }
+#pragma unroll
   for (int i = 0; i < 6; ++i) y[i] /= d[i];
+#pragma unroll
   for (int i = 5; i >= 0; --i) {
     double v = y[i];
+#pragma unroll
     for (int k = i + 1; k < 6; ++k) v -= L[k][i] * x[k];
     x[i] = v;
   }
@@ -113,11 +130,15 @@ MF_HD void se3_exp(const double xi[6], double T[16]) {
     A = 1 - th2 / 6; B = 0.5 - th2 / 24; C = 1.0 / 6 - th2 / 120;
   } else {
     const double th = sqrt(th2);
-    A = sin(th) / th; B = (1 - cos(th)) / th2; C = (1 - A) / th2;
+    double sn, cs;
+    sincos(th, &sn, &cs);
+    A = sn / th; B = (1 - cs) / th2; C = (1 - A) / th2;
   }
   const double W[3][3] = {{0, -w2, w1}, {w2, 0, -w0}, {-w1, w0, 0}};
+#pragma unroll
   for (int i = 0; i < 3; ++i) {
     double t = 0;
+#pragma unroll
     for (int j = 0; j < 3; ++j) {
       const double W2 = W[i][0] * W[0][j] + W[i][1] * W[1][j] + W[i][2] * W[2][j];
       const double I = i == j ? 1.0 : 0.0;
@@ -130,9 +151,12 @@ MF_HD void se3_exp(const double xi[6], double T[16]) {
 }
 
 MF_HD void mul4d(const double* A, const double* B, double* R) {
+#pragma unroll
   for (int i = 0; i < 4; ++i)
+#pragma unroll
     for (int j = 0; j < 4; ++j) {
       double s = 0;
+#pragma unroll
       for (int k = 0; k < 4; ++k) s += A[4 * i + k] * B[4 * k + j];
       R[4 * i + j] = s;
     }
@@ -140,6 +164,7 @@ MF_HD void mul4d(const double* A, const double* B, double* R) {
 
 MF_HD M4 to_m4f(const double* T) {
   M4 m;
+#pragma unroll
   for (int i = 0; i < 4; ++i) {
     m.r[i].x = (float)T[4 * i]; m.r[i].y = (float)T[4 * i + 1];
     m.r[i].z = (float)T[4 * i + 2]; m.r[i].w = (float)T[4 * i + 3];

@@ -6,8 +6,10 @@
 // problem of the stage (the camera, or all moving objects at once), weights
 // them (IRLS), and reduces the 29 sums of the normal equations plus the three
 // outlier counts:
-//   - per thread in FP32 with Kahan-compensated accumulation,
-//   - per warp / block / grid in FP64 (block partials, fixed order),
+//   - per thread in FP32 over at most GN_PIX_MAX pixels (2 rows each), so no
+//     FP32 sum runs over more than 2 * GN_PIX_MAX terms,
+//   - per warp / block / grid in FP64 (block partials, fixed summation order,
+//     so results are bitwise reproducible run to run),
 // and the block that finishes last for a problem runs that problem's GN step
 // on the device (cost test, step back, FP64 6x6 solve, SE(3) update,
 // convergence test).  The host only launches: the whole coarse-to-fine loop is
@@ -24,8 +26,8 @@ namespace mf {
 
 constexpr float INVALIDF = -2.f;
 constexpr int GN_THREADS = 256;
-constexpr int GN_PIX = 4;  // pixels per thread per iteration
-constexpr int GN_TILE = GN_THREADS * GN_PIX;
+constexpr int GN_PIX_MAX = 2;  // pixels per thread per iteration at level 0 (1 above)
+__host__ __device__ constexpr int gn_pix(int L) { return L == 0 ? GN_PIX_MAX : 1; }
 
 struct GNState {
   double T[16], prevT[16];
@@ -221,9 +223,8 @@ __global__ void depth2vertex_slots_kernel(SlotPtrs sp, int w, int h, M4 invK) {
 __global__ void setup_camera_kernel(GNState* st, const float* __restrict__ Twc,
                                     float* __restrict__ Twc_prev, F4 k) {
   GNState& S = st[0];
-  M4 T;
-  memcpy(&T, Twc, 64);
-  memcpy(Twc_prev, Twc, 64);
+  const M4 T = load_m4(Twc);
+  store_m4(Twc_prev, T);
   for (int i = 0; i < 16; ++i) {
     S.T[i] = (double)Twc[i];
     S.prevT[i] = S.T[i];
@@ -246,10 +247,7 @@ __global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __r
   if (t >= slots.n) return;
   const int s = slots.v[t];
   GNState& S = st[s];
-  M4 T_w_c2, T_w_c1, T_wo1;
-  memcpy(&T_w_c2, Twc2, 64);
-  memcpy(&T_w_c1, Twc1, 64);
-  memcpy(&T_wo1, Two + 16 * s, 64);
+  const M4 T_w_c2 = load_m4(Twc2), T_w_c1 = load_m4(Twc1), T_wo1 = load_m4(Two + 16 * s);
   S.kind = 1; S.inst = s; S.label = inst_label[s]; S.done = 0; S.ticket = 0; S.fallback = 0;
   for (int l = 0; l < MAX_PYR; ++l) S.iters[l] = 0;
   S.T_w_c2 = T_w_c2;
@@ -276,8 +274,7 @@ __global__ void level_start_kernel(GNState* st, IdList slots) {
 }
 
 __global__ void finalize_camera_kernel(const GNState* st, float* __restrict__ Twc) {
-  const M4 T = to_m4f(st[0].T);
-  memcpy(Twc, &T, 64);
+  store_m4(Twc, to_m4f(st[0].T));
 }
 
 // volume_pose_ = T_w_c2 * T_c2_o2, tracking.cpp:695.
@@ -285,40 +282,56 @@ __global__ void finalize_objects_kernel(const GNState* st, IdList slots, float* 
   const int t = threadIdx.x;
   if (t >= slots.n) return;
   const int s = slots.v[t];
-  const M4 P = mul(st[s].T_w_c2, to_m4f(st[s].T));
-  memcpy(Two + 16 * s, &P, 64);
+  store_m4(Two + 16 * s, mul(st[s].T_w_c2, to_m4f(st[s].T)));
 }
 
 // ------------------------------------------------------------------ GN step
 // One GN iteration's decision logic (tracking.cpp:287-335, objects :657-686):
 // cost test with step back, solve, convergence test, left-multiplied update.
 MF_HD void gn_step(GNState& S, const double* s, int level) {
+  // work on register copies; one copy-out at the end
+  double T[16], P[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) { T[i] = S.T[i]; P[i] = S.prevT[i]; }
+  const double prev_err = S.prev_err;
   const double err = s[0] / s[28];
-  if (S.kind == 1 && s[28] == 0) { S.done = 1; return; }
-  if (err > S.prev_err) {
-    for (int i = 0; i < 16; ++i) S.T[i] = S.prevT[i];
+  int done = 0, fallback = 0;
+  if (S.kind == 1 && s[28] == 0) {
     S.done = 1;
+    return;
+  }
+  if (err > prev_err) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) T[i] = P[i];
+    done = 1;
   } else {
     S.prev_err = err;
     double A[6][6], b[6], x[6];
+#pragma unroll
     for (int i = 0; i < 6; ++i) b[i] = s[1 + i];
     make_jtj(s + 7, A);
-    if (solve6(A, b, x)) S.fallback = 1;
+    if (solve6(A, b, x)) fallback = 1;
     double nx = 0;
+#pragma unroll
     for (int i = 0; i < 6; ++i) nx += x[i] * x[i];
     if (sqrt(nx) < (double)1e-05f && sqrt(s[0] / s[28]) < 2e-3) {
-      S.done = 1;
+      done = 1;
     } else {
       double E[16], R[16];
       se3_exp(x, E);
-      for (int i = 0; i < 16; ++i) S.prevT[i] = S.T[i];
-      mul4d(E, S.T, R);
-      for (int i = 0; i < 16; ++i) S.T[i] = R[i];
+      mul4d(E, T, R);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) { P[i] = T[i]; T[i] = R[i]; }
     }
   }
+#pragma unroll
+  for (int i = 0; i < 16; ++i) { S.T[i] = T[i]; S.prevT[i] = P[i]; }
+  S.done = done;
+  if (fallback) S.fallback = 1;
   S.iters[level] += 1;
-  S.Tf = to_m4f(S.T);
-  S.invTf = inverse(S.Tf);
+  const M4 Tf = to_m4f(T);
+  S.Tf = Tf;
+  S.invTf = inverse(Tf);
 }
 
 // ------------------------------------------------------------------ residuals
@@ -508,17 +521,11 @@ __device__ __forceinline__ void robust(float e, int kind, float& w, float& loss)
   loss = (float)l;
 }
 
-struct Kahan {
-  float s, c;
-  __device__ __forceinline__ void add(float x) {
-    const float y = x - c;
-    const float t = s + y;
-    c = (t - s) - y;
-    s = t;
-  }
-};
+// Index of J_i J_j (i <= j) among the 21 upper-triangle terms, row-major
+// (reduce, tracking.cpp:1279-1311).
+__host__ __device__ constexpr int jtj_index(int i, int j) { return 7 + i * 6 - i * (i - 1) / 2 + (j - i); }
 
-__device__ __forceinline__ void accumulate(Kahan* acc, int* cnt, const Row& r, int kind) {
+__device__ __forceinline__ void accumulate(float* acc, int* cnt, const Row& r, int kind) {
   if (r.result < 1) {
     cnt[0] += r.result == -4;
     cnt[1] += r.result == -5;
@@ -527,39 +534,43 @@ __device__ __forceinline__ void accumulate(Kahan* acc, int* cnt, const Row& r, i
   }
   float w, loss;
   robust(r.e, kind, w, loss);
-  acc[0].add(loss);
+  acc[0] += loss;
   const float we = w * r.e;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) acc[1 + i].add(we * r.J[i]);
-  int q = 7;
+  for (int i = 0; i < 6; ++i) acc[1 + i] += we * r.J[i];
 #pragma unroll
   for (int i = 0; i < 6; ++i) {
     const float wj = w * r.J[i];
 #pragma unroll
-    for (int j = i; j < 6; ++j) acc[q++].add(wj * r.J[j]);
+    for (int j = i; j < 6; ++j) acc[jtj_index(i, j)] += wj * r.J[j];
   }
-  acc[28].add(1.f);
+  acc[28] += 1.f;
 }
 
-__global__ void __launch_bounds__(GN_THREADS)
+// KIND 0: the camera problem; KIND 1: object problems (one instantiation each
+// keeps the kernel's code small).
+template <int KIND>
+__global__ void __launch_bounds__(GN_THREADS, 2)
 gn_iter_kernel(GNArgs a, IdList slots, int L) {
   const int s = slots.v[blockIdx.y];
   GNState& S = a.st[s];
   if (S.done) return;
   const int w = a.pyr.w[L], h = a.pyr.h[L];
   const int n = w * h;
-  Kahan acc[29];
+  float acc[29];
 #pragma unroll
-  for (int i = 0; i < 29; ++i) { acc[i].s = 0.f; acc[i].c = 0.f; }
+  for (int i = 0; i < 29; ++i) acc[i] = 0.f;
   int cnt[3] = {0, 0, 0};
   const F3* rV = a.rV[s];
-  for (int k = 0; k < GN_PIX; ++k) {
-    const int p = blockIdx.x * GN_TILE + k * GN_THREADS + threadIdx.x;
+  const int ppt = gn_pix(L);
+#pragma unroll 1
+  for (int k = 0; k < ppt; ++k) {
+    const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
     if (p >= n) break;
     Row r;
     if (a.use_icp) {
       r.result = 0;
-      if (S.kind == 0) icp_camera(a, S, L, p, r);
+      if (KIND == 0) icp_camera(a, S, L, p, r);
       else icp_object(a, S, L, p, r);
       accumulate(acc, cnt, r, a.robust);
     }
@@ -572,8 +583,9 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   // FP64 from the warp level up
   __shared__ double sh[GN_THREADS / 32][32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
   for (int i = 0; i < 32; ++i) {
-    double v = i < 29 ? (double)acc[i].s - (double)acc[i].c : (double)cnt[i - 29];
+    double v = i < 29 ? (double)acc[i] : (double)cnt[i - 29];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) sh[warp][i] = v;
@@ -582,6 +594,7 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   __shared__ bool last;
   if (threadIdx.x < 32) {
     double v = 0;
+#pragma unroll
     for (int wi = 0; wi < GN_THREADS / 32; ++wi) v += sh[wi][threadIdx.x];
     a.partials[((size_t)s * a.max_tiles + blockIdx.x) * 32 + threadIdx.x] = v;
     __threadfence();
@@ -594,11 +607,20 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   __syncthreads();
   if (!last) return;
   __threadfence();
+  // last block: sum the block partials in a fixed order with all threads
+  {
+    const int i = threadIdx.x & 31, g = threadIdx.x >> 5;  // 8 groups of tiles
+    double v = 0;
+    for (int b = g; b < (int)gridDim.x; b += GN_THREADS / 32)
+      v += __ldcg(&a.partials[((size_t)s * a.max_tiles + b) * 32 + i]);
+    sh[g][i] = v;
+  }
+  __syncthreads();
   __shared__ double tot[32];
   if (threadIdx.x < 32) {
     double v = 0;
-    for (int b = 0; b < (int)gridDim.x; ++b)
-      v += __ldcg(&a.partials[((size_t)s * a.max_tiles + b) * 32 + threadIdx.x]);
+#pragma unroll
+    for (int g = 0; g < GN_THREADS / 32; ++g) v += sh[g][threadIdx.x];
     tot[threadIdx.x] = v;
     S.sums[L][threadIdx.x] = v;
   }
@@ -650,7 +672,9 @@ int track_init(Context* ctx) {
     }
     if (rc) return MF_E_CUDA;
   }
-  ts->max_tiles = div_up((long long)ctx->W * ctx->H, GN_TILE);
+  ts->max_tiles = 0;
+  for (int l = 0; l < ts->levels; ++l)
+    ts->max_tiles = std::max(ts->max_tiles, div_up((long long)P.w[l] * P.h[l], GN_THREADS * gn_pix(l)));
   if (talloc(ctx, &ts->d_state, MAX_INSTANCES)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_partials, (size_t)MAX_INSTANCES * ts->max_tiles * 32)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_Twc_prev, 16)) return MF_E_CUDA;
@@ -819,14 +843,16 @@ static GNArgs make_args(Context* ctx, int L, int device_step) {
 
 // Coarse-to-fine GN of every problem in `slots`, all on the device
 // (trackLiveFrame :240-335 / trackEachObject :629-694).
-static int gn_device(Context* ctx, const IdList& slots) {
+static int gn_device(Context* ctx, const IdList& slots, int kind) {
   TrackState& T = *ctx->track;
   for (int L = T.levels - 1; L >= 0; --L) {
     level_start_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, slots);
     const GNArgs a = make_args(ctx, L, 1);
-    const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_TILE);
-    for (int it = 0; it < ctx->cfg.gn_iterations[L]; ++it)
-      gn_iter_kernel<<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
+    const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_THREADS * gn_pix(L));
+    for (int it = 0; it < ctx->cfg.gn_iterations[L]; ++it) {
+      if (kind == 0) gn_iter_kernel<0><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
+      else gn_iter_kernel<1><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
+    }
     MF_CUDA(cudaGetLastError());
   }
   return MF_OK;
@@ -848,11 +874,12 @@ static int gn_host(Context* ctx, int slot) {
     S.done = 0;
     S.ticket = 0;
     const GNArgs a = make_args(ctx, L, 0);
-    const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_TILE);
+    const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_THREADS * gn_pix(L));
     for (int it = 0; it < ctx->cfg.gn_iterations[L] && !S.done; ++it) {
       MF_CUDA(cudaMemcpyAsync(T.d_state + slot, &S, sizeof(GNState), cudaMemcpyHostToDevice,
                               ctx->stream));
-      gn_iter_kernel<<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
+      if (S.kind == 0) gn_iter_kernel<0><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
+      else gn_iter_kernel<1><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
       MF_CUDA(cudaGetLastError());
       MF_CUDA(cudaMemcpyAsync(S.sums[L], sums_ptr(T, slot, L), sizeof(double) * 32,
                               cudaMemcpyDeviceToHost, ctx->stream));
@@ -885,7 +912,7 @@ int track_camera(Context* ctx, uint32_t moving) {
   cam.v[0] = 0;
   if (int rc = render_reference(ctx, cam)) return rc;
   if (c.batched) {
-    if (int rc = gn_device(ctx, cam)) return rc;
+    if (int rc = gn_device(ctx, cam, 0)) return rc;
   } else {
     if (int rc = gn_host(ctx, 0)) return rc;
   }
@@ -906,7 +933,7 @@ int track_objects(Context* ctx, const IdList& ids) {
   MF_CUDA(cudaGetLastError());
   if (int rc = render_reference(ctx, ids)) return rc;
   if (ctx->cfg.batched) {
-    if (int rc = gn_device(ctx, ids)) return rc;
+    if (int rc = gn_device(ctx, ids, 1)) return rc;
   } else {
     for (int i = 0; i < ids.n; ++i)
       if (int rc = gn_host(ctx, ids.v[i])) return rc;
@@ -915,6 +942,10 @@ int track_objects(Context* ctx, const IdList& ids) {
   MF_CUDA(cudaGetLastError());
   return MF_OK;
 }
+
+bool track_has_ref(Context* ctx) { return ctx->track && ctx->track->have_ref; }
+int track_parity(Context* ctx) { return ctx->track->cur; }
+void track_set_parity(Context* ctx, int parity) { ctx->track->cur = parity; }
 
 void track_save_prev_camera(Context* ctx) {
   cudaMemcpyAsync(ctx->track->d_Twc_prev, ctx->d_Twc, 64, cudaMemcpyDeviceToDevice, ctx->stream);
@@ -956,12 +987,51 @@ int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums)
   one.n = 1;
   one.v[0] = slot;
   const GNArgs a = make_args(ctx, L, 0);
-  const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_TILE);
-  gn_iter_kernel<<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
+  const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_THREADS * gn_pix(L));
+  if (S.kind == 0) gn_iter_kernel<0><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
+  else gn_iter_kernel<1><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
   MF_CUDA(cudaGetLastError());
   MF_CUDA(cudaMemcpyAsync(sums, sums_ptr(T, slot, L), sizeof(double) * 32,
                           cudaMemcpyDeviceToHost, ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+// Timing and algorithmic bytes of one camera GN evaluation at level 0 on the
+// current frame (used after the timed region).  Bytes per pixel: ICP live
+// vertex, normal, covariance and the model vertex and normal (5 x 12 B), RGB
+// rendered and live reference vertex (2 x 12 B), reference intensity (4 B), the
+// 4-tap intensity and gradient gathers (16 + 32 B) and the outlier mask (2 B).
+int profile_gn(Context* ctx, int reps, double* us, double* bytes) {
+  if (!ctx->track) return MF_E_STATE;
+  TrackState& T = *ctx->track;
+  IdList one;
+  one.n = 1;
+  one.v[0] = 0;
+  GNState S;
+  MF_CUDA(cudaMemcpyAsync(&S, T.d_state, sizeof(GNState), cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  S.done = 0;
+  S.ticket = 0;
+  MF_CUDA(cudaMemcpyAsync(T.d_state, &S, sizeof(GNState), cudaMemcpyHostToDevice, ctx->stream));
+  const GNArgs a = make_args(ctx, 0, 0);
+  const int tiles = div_up((long long)T.pyr.w[0] * T.pyr.h[0], GN_THREADS * gn_pix(0));
+  gn_iter_kernel<0><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, 0);  // warm
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, ctx->stream);
+  for (int r = 0; r < reps; ++r)
+    gn_iter_kernel<0><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, 0);
+  cudaEventRecord(e1, ctx->stream);
+  MF_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  MF_CUDA(cudaGetLastError());
+  *us = 1e3 * ms / reps;
+  *bytes = 138.0 * T.pyr.w[0] * T.pyr.h[0];
   return MF_OK;
 }
 

@@ -26,9 +26,7 @@ __global__ void prepare_kernel(const float* __restrict__ Twc_p, const float* __r
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ids.n) return;
   const int i = ids.v[t];
-  M4 T_w_c, T_w_o;
-  memcpy(&T_w_c, Twc_p, 64);
-  memcpy(&T_w_o, Two_p + 16 * i, 64);
+  const M4 T_w_c = load_m4(Twc_p), T_w_o = load_m4(Two_p + 16 * i);
   const Volume V = vols[i];
   InstFrame f;
   f.T_w_o = T_w_o;
@@ -64,50 +62,64 @@ alloc_mark_kernel(const float* __restrict__ depth, const float* __restrict__ mas
                   int H, const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
                   IdList ids, Pool pool) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= W * H) return;
   const int inst = ids.v[blockIdx.y];
-  const float d = depth[p];
-  if (d == 0 || masks[(size_t)inst * W * H + p] < 0) return;
   const Volume& V = vols[inst];
   const InstFrame& F = frames[inst];
-  const unsigned x = p % W, y = p / W;
-  const float size_f = (float)(unsigned)V.size;
-  const F3 w_vertex = xform(F.kPose, mk3((x + 0.5f) * d, (y + 0.5f) * d, d));
-  const F3 o_vertex = xform(F.inv_T_w_o, w_vertex);
-  const F3 direction = normalize(F.o_cam - o_vertex);
-  const F3 origin = o_vertex - (F.band * 0.5f) * direction;
-  const F3 step = (direction * F.band) / (float)F.num_steps;
-  F3 pos = origin;
-  int run_idx = -1, run_len = 0;
   unsigned count = 0, last_order = 0, last_idx = 0;
-  const int bshift = 3;
-  for (int i = 0; i < F.num_steps; i++) {
-    const F3 s = floor3(pos * F.inv_voxel);
-    if (s.x < size_f && s.y < size_f && s.z < size_f && s.x >= 0 && s.y >= 0 && s.z >= 0) {
-      const I3 v = to_i3(s);
-      const uint32_t bidx = (uint32_t)morton3(v.x >> bshift, v.y >> bshift, v.z >> bshift);
-      const int slot = V.block_tab[bidx];
-      if (slot >= 0) {
-        pool.active[slot] = 1;
-      } else {
-        if ((int)bidx == run_idx) {
-          ++run_len;
-        } else {
-          if (run_len) atomicAdd(&V.req[run_idx], (uint32_t)run_len);
-          run_idx = (int)bidx;
-          run_len = 1;
+  // no early return: every lane reaches the warp reduction below
+  const float d = p < W * H ? depth[p] : 0.f;
+  if (d != 0 && !(masks[(size_t)inst * W * H + p] < 0)) {
+    const unsigned x = p % W, y = p / W;
+    const float size_f = (float)(unsigned)V.size;
+    const F3 w_vertex = xform(F.kPose, mk3((x + 0.5f) * d, (y + 0.5f) * d, d));
+    const F3 o_vertex = xform(F.inv_T_w_o, w_vertex);
+    const F3 direction = normalize(F.o_cam - o_vertex);
+    const F3 origin = o_vertex - (F.band * 0.5f) * direction;
+    const F3 step = (direction * F.band) / (float)F.num_steps;
+    F3 pos = origin;
+    int run_idx = -1, run_len = 0;
+    int cur_key = -1, cur_slot = -1;
+    uint32_t cur_bidx = 0;
+    for (int i = 0; i < F.num_steps; i++) {
+      const F3 s = floor3(pos * F.inv_voxel);
+      if (s.x < size_f && s.y < size_f && s.z < size_f && s.x >= 0 && s.y >= 0 && s.z >= 0) {
+        const I3 v = to_i3(s);
+        const int key = (v.x >> 3) | ((v.y >> 3) << 10) | ((v.z >> 3) << 20);
+        if (key != cur_key) {  // a new block along the ray: look it up once
+          cur_key = key;
+          cur_bidx = (uint32_t)morton3(v.x >> 3, v.y >> 3, v.z >> 3);
+          cur_slot = V.block_tab[cur_bidx];
+          if (cur_slot >= 0) pool.active[cur_slot] = 1;
         }
-        ++count;
-        last_order = (unsigned)p * (unsigned)F.num_steps + (unsigned)i;
-        last_idx = bidx;
+        if (cur_slot < 0) {
+          if ((int)cur_bidx == run_idx) {
+            ++run_len;
+          } else {
+            if (run_len) atomicAdd(&V.req[run_idx], (uint32_t)run_len);
+            run_idx = (int)cur_bidx;
+            run_len = 1;
+          }
+          ++count;
+          last_order = (unsigned)p * (unsigned)F.num_steps + (unsigned)i;
+          last_idx = cur_bidx;
+        }
       }
+      pos = pos + step;
     }
-    pos = pos + step;
+    if (run_len) atomicAdd(&V.req[run_idx], (uint32_t)run_len);
   }
-  if (run_len) atomicAdd(&V.req[run_idx], (uint32_t)run_len);
-  if (count) {
-    atomicAdd(V.emit_total, (unsigned long long)count);
-    atomicMax(V.last_emit, ((unsigned long long)last_order << 32) | last_idx);
+  // one emission-count and one last-emission atomic per warp
+  unsigned long long last = count ? (((unsigned long long)last_order << 32) | last_idx) : 0ULL;
+  unsigned long long tot = count;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, last, o);
+    last = other > last ? other : last;
+  }
+  if ((threadIdx.x & 31) == 0 && tot) {
+    atomicAdd(V.emit_total, tot);
+    atomicMax(V.last_emit, last);
   }
 }
 
@@ -259,6 +271,8 @@ __device__ __forceinline__ void sdf_update(const SdfArgs& a, const float* mask, 
 // projective_functor::update_block, lib/functors/projective_functor.hpp:73-111.
 // One CTA of 256 threads per visited block, two voxels per thread (v and
 // v + 256, i.e. z and z + 4): every field plane is read and written coalesced.
+// The two voxels are processed in phases (project both, fetch both pixels,
+// fetch both voxels' fields, update, store) so their memory accesses overlap.
 // Field planes are only touched for voxels that pass the update test.
 __global__ void __launch_bounds__(256)
 integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
@@ -267,6 +281,8 @@ integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
   const int n = *visit_count;
   const M4 K = camera_matrix(k);
   const float wlim = args.W - 1.5f, hlim = args.H - 1.5f;
+  const int W = args.W;
+  const float mu = args.mu, maxweight = args.maxweight;
   for (int item = blockIdx.x; item < n; item += gridDim.x) {
     const int slot = visit[item];
     const int4 m = pool.meta[slot];
@@ -274,27 +290,118 @@ integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
     const InstFrame& F = frames[m.w];
     const float vs = V.dim / V.size;
     const float* mask = args.masks + (size_t)m.w * args.W * args.H;
-    bool visible = false;
+    bool vis[2], upd[2];
+    F3 pos[2];
+    int pix[2];
+    // phase 1: voxel -> pixel
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int v = threadIdx.x + half * 256;
+    for (int h = 0; h < 2; ++h) {
+      const int v = threadIdx.x + h * 256;
       const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
       const F3 start = xform(F.Tcw, mk3(m.x * vs, (m.y + y) * vs, (m.z + z) * vs));
       const F3 camerastart = xform(K, start);
       const F3 cv = camerastart + ((float)x * F.cam_delta);
-      const F3 pos = start + ((float)x * F.delta);
-      if (pos.z < 0.0001f) continue;
+      pos[h] = start + ((float)x * F.delta);
+      vis[h] = false;
+      pix[h] = 0;
+      if (pos[h].z < 0.0001f) continue;
       const float inv = 1.f / cv.z;
       const float pxf = cv.x * inv + 0.5f, pyf = cv.y * inv + 0.5f;
       if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) continue;
-      visible = true;
-      const size_t o = (size_t)slot * 512 + v;
-      sdf_update(args, mask, pos, pxf, pyf, pool.tsdf[o], pool.wt[o], &pool.r[o], &pool.g[o],
-                 &pool.b[o], pool.c[o], pool.fg[o], pool.w[o]);
+      vis[h] = true;
+      pix[h] = (int)((unsigned)pxf + W * (unsigned)pyf);
     }
-    const int any = __syncthreads_or(visible);
+    // phase 2: depth / mask at the pixel, the update test of sdf_update
+    float depthS[2], mval[2], sdf[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      depthS[h] = vis[h] ? __ldg(args.depth + pix[h]) : 0.f;
+      mval[h] = vis[h] ? __ldg(mask + pix[h]) : -1.f;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      upd[h] = false;
+      sdf[h] = 0.f;
+      if (!vis[h] || depthS[h] <= 0 || mval[h] < 0) continue;
+      const F3 p = pos[h];
+      const float diff = (depthS[h] - p.z) * sqrtf(1 + sq(p.x / p.z) + sq(p.y / p.z));
+      if (diff > -mu) {
+        upd[h] = true;
+        sdf[h] = fmn(1.f, diff / mu);
+      }
+    }
+    // phase 3: read-modify-write of the voxels that update
+    float t[2], wt[2], r[2], g[2], b[2];
+    int c[2], w[2];
+    double fg[2];
+    F3 rgb[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!upd[h]) continue;
+      const size_t o = (size_t)slot * 512 + threadIdx.x + h * 256;
+      t[h] = pool.tsdf[o]; wt[h] = pool.wt[o]; r[h] = pool.r[o]; g[h] = pool.g[o];
+      b[h] = pool.b[o]; c[h] = pool.c[o]; fg[h] = pool.fg[o]; w[h] = pool.w[o];
+      rgb[h] = args.rgb[pix[h]];
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (!upd[h]) continue;
+      // sdf_update, apps/kfusion/src/cpp/kfusion/mapping_impl.hpp:26-46
+      const float x = clampf((wt[h] * t[h] + sdf[h]) / (wt[h] + 1), -1.f, 1.f);
+      const float y = fmn(wt[h] + 1, maxweight);
+      const int cc = c[h];
+      const float nr = (rgb[h].x + r[h] * cc) / (cc + 1);
+      const float ng = (rgb[h].y + g[h] * cc) / (cc + 1);
+      const float nb = (rgb[h].z + b[h] * cc) / (cc + 1);
+      const int ww = w[h];
+      const double nfg = ((double)mval[h] + fg[h] * ww) / (ww + 1);
+      const size_t o = (size_t)slot * 512 + threadIdx.x + h * 256;
+      pool.tsdf[o] = x; pool.wt[o] = y; pool.r[o] = nr; pool.g[o] = ng; pool.b[o] = nb;
+      pool.c[o] = cc + 1; pool.fg[o] = nfg; pool.w[o] = ww + 1;
+    }
+    const int any = __syncthreads_or(vis[0] || vis[1]);
     if (threadIdx.x == 0) pool.active[slot] = any ? 1 : 0;
   }
+}
+
+// Work counts of update_block for the roofline: voxels whose pixel is read
+// (visible: depth and mask fetched) and voxels updated (fields read + written).
+__global__ void __launch_bounds__(256)
+integrate_count_kernel(Pool pool, const Volume* __restrict__ vols,
+                       const InstFrame* __restrict__ frames, SdfArgs args, F4 k,
+                       const int* __restrict__ visit, const int* __restrict__ visit_count,
+                       unsigned long long* __restrict__ counts) {
+  const int n = *visit_count;
+  const M4 K = camera_matrix(k);
+  const float wlim = args.W - 1.5f, hlim = args.H - 1.5f;
+  unsigned long long nvis = 0, nupd = 0;
+  for (int item = blockIdx.x; item < n; item += gridDim.x) {
+    const int slot = visit[item];
+    const int4 m = pool.meta[slot];
+    const Volume& V = vols[m.w];
+    const InstFrame& F = frames[m.w];
+    const float vs = V.dim / V.size;
+    const float* mask = args.masks + (size_t)m.w * args.W * args.H;
+    for (int h = 0; h < 2; ++h) {
+      const int v = threadIdx.x + h * 256;
+      const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
+      const F3 start = xform(F.Tcw, mk3(m.x * vs, (m.y + y) * vs, (m.z + z) * vs));
+      const F3 cv = xform(K, start) + ((float)x * F.cam_delta);
+      const F3 p = start + ((float)x * F.delta);
+      if (p.z < 0.0001f) continue;
+      const float inv = 1.f / cv.z;
+      const float pxf = cv.x * inv + 0.5f, pyf = cv.y * inv + 0.5f;
+      if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) continue;
+      ++nvis;
+      const int pix = (int)((unsigned)pxf + args.W * (unsigned)pyf);
+      const float d = args.depth[pix];
+      if (d <= 0 || mask[pix] < 0) continue;
+      const float diff = (d - p.z) * sqrtf(1 + sq(p.x / p.z) + sq(p.y / p.z));
+      if (diff > -args.mu) ++nupd;
+    }
+  }
+  atomicAdd(&counts[0], nvis);
+  atomicAdd(&counts[1], nupd);
 }
 
 // projective_functor::update_node, lib/functors/projective_functor.hpp:113-137,
@@ -448,6 +555,59 @@ int stage_alloc(Context* ctx, const IdList& ids) {
   alloc_commit_kernel<<<dim3(div_up(max_tab, 256), ids.n), 256, 0, ctx->stream>>>(
       ctx->d_vols, ctx->d_frames, ids, ctx->pool, ctx->d_status);
   MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// Timing and algorithmic bytes of integrate_blocks_kernel on the current
+// frame (re-integrates the frame `reps` times; used after the timed region).
+int profile_integrate(Context* ctx, int reps, double* us, double* bytes) {
+  const int n = (int)ctx->inst.size();
+  IdList all;
+  all.n = n;
+  for (int i = 0; i < n; ++i) all.v[i] = i;
+  const mf_config& c = ctx->cfg;
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  uint32_t mask = 0;
+  for (int i = 0; i < n; ++i) mask |= 1u << i;
+  MF_CUDA(cudaMemsetAsync(ctx->d_visit_count, 0, sizeof(int), ctx->stream));
+  visit_list_kernel<<<div_up(ctx->pool.cap, 256), 256, 0, ctx->stream>>>(
+      ctx->pool, ctx->d_vols, ctx->d_frames, mask, ctx->W, ctx->H, ctx->d_visit,
+      ctx->d_visit_count);
+  SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
+  const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  unsigned long long* d_cnt = nullptr;
+  MF_CUDA(cudaMalloc(&d_cnt, 2 * sizeof(unsigned long long)));
+  MF_CUDA(cudaMemsetAsync(d_cnt, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  integrate_count_kernel<<<sms * 8, 256, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
+                                                          a, k, ctx->d_visit, ctx->d_visit_count,
+                                                          d_cnt);
+  unsigned long long cnt[2] = {0, 0};
+  int nv = 0;
+  MF_CUDA(cudaMemcpyAsync(cnt, d_cnt, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(&nv, ctx->d_visit_count, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, ctx->stream);
+  for (int r = 0; r < reps; ++r)
+    integrate_blocks_kernel<<<sms * 8, 256, 0, ctx->stream>>>(ctx->pool, ctx->d_vols,
+                                                             ctx->d_frames, a, k, ctx->d_visit,
+                                                             ctx->d_visit_count);
+  cudaEventRecord(e1, ctx->stream);
+  MF_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_cnt);
+  MF_CUDA(cudaGetLastError());
+  *us = 1e3 * ms / reps;
+  // per visible voxel: depth + mask (8 B); per updated voxel: the 36-byte field
+  // payload read and written and the pixel's rgb (12 B); per block: slot + meta.
+  *bytes = 8.0 * cnt[0] + (36.0 + 36.0 + 12.0) * cnt[1] + 20.0 * nv;
   return MF_OK;
 }
 

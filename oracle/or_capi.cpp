@@ -100,4 +100,18 @@ void or_raycast_objects(void** vols, const float* Two, const int* labels, int n,
                       F4{k4[0], k4[1], k4[2], k4[3]}, W, H, nearp, farp, mu, eps);
 }
 
+// Unit-level entry points for the reference's own unit tests.
+int or_unique_multiscale(uint64_t* keys, int n, uint64_t level_mask, int cur_level) {
+  return cur_level < 0 ? unique_multiscale(keys, n, level_mask)
+                       : unique_multiscale_level(keys, n, level_mask, (unsigned)cur_level);
+}
+uint64_t or_encode(int x, int y, int z, int level, int max_depth) {
+  return encode(x, y, z, level, max_depth);
+}
+uint64_t or_morton(unsigned x, unsigned y, unsigned z) { return morton(x, y, z); }
+void or_unpack(uint64_t code, unsigned* xyz) { unpack(code, xyz[0], xyz[1], xyz[2]); }
+float or_bilinear(const float* img, int w, float x, float y) {
+  return bilinear(img, w, F2{x, y});
+}
+
 }  // extern "C"

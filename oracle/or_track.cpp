@@ -132,6 +132,7 @@ static void bilateral(std::vector<T>& out, const std::vector<T>& in, int W, int 
                       const T* gaussian, T e_d, int r) {
   const T e2 = e_d * e_d * 2;
   out.assign((size_t)W * H, T(0));
+#pragma omp parallel for schedule(static)
   for (int y = 0; y < H; ++y)
     for (int x = 0; x < W; ++x) {
       const int pos = x + y * W;
@@ -393,6 +394,7 @@ void Tracker<T>::camera_sums(int level, const M4<T>& T_w_l, const M4<T>& T_w_r,
   const M4<T> KL = camera_matrix<T>(T(p.k[0]) / dl, T(p.k[1]) / dl, T(p.k[2]) / dl, T(p.k[3]) / dl);
   std::vector<Row> icp((size_t)w * h), rgb((size_t)w * h);
   const M4<T> inv_l = inverse(T_w_l);
+#pragma omp parallel for schedule(static)
   for (int y = 0; y < h; ++y)
     for (int x = 0; x < w; ++x) {
       const int i = x + y * w;
@@ -511,6 +513,7 @@ void Tracker<T>::object_sums(int level, const M4<T>& T_c2_o2, const M4<T>& T_c1_
   const M4<T> KL = camera_matrix<T>(T(p.k[0]) / dl, T(p.k[1]) / dl, T(p.k[2]) / dl, T(p.k[3]) / dl);
   std::vector<Row> icp((size_t)w * h), rgb((size_t)w * h);
   const M4<T> inv_c2o2 = inverse(T_c2_o2);
+#pragma omp parallel for schedule(static)
   for (int y = 0; y < h; ++y)
     for (int x = 0; x < w; ++x) {
       const int i = x + y * w;

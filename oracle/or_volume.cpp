@@ -44,7 +44,7 @@ bool Volume::child_exists(int level, int cx, int cy, int cz, int child) const {
 }
 
 // lib/algorithms/unique.hpp:49-71
-static int unique_multiscale(key_t* keys, int n, key_t level_mask) {
+int unique_multiscale(key_t* keys, int n, key_t level_mask) {
   int end = 1;
   const key_t key_mask = ~level_mask;
   if (n < 2) return end;
@@ -58,7 +58,7 @@ static int unique_multiscale(key_t* keys, int n, key_t level_mask) {
   return end;
 }
 // lib/algorithms/unique.hpp:73-98
-static int unique_multiscale_level(key_t* keys, int n, key_t level_mask, unsigned cur) {
+int unique_multiscale_level(key_t* keys, int n, key_t level_mask, unsigned cur) {
   int end = 1;
   const key_t key_mask = ~level_mask;
   if (n < 2) return end;
@@ -218,8 +218,10 @@ void integrate(Volume& vol, const float* depth, const F3* rgb, const float* mask
     if (vol.blocks[i].active || in_frustum(vol.blocks[i], vs, KT, W, H)) active.push_back(i);
   const F3 delta = rotate(Tcw, mk3(vs, 0, 0));
   const F3 cameraDelta = rotate(K, delta);
-  for (int bi : active) {
-    Block& B = vol.blocks[bi];
+  // blocks are independent (projective_functor.hpp:144 parallelises the same loop)
+#pragma omp parallel for schedule(dynamic, 16)
+  for (size_t ai = 0; ai < active.size(); ++ai) {
+    Block& B = vol.blocks[active[ai]];
     bool visible = false;
     for (unsigned z = B.cz; z < (unsigned)B.cz + 8; ++z)
       for (unsigned y = B.cy; y < (unsigned)B.cy + 8; ++y) {
@@ -239,7 +241,9 @@ void integrate(Volume& vol, const float* depth, const F3* rgb, const float* mask
       }
     B.active = visible;
   }
-  for (Node& N : vol.nodes) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (size_t ni = 0; ni < vol.nodes.size(); ++ni) {
+    Node& N = vol.nodes[ni];
     unsigned ux, uy, uz; unpack(N.code, ux, uy, uz);  // includes the level bits
     const F3 voxel = mk3((float)(int)ux, (float)(int)uy, (float)(int)uz);
     const F3 d = rotate(Tcw, mk3(0.5f * vs * N.side));
@@ -494,6 +498,8 @@ void raycast_object_list(const RaycastInstance* inst, int n, F3* vertex, F3* nor
   const M4 view = mul(T_w_c, inverse_camera_matrix(k));
   std::vector<M4> inv(n);
   for (int i = 0; i < n; ++i) inv[i] = inverse(inst[i].T_w_o);
+  // pixels are independent (rendering.cpp:18 parallelises the same loop)
+#pragma omp parallel for schedule(dynamic, 4)
   for (int y = 0; y < H; ++y)
     for (int x = 0; x < W; ++x) {
       const int p = x + y * W;

@@ -94,7 +94,8 @@ struct Volume {
   void alloc_update(key_t* keys, int n);
 };
 
-struct AllocResult { unsigned count; };
+int unique_multiscale(key_t* keys, int n, key_t level_mask);
+int unique_multiscale_level(key_t* keys, int n, key_t level_mask, unsigned cur);
 unsigned build_volume_allocation_list(Volume& vol, const float* depth, const float* mask,
                                       int W, int H, const M4& T_w_c, const M4& T_w_o,
                                       const M4& K, float band);

@@ -1,0 +1,64 @@
+"""The C ABI library on a machine without a GPU: it loads, exports every entry
+point include/midfusion_b200.h declares, and fails loudly (an error code, no
+CPU fallback) when asked to create a context without a device."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from mid_fusion_b200 import build, capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if f.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", f)).read()
+            names |= set(re.findall(r"^\s*(?:int|const char\*)\s+(mf_\w+)\s*\(", txt, re.M))
+    return names
+
+
+@pytest.fixture(scope="module")
+def lib():
+    build.build()
+    return capi.load()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared()
+    assert len(names) >= 30
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(capi.EXPORTS) == names
+
+
+def test_config_defaults(lib):
+    cfg = capi.MfConfig()
+    assert lib.mf_config_default(C.byref(cfg), 640, 480) == 0
+    assert (cfg.width, cfg.height) == (640, 480)
+    assert list(cfg.gn_iterations)[:3] == [10, 5, 4]
+    assert abs(cfg.mu - 0.1) < 1e-7 and cfg.max_weight == 100
+    assert abs(cfg.k[0] - 525.0) < 1e-4 and abs(cfg.k[2] - 319.5) < 1e-4
+    assert lib.mf_config_default(None, 640, 480) == -1
+
+
+def test_create_without_device_fails_loudly(lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cfg = capi.MfConfig()
+    lib.mf_config_default(C.byref(cfg), 64, 48)
+    h = C.c_void_p()
+    rc = lib.mf_create(C.byref(cfg), C.byref(h))
+    assert rc == -2 and not h.value  # MF_E_CUDA, no context, no fallback
+
+
+def test_bad_arguments_are_rejected(lib):
+    cfg = capi.MfConfig()
+    lib.mf_config_default(C.byref(cfg), 64, 48)
+    cfg.max_instances = 1000
+    h = C.c_void_p()
+    assert lib.mf_create(C.byref(cfg), C.byref(h)) == -1

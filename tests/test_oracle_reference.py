@@ -1,0 +1,86 @@
+"""The oracle against the reference compiled from its own sources (CPU only;
+skipped where oracle/_ref was not built, e.g. without the reference tree)."""
+import numpy as np
+import pytest
+
+import _oracle as O
+from mid_fusion_b200.scene import generalize_masks, make_scene
+
+ref = O.reference()
+pytestmark = pytest.mark.skipif(ref is None, reason="oracle/_ref not built (no reference tree)")
+
+
+@pytest.mark.parametrize("seed", [3, 8])
+def test_oracle_matches_reference_sequence(seed):
+    W, H = 128, 96
+    s = make_scene("multi", W, H, n_frames=3, seed=seed, bg_size=128, obj_size=64, n_objects=2)
+    ref.lib.ref_pin_epsilon(s.instances[0].size)
+    orc = O.oracle()
+    labels = [i.label for i in s.instances]
+    vo = [orc.volume(i.size, i.dim) for i in s.instances]
+    vr = [ref.volume(i.size, i.dim) for i in s.instances]
+    bo = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+    br = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+    for f in range(3):
+        d, rgb, lab = s.render(f)
+        masks = generalize_masks(lab, labels)
+        poses = s.volume_poses(f)
+        T = s.cam_poses[f].astype(np.float32)
+        rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+        for i in range(len(labels)):
+            a = vo[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, 0.1)
+            b = vr[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, 0.1)
+            assert a == b
+            ko, co, ao, xo = vo[i].blocks()
+            kr, cr, ar, xr = vr[i].blocks()
+            assert np.array_equal(ko, kr) and np.array_equal(co, cr) and np.array_equal(ao, ar)
+            assert xo.tobytes() == xr.tobytes()
+            no, so, cmo, nvo = vo[i].nodes()
+            nr, sr, cmr, nvr = vr[i].nodes()
+            assert np.array_equal(no, nr) and np.array_equal(cmo, cmr) and np.array_equal(so, sr)
+            assert nvo.tobytes() == nvr.tobytes()
+            assert vo[i].root_children() == vr[i].root_children()
+        orc.raycast_objects(vo, poses, labels, T, s.k, W, H, eps_size=s.instances[0].size,
+                            vertex=bo[0], normal=bo[1], label_img=bo[2])
+        ref.raycast_objects(vr, poses, labels, T, s.k, W, H, vertex=br[0], normal=br[1],
+                            label_img=br[2])
+        # A ray that enters a volume exactly on its far face samples coordinate
+        # == size; the reference's bit descent aliases that to block 0 and reads
+        # past the end of the block's voxel array (lib/octree.hpp:359-379,
+        # lib/node.hpp:144-149), i.e. another block's memory.  The oracle and
+        # the device read such samples as unallocated.  Those few pixels (and
+        # the later frames' copies of them) are the only tolerated differences.
+        bad = np.any(bo[0] != br[0], axis=-1) | np.any(bo[1] != br[1], axis=-1) | (bo[2] != br[2])
+        assert bad.sum() <= max(3, 3e-4 * bad.size), bad.sum()
+        for a, b in zip(bo, br):
+            b[...] = a  # continue from the same maps
+
+
+def test_alloc_update_multiscale_keys_match_reference():
+    blocks = [(56, 12, 12), (56, 12, 15), (128, 128, 128), (128, 128, 125), (128, 128, 127),
+              (128, 136, 129), (128, 136, 127), (136, 128, 136), (128, 240, 136), (128, 241, 136)]
+    levels = [5, 5, 3, 5, 4, 5, 5, 5, 5, 5]
+    keys = np.array([O.encode(x, y, z, l, 8) for (x, y, z), l in zip(blocks, levels)], np.uint64)
+    orc = O.oracle()
+    a, b = orc.volume(256, 2.56), ref.volume(256, 2.56)
+    a.alloc_update(keys)
+    b.alloc_update(keys)
+    assert np.array_equal(a.blocks(False)[0], b.blocks(False)[0])
+    na, nb = a.nodes(False), b.nodes(False)
+    assert np.array_equal(na[0], nb[0]) and np.array_equal(na[2], nb[2])
+
+
+def test_interp_and_grad_match_reference():
+    s = make_scene("room", 96, 72, n_frames=1, seed=4, bg_size=128)
+    orc = O.oracle()
+    a, b = orc.volume(128, 5.12), ref.volume(128, 5.12)
+    d, rgb, lab = s.render(0)
+    m = generalize_masks(lab, [0])[0]
+    rgb3 = rgb.astype(np.float32) / np.float32(255)
+    for v in (a, b):
+        v.integrate(d, rgb3, m, s.cam_poses[0], np.eye(4), s.k, 0.1)
+    rng = np.random.default_rng(1)
+    for p in rng.uniform(0.5, 4.6, size=(400, 3)).astype(np.float32):
+        assert a.interp(p, 0) == b.interp(p, 0)
+        assert a.interp(p, 1) == b.interp(p, 1)
+        assert np.array_equal(a.grad(p), b.grad(p))
