@@ -267,7 +267,7 @@ def run_reference(args):
     value = len(t) / total
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "frames/s",
-        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "device": "host cores only", "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(1e3 * total / len(t), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4},
@@ -293,13 +293,27 @@ def traffic_from_profiles(name):
 
 
 def reduce_max(x, world):
+    """Max over ranks (device time of the slowest rank); NCCL tensors live on the
+    GPU, gloo ones on the host."""
     if world <= 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def whole_job(totals, steps, world):
+    """Whole-job frames/s per timed path: every rank runs `steps` frames of its own
+    sequence (weak scaling), so the job processed steps * world frames in the
+    time of the slowest rank."""
+    out = {}
+    for k, v in totals.items():
+        t = reduce_max(v, world)
+        out[k] = (t, steps * world / t)
+    return out
 
 
 def main():
@@ -336,11 +350,9 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    total_b = reduce_max(r["total_b"], world)
-    total_p = reduce_max(r["total_p"], world)
-    total_e = reduce_max(r["total_e"], world)
-    frames = args.steps * world
-    value = frames / total_b
+    agg = whole_job({"b": r["total_b"], "p": r["total_p"], "e": r["total_e"]}, args.steps,
+                    world)
+    (total_b, value), (total_p, value_p), (total_e, value_e) = agg["b"], agg["p"], agg["e"]
     hbm, peak_kind = measured_peaks()
     prof = r["prof"]
     gbs = lambda nbytes, us: nbytes / (us * 1e-6) / 1e9
@@ -361,7 +373,10 @@ def main():
                                     "algorithmic_bytes_per_launch": int(prof["integrate_bytes"]),
                                     "traffic": traffic_from_profiles(
                                         "integrate_blocks_kernel_640x480.md")},
-        "raycast_objects_kernel": {"us_per_launch": round(prof["raycast_us"], 2)},
+        "raycast_objects_kernel": {"us_per_launch": round(prof["raycast_us"], 2),
+                                   "bound": "instruction fetch (ncu: no_instruction stalls)",
+                                   "traffic": traffic_from_profiles(
+                                       "raycast_objects_kernel_640x480.md")},
     }
     per_frame = (r["stats"] or {}).get("graph_kernels", 0) + 1  # graph + rgb conversion
     launches = per_frame * args.steps
@@ -382,12 +397,12 @@ def main():
         "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4,
                    "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "plain": {"value": round(frames / total_p, 2), "unit": "frames/s",
+        "plain": {"value": round(value_p, 2), "unit": "frames/s",
                   "ms_per_step": round(1e3 * total_p / args.steps, 4)},
         "batched_over_plain": round(total_p / total_b, 3),
         "pose_diff_batched_vs_plain_m": r["dpos"],
         "camera_err_vs_gt_m": r["gt_err"],
-        "e2e": {"value": round(frames / total_e, 2), "unit": "frames/s",
+        "e2e": {"value": round(value_e, 2), "unit": "frames/s",
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]},
         "roofline": roofline,
         "rooflines_other": others,

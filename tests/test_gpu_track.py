@@ -5,8 +5,9 @@
   whose last bits differ between CUDA and glibc, so values are compared within
   a few float ulps and the validity masks exactly.
 * Normal equations (the 32 reduceKernel sums) at fixed poses against the
-  all-FP64 oracle: the GPU evaluates residuals in FP32 and reduces with Kahan /
-  FP64, so sums agree to ~1e-5 relative and the inlier count exactly up to
+  all-FP64 oracle: the GPU evaluates residuals in FP32, sums at most four rows
+  per thread in FP32 and reduces in FP64 from the warp level up, so sums agree
+  to ~1e-5 relative and the inlier count exactly up to
   a handful of threshold flips.
 * Full coarse-to-fine Gauss-Newton (camera and objects, batched device GN and
   the host-driven plain path) against the all-FP64 oracle from the same
