@@ -146,6 +146,23 @@ int mf_track_info(mf_context* ctx, int slot, int* iterations, double* sums, doub
  * tracking.cpp:1191-1352) of a problem at `level` and at `pose` (NULL: its
  * current pose), without a GN step. */
 int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, double* sums);
+/* No counterpart in the reference.  mf_track_eval without any device memory
+ * allocation, for callers that must not allocate while they run: a real-time
+ * tracking loop with a fixed memory budget, or a host that has handed the rest
+ * of the device memory to other work.  Its scratch (FP64 per-CTA partials, the
+ * 32 sums and a CTA ticket) is one static device array of 1 MiB + 512 B, so a
+ * level may have at most 4096 x 512 pixels at level 0 and 4096 x 256 above
+ * (larger levels return MF_E_ARG).  The pose is passed to the kernel by value
+ * and the context's tracking state is not modified.  Same results as
+ * mf_track_eval, bit for bit.
+ *  - The first call on a device looks up the scratch's device address; make
+ *    it (for example once at start-up) before any stream capture.
+ *  - The context's device must be the current device.
+ *  - The scratch is shared by every context on the device: calls that overlap
+ *    in time (other threads, other contexts) race on it and give wrong sums.
+ *    Calls from one thread are serialised, because the call synchronises. */
+int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose,
+                         double* sums);
 /* Pyramid planes of the current frame: which 0 depth, 1 intensity, 2 vertex,
  * 3 normal, 4 x-gradient, 5 y-gradient, 6 ICP covariance, 7 camera reference
  * vertex (float3 planes are 3 floats per pixel). */

@@ -34,7 +34,7 @@ EXPORTS = [
     "mf_preprocess", "mf_set_ref_from_current", "mf_track_camera", "mf_track_objects",
     "mf_track_info", "mf_track_eval", "mf_download_pyramid", "mf_process_frame",
     "mf_process_frame_device", "mf_get_poses", "mf_frame_stats", "mf_set_graphs",
-    "mf_profile",
+    "mf_profile", "mf_track_eval_static",
 ]
 
 
@@ -238,6 +238,14 @@ class Context:
         p = None if pose is None else _m4(pose)
         self._check(self.lib.mf_track_eval(self.h, slot, level, _ptr(p, np.float32),
                                            _ptr(sums, np.float64)))
+        return sums
+
+    def track_eval_static(self, slot, level, pose=None):
+        """mf_track_eval with static device scratch (allocates nothing)."""
+        sums = np.zeros(32, np.float64)
+        p = None if pose is None else _m4(pose)
+        self._check(self.lib.mf_track_eval_static(self.h, slot, level, _ptr(p, np.float32),
+                                                  _ptr(sums, np.float64)))
         return sums
 
     def pyramid(self, level, which):

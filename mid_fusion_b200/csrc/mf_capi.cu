@@ -547,6 +547,14 @@ int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, doubl
   return track_eval(ctx, slot, level, pose, sums);
 }
 
+int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose,
+                         double* sums) {
+  if (check(ctx) || !sums || slot < 0 || slot >= ctx->cfg.max_instances || level < 0 ||
+      level >= ctx->cfg.pyramid_levels)
+    return MF_E_ARG;
+  return track_eval_static(ctx, slot, level, pose, sums);
+}
+
 int mf_download_pyramid(mf_context* ctx, int level, int which, float* out) {
   if (check(ctx) || !out || level < 0 || level >= ctx->cfg.pyramid_levels) return MF_E_ARG;
   return track_download_level(ctx, level, which, out);

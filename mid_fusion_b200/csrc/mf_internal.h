@@ -126,6 +126,7 @@ int track_camera(Context* ctx, uint32_t moving);
 int track_objects(Context* ctx, const IdList& ids);
 int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
+int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int track_download_level(Context* ctx, int L, int which, float* out);
 void track_save_prev_camera(Context* ctx);
 bool track_has_ref(Context* ctx);

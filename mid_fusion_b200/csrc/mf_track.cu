@@ -18,6 +18,8 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 #include "mf_internal.h"
 #include "mf_solve.cuh"
@@ -1054,6 +1056,179 @@ int track_download_level(Context* ctx, int L, int which, float* out) {
     default: return MF_E_ARG;
   }
   MF_CUDA(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+// ------------------------------------------------------------------------
+// Normal-equation evaluation that allocates nothing (mf_track_eval_static).
+//
+// Same sums as track_eval (the per-pixel rows and the FP64 reduction of
+// gn_iter_kernel, in the same order, so the two agree bit for bit), but the
+// scratch -- the per-CTA FP64 partials, the 32 result sums and the CTA ticket
+// -- is the file-scope array below, not a cudaMalloc'd buffer, and the pose is
+// a kernel argument, so the context's GN state is not touched either.
+// Layout of the array (bytes):
+//   [0, EVAL_PARTIALS_BYTES)        double partials[EVAL_MAX_TILES][32]
+//   [EVAL_SUMS_OFF, +256)           double sums[32]
+//   [EVAL_TICKET_OFF, +4)           unsigned ticket (zeroed before each launch)
+// EVAL_MAX_TILES bounds the level's pixel count: 4096 CTAs x 512 pixels at
+// level 0 (2 097 152 px, e.g. 1920x1080) and 4096 x 256 above it.
+constexpr int EVAL_MAX_TILES = 4096;
+constexpr size_t EVAL_PARTIALS_BYTES = (size_t)EVAL_MAX_TILES * 32 * sizeof(double);
+constexpr size_t EVAL_SUMS_OFF = EVAL_PARTIALS_BYTES;
+constexpr size_t EVAL_TICKET_OFF = EVAL_SUMS_OFF + 32 * sizeof(double);
+constexpr size_t EVAL_SCRATCH_BYTES = EVAL_TICKET_OFF + 256;
+static __device__ __align__(256) unsigned char g_eval_scratch[EVAL_SCRATCH_BYTES];
+
+template <int KIND>
+__global__ void __launch_bounds__(GN_THREADS, 2)
+gn_eval_static_kernel(GNArgs a, int s, int L, int set_pose, M4 Tf, M4 invTf,
+                      unsigned char* scratch) {
+  // the problem's constants, with the pose to evaluate at, in shared memory
+  __shared__ GNState S;
+  {
+    static_assert(sizeof(GNState) % 4 == 0, "GNState is copied as words");
+    const int* src = reinterpret_cast<const int*>(&a.st[s]);
+    int* dst = reinterpret_cast<int*>(&S);
+    for (int i = threadIdx.x; i < (int)(sizeof(GNState) / 4); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && set_pose) {
+    S.Tf = Tf;
+    S.invTf = invTf;
+  }
+  __syncthreads();
+  double* partials = reinterpret_cast<double*>(scratch);
+  double* out = reinterpret_cast<double*>(scratch + EVAL_SUMS_OFF);
+  unsigned* ticket = reinterpret_cast<unsigned*>(scratch + EVAL_TICKET_OFF);
+
+  const int w = a.pyr.w[L], h = a.pyr.h[L];
+  const int n = w * h;
+  float acc[29];
+#pragma unroll
+  for (int i = 0; i < 29; ++i) acc[i] = 0.f;
+  int cnt[3] = {0, 0, 0};
+  const F3* rV = a.rV[s];
+  const int ppt = gn_pix(L);
+#pragma unroll 1
+  for (int k = 0; k < ppt; ++k) {
+    const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
+    if (p >= n) break;
+    Row r;
+    if (a.use_icp) {
+      r.result = 0;
+      if (KIND == 0) icp_camera(a, S, L, p, r);
+      else icp_object(a, S, L, p, r);
+      accumulate(acc, cnt, r, a.robust);
+    }
+    if (a.use_rgb) {
+      r.result = 0;
+      rgb_row(a, S, rV, L, p, w, h, r);
+      accumulate(acc, cnt, r, a.robust);
+    }
+  }
+  __shared__ double sh[GN_THREADS / 32][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    double v = i < 29 ? (double)acc[i] : (double)cnt[i - 29];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[warp][i] = v;
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x < 32) {
+    double v = 0;
+#pragma unroll
+    for (int wi = 0; wi < GN_THREADS / 32; ++wi) v += sh[wi][threadIdx.x];
+    partials[(size_t)blockIdx.x * 32 + threadIdx.x] = v;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  {
+    const int i = threadIdx.x & 31, g = threadIdx.x >> 5;
+    double v = 0;
+    for (int b = g; b < (int)gridDim.x; b += GN_THREADS / 32)
+      v += __ldcg(&partials[(size_t)b * 32 + i]);
+    sh[g][i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = 0;
+#pragma unroll
+    for (int g = 0; g < GN_THREADS / 32; ++g) v += sh[g][threadIdx.x];
+    out[threadIdx.x] = v;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// Device address of g_eval_scratch for each device, looked up once per device
+// with that device current, on the first call (host code cannot use the
+// address of a __device__ variable directly).
+static std::mutex g_eval_mutex;
+static unsigned char* g_eval_ptr[64] = {};
+
+static int eval_scratch_setup(Context* ctx, unsigned char** out) {
+  int dev = -1;
+  MF_CUDA(cudaGetDevice(&dev));
+  if (dev != ctx->device) {
+    ctx->last_error = "mf_track_eval_static: the context's device is not the current device";
+    return MF_E_STATE;
+  }
+  if (dev < 0 || dev >= 64) {
+    ctx->last_error = "mf_track_eval_static: device ordinal above 63";
+    return MF_E_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_eval_mutex);
+  if (!g_eval_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_eval_scratch);
+    if (e != cudaSuccess || !p) {
+      ctx->last_error = std::string("cudaGetSymbolAddress(g_eval_scratch): ") +
+                        cudaGetErrorString(e);
+      return MF_E_CUDA;
+    }
+    g_eval_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = g_eval_ptr[dev];
+  return MF_OK;
+}
+
+int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double* sums) {
+  const int tiles = div_up((long long)(ctx->W >> L) * (ctx->H >> L), GN_THREADS * gn_pix(L));
+  if (tiles > EVAL_MAX_TILES) {
+    ctx->last_error = "mf_track_eval_static: level has more than 4096 x " +
+                      std::to_string(GN_THREADS * gn_pix(L)) +
+                      " pixels (the static scratch holds 4096 CTA partials)";
+    return MF_E_ARG;
+  }
+  if (!ctx->track) return MF_E_STATE;
+  unsigned char* scratch = nullptr;
+  if (int rc = eval_scratch_setup(ctx, &scratch)) return rc;
+  M4 Tf{}, invTf{};
+  const int set_pose = pose16 ? 1 : 0;
+  if (pose16) {
+    std::memcpy(&Tf, pose16, 64);
+    invTf = inverse(Tf);
+  }
+  const GNArgs a = make_args(ctx, L, 0);
+  // the ticket must be zero when the launch starts (the last CTA also resets it)
+  MF_CUDA(cudaMemsetAsync(scratch + EVAL_TICKET_OFF, 0, sizeof(unsigned), ctx->stream));
+  if (slot == 0)
+    gn_eval_static_kernel<0><<<tiles, GN_THREADS, 0, ctx->stream>>>(a, slot, L, set_pose, Tf,
+                                                                     invTf, scratch);
+  else
+    gn_eval_static_kernel<1><<<tiles, GN_THREADS, 0, ctx->stream>>>(a, slot, L, set_pose, Tf,
+                                                                     invTf, scratch);
+  MF_CUDA(cudaGetLastError());
+  MF_CUDA(cudaMemcpyAsync(sums, scratch + EVAL_SUMS_OFF, 32 * sizeof(double),
+                          cudaMemcpyDeviceToHost, ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
   return MF_OK;
 }
