@@ -181,6 +181,7 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
   const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
   if (x >= a.W || y >= a.H) return;
   const int p = x + y * a.W;
+  __shared__ int s_slot[8 * 128];
   const float INVALID = -2;
   float nearest = 1.0e3f;
   double high_fg = 0.f;
@@ -216,7 +217,7 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
     high_fg = fg;
     a.label[p] = F.label;
     a.vertex[p] = xform(F.T_w_o, mk3(hit.x, hit.y, hit.z));
-    const F3 gn = volume_grad(pool, V, mk3(hit.x, hit.y, hit.z));
+    const F3 gn = volume_grad(pool, V, mk3(hit.x, hit.y, hit.z), s_slot + threadIdx.x, 128);
     if (length(gn) == 0) a.normal[p].x = INVALID;
     else a.normal[p] = normalize(rotate(F.T_w_o, gn));
   }

@@ -87,10 +87,9 @@ __device__ __forceinline__ float tsdf_at_m(const Pool& P, const Volume& V, Block
 // Octree::grad(pos, select), lib/octree.hpp:593-680: 48 reads through the
 // cached get(x, y, z, block), which falls back to the init value (not to the
 // node value) when a block is missing, i.e. get_fine semantics.  The taps span
-// at most 2 blocks per axis; their slots are resolved once.
-// Not inlined: called once per accepted hit; inlining its 48 taps into the
-// raycast loop overflows the instruction cache.
-static __device__ __noinline__ F3 volume_grad(const Pool& P, const Volume& V, F3 pos_m) {
+// at most 2 blocks per axis; their slots are resolved once.  General form,
+// used when the sample's voxel lies outside the volume (see volume_grad).
+static __device__ __noinline__ F3 volume_grad_generic(const Pool& P, const Volume& V, F3 pos_m) {
   const float inv = V.size / V.dim;
   const F3 pos = mk3(pos_m.x * inv, pos_m.y * inv, pos_m.z * inv);
   const F3 fl = floor3(pos);
@@ -151,6 +150,109 @@ static __device__ __noinline__ F3 volume_grad(const Pool& P, const Volume& V, F3
           ((G(lo.x, up.y, uu.z) - G(lo.x, up.y, lu.z)) * (1 - f.x) +
            (G(up.x, up.y, uu.z) - G(up.x, up.y, lu.z)) * f.x) * f.y) * f.z;
 #undef G
+  const float s = V.dim / V.size;
+  return gr * mk3(s, s, s) * 0.5f;
+}
+
+// Octree::grad with every tap inside the volume (the sample's voxel in
+// [0, size)): the 48 reads touch 32 distinct voxels, which are loaded once
+// each; per axis the four tap coordinates lie in at most two blocks, whose
+// eight combinations are resolved once and kept in shared memory (`st`, this
+// thread's column of a [8][stride] table).  Same expression, same float order.
+// Not inlined: called once per accepted hit, and the raycast loop around it
+// is bound by instruction fetch.
+static __device__ __noinline__ F3 volume_grad(const Pool& P, const Volume& V, F3 pos_m,
+                                              int* __restrict__ st, int stride) {
+  const float inv = V.size / V.dim;
+  const F3 pos = mk3(pos_m.x * inv, pos_m.y * inv, pos_m.z * inv);
+  const F3 fl = floor3(pos);
+  const I3 base = to_i3(fl);
+  const int s1 = V.size - 1;
+  if ((unsigned)base.x > (unsigned)s1 || (unsigned)base.y > (unsigned)s1 ||
+      (unsigned)base.z > (unsigned)s1)
+    return volume_grad_generic(P, V, pos_m);
+  const F3 f = mk3(pos.x - fl.x, pos.y - fl.y, pos.z - fl.z);
+  // tap coordinates ll, lu, ul, uu per axis (lo = lu, up = ul)
+  const int cx[4] = {imx(base.x - 1, 0), base.x, imn(base.x + 1, s1), imn(base.x + 2, s1)};
+  const int cy[4] = {imx(base.y - 1, 0), base.y, imn(base.y + 1, s1), imn(base.y + 2, s1)};
+  const int cz[4] = {imx(base.z - 1, 0), base.z, imn(base.z + 1, s1), imn(base.z + 2, s1)};
+  const int bx0 = cx[0] >> 3, by0 = cy[0] >> 3, bz0 = cz[0] >> 3;
+  const int bx1 = cx[3] >> 3, by1 = cy[3] >> 3, bz1 = cz[3] >> 3;
+#pragma unroll
+  for (int c = 0; c < 8; ++c)
+    st[c * stride] = V.block_tab[morton3((c & 1) ? bx1 : bx0, (c & 2) ? by1 : by0,
+                                         (c & 4) ? bz1 : bz0)];
+  int sx[4], sy[4], sz[4], ox[4], oy[4], oz[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    sx[i] = ((cx[i] >> 3) != bx0 ? 1 : 0) * stride;
+    sy[i] = ((cy[i] >> 3) != by0 ? 2 : 0) * stride;
+    sz[i] = ((cz[i] >> 3) != bz0 ? 4 : 0) * stride;
+    ox[i] = cx[i] & 7;
+    oy[i] = (cy[i] & 7) << 3;
+    oz[i] = (cz[i] & 7) << 6;
+  }
+  auto tap = [&](int xi, int yi, int zi) -> float {
+    const int sl = st[sx[xi] + sy[yi] + sz[zi]];
+    return sl < 0 ? 1.f : __ldg(P.tsdf + (size_t)sl * 512 + (ox[xi] + oy[yi] + oz[zi]));
+  };
+  const float t011 = tap(0, 1, 1);
+  const float t012 = tap(0, 1, 2);
+  const float t021 = tap(0, 2, 1);
+  const float t022 = tap(0, 2, 2);
+  const float t101 = tap(1, 0, 1);
+  const float t102 = tap(1, 0, 2);
+  const float t110 = tap(1, 1, 0);
+  const float t111 = tap(1, 1, 1);
+  const float t112 = tap(1, 1, 2);
+  const float t113 = tap(1, 1, 3);
+  const float t120 = tap(1, 2, 0);
+  const float t121 = tap(1, 2, 1);
+  const float t122 = tap(1, 2, 2);
+  const float t123 = tap(1, 2, 3);
+  const float t131 = tap(1, 3, 1);
+  const float t132 = tap(1, 3, 2);
+  const float t201 = tap(2, 0, 1);
+  const float t202 = tap(2, 0, 2);
+  const float t210 = tap(2, 1, 0);
+  const float t211 = tap(2, 1, 1);
+  const float t212 = tap(2, 1, 2);
+  const float t213 = tap(2, 1, 3);
+  const float t220 = tap(2, 2, 0);
+  const float t221 = tap(2, 2, 1);
+  const float t222 = tap(2, 2, 2);
+  const float t223 = tap(2, 2, 3);
+  const float t231 = tap(2, 3, 1);
+  const float t232 = tap(2, 3, 2);
+  const float t311 = tap(3, 1, 1);
+  const float t312 = tap(3, 1, 2);
+  const float t321 = tap(3, 2, 1);
+  const float t322 = tap(3, 2, 2);
+  F3 gr;
+  gr.x = (((t211 - t011) * (1 - f.x) +
+           (t311 - t111) * f.x) * (1 - f.y) +
+          ((t221 - t021) * (1 - f.x) +
+           (t321 - t121) * f.x) * f.y) * (1 - f.z) +
+         (((t212 - t012) * (1 - f.x) +
+           (t312 - t112) * f.x) * (1 - f.y) +
+          ((t222 - t022) * (1 - f.x) +
+           (t322 - t122) * f.x) * f.y) * f.z;
+  gr.y = (((t121 - t101) * (1 - f.x) +
+           (t221 - t201) * f.x) * (1 - f.y) +
+          ((t131 - t111) * (1 - f.x) +
+           (t231 - t211) * f.x) * f.y) * (1 - f.z) +
+         (((t122 - t102) * (1 - f.x) +
+           (t222 - t202) * f.x) * (1 - f.y) +
+          ((t132 - t112) * (1 - f.x) +
+           (t232 - t212) * f.x) * f.y) * f.z;
+  gr.z = (((t112 - t110) * (1 - f.x) +
+           (t212 - t210) * f.x) * (1 - f.y) +
+          ((t122 - t120) * (1 - f.x) +
+           (t222 - t220) * f.x) * f.y) * (1 - f.z) +
+         (((t113 - t111) * (1 - f.x) +
+           (t213 - t211) * f.x) * (1 - f.y) +
+          ((t123 - t121) * (1 - f.x) +
+           (t223 - t221) * f.x) * f.y) * f.z;
   const float s = V.dim / V.size;
   return gr * mk3(s, s, s) * 0.5f;
 }

@@ -336,6 +336,10 @@ MF_HD void gn_step(GNState& S, const double* s, int level) {
   S.invTf = inverse(Tf);
 }
 
+__device__ __noinline__ void gn_step_dev(GNState& S, const double* s, int level) {
+  gn_step(S, s, level);
+}
+
 // ------------------------------------------------------------------ residuals
 struct GNArgs {
   PyrPtrs pyr;
@@ -552,7 +556,7 @@ __device__ __forceinline__ void accumulate(float* acc, int* cnt, const Row& r, i
 // KIND 0: the camera problem; KIND 1: object problems (one instantiation each
 // keeps the kernel's code small).
 template <int KIND>
-__global__ void __launch_bounds__(GN_THREADS, 2)
+__global__ void __launch_bounds__(GN_THREADS, 3)
 gn_iter_kernel(GNArgs a, IdList slots, int L) {
   const int s = slots.v[blockIdx.y];
   GNState& S = a.st[s];
@@ -613,6 +617,7 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   {
     const int i = threadIdx.x & 31, g = threadIdx.x >> 5;  // 8 groups of tiles
     double v = 0;
+#pragma unroll 8
     for (int b = g; b < (int)gridDim.x; b += GN_THREADS / 32)
       v += __ldcg(&a.partials[((size_t)s * a.max_tiles + b) * 32 + i]);
     sh[g][i] = v;
@@ -629,7 +634,7 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   __syncthreads();
   if (threadIdx.x == 0) {
     S.ticket = 0;
-    if (a.device_step) gn_step(S, tot, L);
+    if (a.device_step) gn_step_dev(S, tot, L);
   }
 }
 
