@@ -319,7 +319,12 @@ def _smooth_path(rng, n, base, target, max_step=0.009, max_rot_deg=0.9):
 def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_objects=3,
                bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512, noise=True):
     """``preset='room'``: one static room (plain method, one octree).
-    ``preset='multi'``: background room + moving rigid objects, one octree each."""
+    ``preset='multi'``: background room + moving rigid objects, one octree each.
+    ``preset='uneven'``: background room + ``n_objects`` (default use: 12) rigid
+    primitives of seeded kinds and sizes (0.05-0.4 m), each with its own octree
+    of 32^3, 64^3, 128^3 or 256^3 voxels at 2-5 mm; the largest object sits in
+    the centre at 0.8 m, the others on an ellipse around it 1.2-1.9 m away,
+    sized so that their target mask areas span 0.5 %-25 % of the frame."""
     rng = np.random.default_rng(seed)
     scale = width / 640.0
     k = (525.0 * scale, 525.0 * scale, (width - 1) / 2.0, (height - 1) / 2.0)
@@ -361,4 +366,41 @@ def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_ob
             sh = Shape(kind, size, p, rng.uniform(0.3, 1.0, 3), label=i + 1, twist=tw)
             movers.append(sh)
             instances.append(Instance(i + 1, obj_size, obj_dim, sh))
+    elif preset == "uneven":
+        cam0 = cams[0]
+        fpx = k[0]
+        # target mask areas, log-uniform over [0.5 %, 25 %] of the frame, the
+        # largest object nearest and in the centre, the others on a grid behind
+        areas = np.sort(np.exp(rng.uniform(np.log(0.005), np.log(0.25), n_objects)))[::-1]
+        areas[0] = 0.25
+        for i in range(n_objects):
+            kind = ("sphere", "box", "cylinder")[int(rng.integers(3))]
+            if i == 0:
+                z, x, y = 0.8, 0.0, 0.0
+            else:  # on an ellipse around the central object, in view
+                ang = 2 * math.pi * (i - 1) / max(n_objects - 1, 1) + 0.3
+                z = rng.uniform(1.2, 1.9)
+                x = 0.45 * math.cos(ang) * z
+                y = 0.33 * math.sin(ang) * z
+            extent = float(np.clip(math.sqrt(areas[i] * width * height) * z / fpx, 0.05, 0.4))
+            if kind == "sphere":
+                size = (0.5 * extent,)
+            elif kind == "box":
+                size = tuple(extent * rng.uniform(0.6, 1.0, 3))
+            else:
+                size = (0.3 * extent, extent)
+            octree = int(rng.choice([32, 64, 128, 256]))
+            # voxel 2-5 mm, enlarged within that range so that the volume covers
+            # the object and the truncation band where the octree size allows it
+            need = 1.8 * extent + 0.2
+            voxel = float(np.clip(need / octree, 0.002, 0.005))
+            dim = octree * voxel
+            p = np.eye(4)
+            p[:3, :3] = rot_axis(rng.normal(size=3), rng.uniform(0, math.pi))
+            p[:3, 3] = (cam0 @ np.array([x, y, z, 1.0]))[:3]
+            tw = np.concatenate([rng.uniform(-1, 1, 3) * 0.004, rng.uniform(-1, 1, 3) *
+                                 math.radians(0.6)])
+            sh = Shape(kind, size, p, rng.uniform(0.3, 1.0, 3), label=i + 1, twist=tw)
+            movers.append(sh)
+            instances.append(Instance(i + 1, octree, dim, sh))
     return Scene(width, height, k, lo, hi, statics, movers, instances, cams, seed, noise)

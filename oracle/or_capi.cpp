@@ -100,6 +100,19 @@ void or_raycast_objects(void** vols, const float* Two, const int* labels, int n,
                       F4{k4[0], k4[1], k4[2], k4[3]}, W, H, nearp, farp, mu, eps);
 }
 
+void or_raycast_oob_mask(void** vols, const float* Two, int n, const float* Twc,
+                         const float* k4, int W, int H, float nearp, float farp, float mu,
+                         float eps, unsigned char* mask) {
+  std::vector<RaycastInstance> inst(n);
+  for (int i = 0; i < n; ++i) {
+    inst[i].vol = (const Volume*)vols[i];
+    inst[i].T_w_o = load_m4(Two + 16 * i);
+    inst[i].label = 0;
+  }
+  raycast_oob_mask(inst.data(), n, mask, load_m4(Twc), F4{k4[0], k4[1], k4[2], k4[3]}, W, H,
+                   nearp, farp, mu, eps);
+}
+
 // Unit-level entry points for the reference's own unit tests.
 int or_unique_multiscale(uint64_t* keys, int n, uint64_t level_mask, int cur_level) {
   return cur_level < 0 ? unique_multiscale(keys, n, level_mask)

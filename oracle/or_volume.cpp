@@ -547,4 +547,95 @@ void raycast_object_list(const RaycastInstance* inst, int n, F3* vertex, F3* nor
     }
 }
 
+// Test support, no reference counterpart: marks the pixels where any
+// instance's raycast (first-block search, march, foreground interpolation at
+// the hit; every instance with the full far plane, so a superset of the rays
+// the composite actually evaluates) reads a voxel outside [0, size) that the
+// reference aliases into an allocated block.  The reference's bit descent
+// (lib/octree.hpp:359-379) maps such coordinates into another block and
+// indexes that block's voxel array out of its bounds (lib/node.hpp:144-149),
+// so its result there depends on memory layout; the restatement reads them as
+// unallocated.  Parity tests exclude these pixels.
+// A read at (x, y, z) outside [0, size) whose aliased block (the reference
+// descends by the coordinate bits below size) is allocated: there the
+// reference returns some voxel of that block or memory past it, the
+// restatement the unallocated value.  Aliasing into an unallocated block gives
+// the unallocated value in both.
+static bool aliased_read(const Volume& v, int x, int y, int z) {
+  if (x >= 0 && y >= 0 && z >= 0 && x < v.size && y < v.size && z < v.size) return false;
+  const int m = v.size - 1;
+  return v.block_index(x & m, y & m, z & m) >= 0;
+}
+static bool oob_voxel(const Volume& v, F3 p) {
+  const float inv = v.size / v.dim;
+  const I3 s = to_i3(mk3(p.x * inv, p.y * inv, p.z * inv));
+  return aliased_read(v, s.x, s.y, s.z);
+}
+static bool oob_cell(const Volume& v, F3 pm) {
+  const float inv = v.size / v.dim;
+  const I3 b = to_i3(floor3(mk3(pm.x * inv, pm.y * inv, pm.z * inv)));
+  const I3 lo{imax(b.x, 0), imax(b.y, 0), imax(b.z, 0)};
+  for (int i = 0; i < 8; ++i)
+    if (aliased_read(v, lo.x + (i & 1), lo.y + ((i >> 1) & 1), lo.z + ((i >> 2) & 1)))
+      return true;
+  return false;
+}
+static bool raycast_touches_oob(const Volume& v, F3 origin, F3 direction, float nearPlane,
+                                float farPlane, float mu, float step, float largestep) {
+  const F3 invR = mk3(1.0f / direction.x, 1.0f / direction.y, 1.0f / direction.z);
+  const F3 tbot = (-1.f * invR) * origin;
+  const F3 ttop = invR * (v.dim - origin);
+  const F3 tmin = fmn3(ttop, tbot), tmax = fmx3(ttop, tbot);
+  const float tnear = fmx(fmx(fmx(tmin.x, tmin.y), fmx(tmin.x, tmin.z)), nearPlane);
+  const float tfar = fmn(fmn(fmn(tmax.x, tmax.y), fmn(tmax.x, tmax.z)), farPlane);
+  if (!(tnear < tfar)) return false;
+  float t = tnear, stepsize = largestep;
+  F3 position = origin + direction * t;
+  if (oob_cell(v, position)) return true;
+  float f_t = interp(v, position, 0), f_tt = 0;
+  if (!(f_t > 0)) return false;
+  for (; t < tfar; t += stepsize) {
+    if (oob_voxel(v, position)) return true;
+    f_tt = get_tsdf_at(v, position);
+    if ((double)f_tt <= 0.1 && f_tt >= -0.5f) {
+      if (oob_cell(v, position)) return true;
+      f_tt = interp(v, position, 0);
+    }
+    if (f_tt < 0) break;
+    stepsize = fmx(f_tt * mu, step);
+    position += stepsize * direction;
+    f_t = f_tt;
+  }
+  if (f_tt < 0) {
+    t = t + stepsize * f_tt / (f_t - f_tt);
+    if (oob_cell(v, origin + direction * t)) return true;
+  }
+  return false;
+}
+
+void raycast_oob_mask(const RaycastInstance* inst, int n, unsigned char* mask, const M4& T_w_c,
+                      F4 k, int W, int H, float nearPlane, float farPlane, float mu,
+                      float epsilon) {
+  const M4 view = mul(T_w_c, inverse_camera_matrix(k));
+  std::vector<M4> inv(n);
+  for (int i = 0; i < n; ++i) inv[i] = inverse(inst[i].T_w_o);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      unsigned char m = 0;
+      for (int o = 0; o < n && !m; ++o) {
+        const Volume& vol = *inst[o].vol;
+        const float step = vol.dim / vol.size;
+        const F3 o_origin = inv[o] * get_translation(view);
+        const F3 o_dir = normalize(rotate(inv[o], rotate(view, mk3((float)x, (float)y, 1.f))));
+        const float t_min = ray_first_block(vol, o_origin, o_dir, nearPlane, farPlane, epsilon);
+        if (t_min > 0.f &&
+            raycast_touches_oob(vol, o_origin, o_dir, t_min * vol.dim / (unsigned)vol.size,
+                                farPlane, mu, step, 8 * step))
+          m = 1;
+      }
+      mask[x + y * W] = m;
+    }
+}
+
 }  // namespace orc

@@ -122,5 +122,8 @@ struct RaycastInstance {
 void raycast_object_list(const RaycastInstance* inst, int n, F3* vertex, F3* normal,
                          int* label_img, const M4& T_w_c, F4 k, int W, int H,
                          float nearp, float farp, float mu, float epsilon);
+// pixels whose raycast reads voxels outside [0, size) (test support)
+void raycast_oob_mask(const RaycastInstance* inst, int n, unsigned char* mask, const M4& T_w_c,
+                      F4 k, int W, int H, float nearp, float farp, float mu, float epsilon);
 
 }  // namespace orc

@@ -175,6 +175,21 @@ class Impl:
                                          far, mu, vertex, normal, label_img)
         return vertex, normal, label_img
 
+    def raycast_oob_mask(self, vols, poses, T_w_c, k, W, H, near=0.1, far=4.0, mu=0.1,
+                         eps_size=None):
+        """Pixels whose raycast reads voxels outside [0, size) (oracle only)."""
+        n = len(vols)
+        arr = (P * n)(*[v.h for v in vols])
+        mask = np.zeros((H, W), np.uint8)
+        eps = float(np.float32(2.0 ** -np.log2(eps_size or vols[0].size)))
+        f = self.lib.or_raycast_oob_mask
+        f.restype = None
+        f.argtypes = [C.POINTER(P), FP, C.c_int, FP, FP, C.c_int, C.c_int, C.c_float, C.c_float,
+                      C.c_float, C.c_float, U8P]
+        f(arr, _f32(np.stack(poses).reshape(n, 16)), n, _f32(T_w_c), _f32(k), W, H, near, far,
+          mu, eps, mask)
+        return mask.astype(bool)
+
 
 _cache = {}
 
