@@ -39,25 +39,36 @@ METRIC = "640x480 frames/s, K objects: batched vs plain GPU at <=1e-5 pose err; 
 WORKLOAD = "640x480 RGB-D, background 512^3@1cm + 3 objects 256^3@2mm (sphere, box, cylinder)"
 
 
-def scene_for(rank, n_frames):
+UNEVEN = ("640x480 RGB-D, background 512^3@1cm + 12 objects with octrees of 32^3-256^3 at "
+          "2-5 mm, mask areas 0.4-25 %")
+UNEVEN_STEPS = 8
+
+
+def scene_for(rank, n_frames, workload="multi"):
     from mid_fusion_b200.scene import make_scene
+    if workload == "uneven":
+        return make_scene("uneven", W, H, n_frames=n_frames, seed=23 + rank, n_objects=12)
     return make_scene("multi", W, H, n_frames=n_frames, seed=11 + rank, n_objects=3,
                       bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512)
 
 
 def _render(args):
-    rank, n_frames, f = args
-    s = scene_for(rank, n_frames)
+    rank, n_frames, f, workload = args
+    s = scene_for(rank, n_frames, workload)
     d, rgb, lab = s.render(f)
-    return f, d, rgb, lab
+    return workload, f, d, rgb, lab
 
 
-def render_frames(rank, n_frames, workers):
+def render_frames(rank, jobs, workers):
+    """jobs: {workload: n_frames}.  Returns {workload: [(depth, rgb, labels), ...]}."""
     ctx = mp.get_context("spawn")
+    tasks = [(rank, n, f, w) for w, n in jobs.items() for f in range(n)]
     with ctx.Pool(workers) as pool:
-        out = pool.map(_render, [(rank, n_frames, f) for f in range(n_frames)])
-    out.sort(key=lambda t: t[0])
-    return [o[1:] for o in out]
+        out = pool.map(_render, tasks)
+    res = {w: [None] * n for w, n in jobs.items()}
+    for w, f, d, rgb, lab in out:
+        res[w][f] = (d, rgb, lab)
+    return res
 
 
 class ClockSampler:
@@ -121,37 +132,51 @@ def run_ours(args, rank, world, local_rank):
     from mid_fusion_b200.capi import Context
 
     n_frames = 1 + args.warmup + args.steps
-    frames = render_frames(rank, n_frames, args.workers)  # before the first CUDA call
+    n_uneven = 1 + args.warmup + UNEVEN_STEPS
+    do_uneven = world == 1 and not args.profile
+    jobs = {"multi": n_frames}
+    if do_uneven:
+        jobs["uneven"] = n_uneven
+    rendered = render_frames(rank, jobs, args.workers)  # before the first CUDA call
+    frames = rendered["multi"]
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     build.build()
     s = scene_for(rank, n_frames)
-
-    def make_ctx(batched):
-        ctx = Context(W, H, k=s.k, pool_blocks=args.pool_blocks, batched=batched, robust="huber")
-        for inst, T in zip(s.instances, s.volume_poses(0)):
-            ctx.add_instance(inst.size, inst.dim, T, inst.label)
-        ctx.set_camera_pose(s.cam_poses[0])
-        return ctx
-
-    # device-resident inputs
-    d_depth = [torch.from_numpy(f[0]).to(dev) for f in frames]
-    d_rgb = [torch.from_numpy(np.ascontiguousarray(f[1])).to(dev) for f in frames]
-    d_lab = [torch.from_numpy(f[2].astype(np.int16)).to(dev) for f in frames]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
-    def run(batched, record_poses=True):
-        ctx = make_ctx(batched)
+    def make_ctx(batched, scene=None):
+        sc = scene or s
+        ctx = Context(W, H, k=sc.k, pool_blocks=args.pool_blocks, batched=batched,
+                      robust="huber")
+        for inst, T in zip(sc.instances, sc.volume_poses(0)):
+            ctx.add_instance(inst.size, inst.dim, T, inst.label)
+        ctx.set_camera_pose(sc.cam_poses[0])
+        return ctx
+
+    def to_device(fr):
+        return ([torch.from_numpy(f[0]).to(dev) for f in fr],
+                [torch.from_numpy(np.ascontiguousarray(f[1])).to(dev) for f in fr],
+                [torch.from_numpy(f[2].astype(np.int16)).to(dev) for f in fr])
+
+    # device-resident inputs
+    d_depth, d_rgb, d_lab = to_device(frames)
+
+    def run(batched, record_poses=True, scene=None, inputs=None):
+        """Frames through mf_process_frame_device; device time per frame after
+        1 + warmup untimed frames."""
+        ctx = make_ctx(batched, scene)
+        dd, dr, dl = inputs or (d_depth, d_rgb, d_lab)
         stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
         lib = ctx.lib
         times, poses = [], []
-        for f in range(n_frames):
+        for f in range(len(dd)):
             flush.fill_(f & 0xff)
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            rc = lib.mf_process_frame_device(ctx.h, ctx_ptr(d_depth[f]), ctx_ptr(d_rgb[f]),
-                                             ctx_ptr(d_lab[f]))
+            rc = lib.mf_process_frame_device(ctx.h, ctx_ptr(dd[f]), ctx_ptr(dr[f]),
+                                             ctx_ptr(dl[f]))
             if rc != 0:
                 raise RuntimeError(f"mf_process_frame_device failed: {rc}")
             e1.record(stream)
@@ -161,7 +186,7 @@ def run_ours(args, rank, world, local_rank):
             if record_poses:
                 poses.append(ctx_poses(ctx))
         st = ctx.status()
-        if batched:
+        if batched and scene is None:
             stats.update(ctx.frame_stats())
         return ctx, times, poses, st
 
@@ -172,7 +197,7 @@ def run_ours(args, rank, world, local_rank):
     def ctx_poses(ctx):
         import ctypes
         Tc = np.zeros(16, np.float32)
-        To = np.zeros(16 * len(s.instances), np.float32)
+        To = np.zeros(16 * ctx.n_instances, np.float32)
         ctx.lib.mf_get_poses(ctx.h, Tc.ctypes.data_as(ctypes.c_void_p),
                              To.ctypes.data_as(ctypes.c_void_p))
         return Tc.reshape(4, 4), To.reshape(-1, 4, 4)
@@ -198,6 +223,28 @@ def run_ours(args, rank, world, local_rank):
                    float(np.abs(ob[:, :3, 3] - op[:, :3, 3]).max()))
     # pose error against ground truth (last frame), informative
     gt_err = float(np.linalg.norm(poses_b[-1][0][:3, 3] - s.cam_poses[n_frames - 1][:3, 3]))
+
+    # ---- 12 uneven objects: batched against plain on the same frames
+    uneven = None
+    if do_uneven:
+        su = scene_for(rank, n_uneven, "uneven")
+        ins = to_device(rendered["uneven"])
+        cub, tub, pub, stub = run(True, scene=su, inputs=ins)
+        cup, tup, pup, stup = run(False, scene=su, inputs=ins)
+        du = 0.0
+        for (cb, ob), (cp, op) in zip(pub, pup):
+            du = max(du, float(np.abs(cb[:3, 3] - cp[:3, 3]).max()),
+                     float(np.abs(ob[:, :3, 3] - op[:, :3, 3]).max()))
+        ub, up = sum(tub), sum(tup)
+        uneven = {"workload": UNEVEN, "instances": len(su.instances), "steps": len(tub),
+                  "batched": round(len(tub) / ub, 2), "plain": round(len(tup) / up, 2),
+                  "ms_batched": round(1e3 * ub / len(tub), 4),
+                  "ms_plain": round(1e3 * up / len(tup), 4),
+                  "batched_over_plain": round(up / ub, 3), "pose_diff_batched_vs_plain_m": du,
+                  "status_flags": [stub, stup]}
+        for c in (cub, cup):
+            c.close()
+        del ins
 
     # ---- e2e through the C ABI from pinned host buffers
     import ctypes
@@ -242,7 +289,7 @@ def run_ours(args, rank, world, local_rank):
     return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
                 status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
                 ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
-                n_inst=len(s.instances))
+                n_inst=len(s.instances), uneven=uneven)
 
 
 def run_reference(args):
@@ -253,7 +300,7 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cpu_baseline as CB
     n_frames = 1 + args.warmup + args.steps
-    frames = render_frames(0, n_frames, args.workers)
+    frames = render_frames(0, {"multi": n_frames}, args.workers)["multi"]
     s = scene_for(0, n_frames)
     p = CB.CpuPipeline(s, use_reference=True)
     t = []
@@ -400,6 +447,7 @@ def main():
         "plain": {"value": round(value_p, 2), "unit": "frames/s",
                   "ms_per_step": round(1e3 * total_p / args.steps, 4)},
         "batched_over_plain": round(total_p / total_b, 3),
+        "uneven12": r.get("uneven"),
         "pose_diff_batched_vs_plain_m": r["dpos"],
         "camera_err_vs_gt_m": r["gt_err"],
         "e2e": {"value": round(value_e, 2), "unit": "frames/s",

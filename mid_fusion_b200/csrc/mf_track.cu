@@ -298,8 +298,9 @@ MF_HD void gn_step(GNState& S, const double* s, int level) {
   const double prev_err = S.prev_err;
   const double err = s[0] / s[28];
   int done = 0, fallback = 0;
-  if (S.kind == 1 && s[28] == 0) {
+  if (S.kind == 1 && s[28] == 0) {  // no valid row: the object loop stops (:674-676)
     S.done = 1;
+    S.iters[level] += 1;
     return;
   }
   if (err > prev_err) {

@@ -323,8 +323,8 @@ def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_ob
     ``preset='uneven'``: background room + ``n_objects`` (default use: 12) rigid
     primitives of seeded kinds and sizes (0.05-0.4 m), each with its own octree
     of 32^3, 64^3, 128^3 or 256^3 voxels at 2-5 mm; the largest object sits in
-    the centre at 0.8 m, the others on an ellipse around it 1.2-1.9 m away,
-    sized so that their target mask areas span 0.5 %-25 % of the frame."""
+    the centre, the others on an ellipse around it, at depths chosen so that
+    their mask areas span about 0.5 %-25 % of the frame."""
     rng = np.random.default_rng(seed)
     scale = width / 640.0
     k = (525.0 * scale, 525.0 * scale, (width - 1) / 2.0, (height - 1) / 2.0)
@@ -369,30 +369,40 @@ def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_ob
     elif preset == "uneven":
         cam0 = cams[0]
         fpx = k[0]
-        # target mask areas, log-uniform over [0.5 %, 25 %] of the frame, the
-        # largest object nearest and in the centre, the others on a grid behind
-        areas = np.sort(np.exp(rng.uniform(np.log(0.005), np.log(0.25), n_objects)))[::-1]
-        areas[0] = 0.25
+        # object extents log-uniform over 0.05-0.4 m (largest first) and target
+        # mask areas log-uniform over 0.5-15 %, the largest object 25 % in the
+        # centre; the depth follows from extent and area
+        extents = np.sort(np.exp(rng.uniform(np.log(0.05), np.log(0.4), n_objects)))[::-1]
+        extents[0], extents[-1] = 0.4, 0.05
+        areas = np.exp(rng.uniform(np.log(0.005), np.log(0.15), n_objects))
+        areas[0] = 0.4  # of the bounding square: about 25 % for a box or sphere
         for i in range(n_objects):
             kind = ("sphere", "box", "cylinder")[int(rng.integers(3))]
+            extent = float(extents[i])
+            z = float(np.clip(extent * fpx / math.sqrt(areas[i] * width * height), 0.5, 3.0))
             if i == 0:
-                z, x, y = 0.8, 0.0, 0.0
-            else:  # on an ellipse around the central object, in view
+                x = y = 0.0
+            else:  # on an ellipse around the central object
                 ang = 2 * math.pi * (i - 1) / max(n_objects - 1, 1) + 0.3
-                z = rng.uniform(1.2, 1.9)
                 x = 0.45 * math.cos(ang) * z
                 y = 0.33 * math.sin(ang) * z
-            extent = float(np.clip(math.sqrt(areas[i] * width * height) * z / fpx, 0.05, 0.4))
             if kind == "sphere":
                 size = (0.5 * extent,)
             elif kind == "box":
                 size = tuple(extent * rng.uniform(0.6, 1.0, 3))
             else:
                 size = (0.3 * extent, extent)
-            octree = int(rng.choice([32, 64, 128, 256]))
-            # voxel 2-5 mm, enlarged within that range so that the volume covers
-            # the object and the truncation band where the octree size allows it
-            need = 1.8 * extent + 0.2
+            # The volume is centred on the object with a margin (as
+            # spawnNewObjectKernel sizes it): the smallest octree of 32^3 ...
+            # 256^3 whose 5 mm voxels span twice the object's extent plus 6 cm,
+            # sometimes the next finer one, at a voxel of 2-5 mm.  Without the
+            # margin the volume corner lies in front of the object and takes
+            # its foreground probability, and a raycast miss (which the
+            # reference samples at the volume corner) would claim the pixel.
+            need = 2.0 * extent + 0.06
+            octree = next((o for o in (32, 64, 128, 256) if o * 0.005 >= need), 256)
+            if octree < 256 and rng.random() < 0.3:
+                octree *= 2
             voxel = float(np.clip(need / octree, 0.002, 0.005))
             dim = octree * voxel
             p = np.eye(4)
