@@ -133,16 +133,17 @@ def run_ours(args, rank, world, local_rank):
 
     n_frames = 1 + args.warmup + args.steps
     n_uneven = 1 + args.warmup + UNEVEN_STEPS
-    do_uneven = world == 1 and not args.profile
-    jobs = {"multi": n_frames}
+    main = args.workload
+    do_uneven = world == 1 and not args.profile and main == "multi"
+    jobs = {main: n_frames}
     if do_uneven:
         jobs["uneven"] = n_uneven
     rendered = render_frames(rank, jobs, args.workers)  # before the first CUDA call
-    frames = rendered["multi"]
+    frames = rendered[main]
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     build.build()
-    s = scene_for(rank, n_frames)
+    s = scene_for(rank, n_frames, main)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def make_ctx(batched, scene=None):
@@ -372,6 +373,8 @@ def main():
     ap.add_argument("--workers", type=int, default=min(32, os.cpu_count() or 4))
     ap.add_argument("--pool-blocks", type=int, default=1 << 18)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--workload", default="multi", choices=["multi", "uneven"],
+                    help="multi: background + 3 objects (the headline); uneven: + 12 objects")
     ap.add_argument("--profile", action="store_true",
                     help="run only the batched device-resident path (profiler runs)")
     args = ap.parse_args()
@@ -441,7 +444,8 @@ def main():
         "dtype": "f32",
         "precision": "f32 per-pixel arithmetic, f64 reductions, 6x6 solve and SE(3) update",
         "data": "synthetic (seeded analytic RGB-D scenes)",
-        "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4,
+        "config": {"workload": WORKLOAD if args.workload == "multi" else UNEVEN,
+                   "frame": [W, H], "instances": r["n_inst"],
                    "l2": "flushed between steps (256 MiB write)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "plain": {"value": round(value_p, 2), "unit": "frames/s",
