@@ -15,6 +15,7 @@
 // convergence test).  The host only launches: the whole coarse-to-fine loop is
 // a fixed sequence of launches, and problems that stopped skip their work.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -42,6 +43,9 @@ struct GNState {
   int fallback;
   int ticket;
   int pad_;
+  // objects: bounding box (x0, y0, x1, y1) of the object's pixels in the
+  // full-resolution model label map; empty when x1 < x0
+  int box[4];
   M4 Tf, invTf;      // float pose (and inverse) seen by the per-pixel kernels
   M4 T_w_r, inv_T_w_r, view;               // camera: reference pose, K * inverse(T_w_r)
   M4 T_c1_o1, inv_T_c1_o1, inv_T_w_o1, T_w_c2;  // object constants
@@ -183,15 +187,32 @@ struct SlotPtrs {
 // object, its own map: the composite where label == object, 0 elsewhere
 // (rendering.cpp:153-178) -- seen from the reference camera (T_w_r for the
 // camera problem, T_w_c1 for an object; its inverse is kept in inv_T_w_r).
+// For an object it also gathers the bounding box of the object's pixels in the
+// label map (warp-reduced atomics); the object rows use it to skip gathers that
+// can only find other labels.
 __global__ void render_depth_kernel(const F3* __restrict__ vertex, const int* __restrict__ label,
-                                    const GNState* __restrict__ st, IdList slots, SlotPtrs sp,
-                                    int WH) {
+                                    GNState* __restrict__ st, IdList slots, SlotPtrs sp,
+                                    int W, int WH) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= WH) return;
-  const GNState& S = st[slots.v[blockIdx.y]];
-  F3 v = vertex[p];
-  if (S.kind == 1 && label[p] != S.label) v = mk3(0.f);
-  sp.D[blockIdx.y][p] = v.z > 0.0 ? xform(S.inv_T_w_r, v).z : 0.f;
+  GNState& S = st[slots.v[blockIdx.y]];
+  bool mine = false;
+  if (p < WH) {
+    F3 v = vertex[p];
+    if (S.kind == 1) {
+      mine = label[p] == S.label;
+      if (!mine) v = mk3(0.f);
+    }
+    sp.D[blockIdx.y][p] = v.z > 0.0 ? xform(S.inv_T_w_r, v).z : 0.f;
+  }
+  if (S.kind != 1) return;
+  const int x = mine ? p % W : INT_MAX, y = mine ? p / W : INT_MAX;
+  const int x0 = __reduce_min_sync(0xffffffffu, x), y0 = __reduce_min_sync(0xffffffffu, y);
+  const int x1 = __reduce_max_sync(0xffffffffu, mine ? x : -1);
+  const int y1 = __reduce_max_sync(0xffffffffu, mine ? y : -1);
+  if ((threadIdx.x & 31) == 0 && x1 >= 0) {
+    atomicMin(&S.box[0], x0); atomicMin(&S.box[1], y0);
+    atomicMax(&S.box[2], x1); atomicMax(&S.box[3], y1);
+  }
 }
 
 __global__ void half_sample_slots_kernel(SlotPtrs sp, int iw, int ih, float e_d) {
@@ -252,6 +273,8 @@ __global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __r
   const M4 T_w_c2 = load_m4(Twc2), T_w_c1 = load_m4(Twc1), T_wo1 = load_m4(Two + 16 * s);
   S.kind = 1; S.inst = s; S.label = inst_label[s]; S.done = 0; S.ticket = 0; S.fallback = 0;
   for (int l = 0; l < MAX_PYR; ++l) S.iters[l] = 0;
+  S.box[0] = S.box[1] = INT_MAX;
+  S.box[2] = S.box[3] = -1;
   S.T_w_c2 = T_w_c2;
   S.inv_T_w_r = inverse(T_w_c1);
   S.T_c1_o1 = mul(S.inv_T_w_r, T_wo1);
@@ -374,16 +397,23 @@ __device__ __forceinline__ void obj_maps(const GNArgs& a, int idx, int label, F3
   if (a.mlabel[idx] == label) { v = a.mvertex[idx]; n = a.mnormal[idx]; }
   else { v = mk3(0.f); n = mk3(INVALIDF, 0.f, 0.f); }
 }
-__device__ __forceinline__ void bil_obj(const GNArgs& a, int label, float px, float py, F3& v,
-                                        F3& n) {
+// A 2x2 cell outside the object's label box holds only other labels: its four
+// taps are (0, INVALID normal) without reading the maps (same arithmetic).
+__device__ __forceinline__ void bil_obj(const GNArgs& a, const GNState& S, float px, float py,
+                                        F3& v, F3& n) {
   const float fx0 = floorf(px), fy0 = floorf(py);
   const int bx = (int)fx0, by = (int)fy0;
   const float fx = px - fx0, fy = py - fy0;
   F3 v0, v1, v2, v3, n0, n1, n2, n3;
-  obj_maps(a, bx + by * a.W, label, v0, n0);
-  obj_maps(a, bx + 1 + by * a.W, label, v1, n1);
-  obj_maps(a, bx + (by + 1) * a.W, label, v2, n2);
-  obj_maps(a, bx + 1 + (by + 1) * a.W, label, v3, n3);
+  if (bx + 1 < S.box[0] || bx > S.box[2] || by + 1 < S.box[1] || by > S.box[3]) {
+    v0 = v1 = v2 = v3 = mk3(0.f);
+    n0 = n1 = n2 = n3 = mk3(INVALIDF, 0.f, 0.f);
+  } else {
+    obj_maps(a, bx + by * a.W, S.label, v0, n0);
+    obj_maps(a, bx + 1 + by * a.W, S.label, v1, n1);
+    obj_maps(a, bx + (by + 1) * a.W, S.label, v2, n2);
+    obj_maps(a, bx + 1 + (by + 1) * a.W, S.label, v3, n3);
+  }
   const float A = 1.f - fx, B = 1.f - fy;
   v = mk3(v0.x * A * B + v1.x * B * fx + v2.x * A * fy + v3.x * fx * fy,
           v0.y * A * B + v1.y * B * fx + v2.y * A * fy + v3.y * fx * fy,
@@ -434,7 +464,7 @@ __device__ void icp_object(const GNArgs& a, const GNState& S, int L, int p, Row&
       isnan(px) || isnan(py)) { r.result = -2; return; }
   const F3 o2n = rotate(S.invTf, cn);
   F3 wrv, wrn;
-  bil_obj(a, S.label, px, py, wrv, wrn);
+  bil_obj(a, S, px, py, wrv, wrn);
   if (wrn.x == INVALIDF) { r.result = -3; return; }
   const F3 o1rv = xform(S.inv_T_w_o1, wrv);
   const F3 o1rn = rotate(S.inv_T_w_o1, wrn);
@@ -459,6 +489,16 @@ __device__ void icp_object(const GNArgs& a, const GNState& S, int L, int p, Row&
 // :1152-1178).  The photometric outlier mask of the reference is all zero.
 __device__ void rgb_row(const GNArgs& a, const GNState& S, const F3* rV, int L, int p, int w,
                         int h, Row& r) {
+  if (S.kind == 1) {
+    // an object's rendered reference is valid only inside its label box,
+    // halved per pyramid level (half-sampling never widens it)
+    const int x = p % w, y = p / w;
+    if (x < (S.box[0] >> L) || x > (S.box[2] >> L) || y < (S.box[1] >> L) ||
+        y > (S.box[3] >> L)) {
+      r.result = -1;
+      return;
+    }
+  }
   const F3 rv = rV[p];
   const F3 rl = a.pyr.V[1 - a.cur][L][p];
   if (rv.z <= 0.f || rv.z == INVALIDF) { r.result = -1; return; }
@@ -554,6 +594,25 @@ __device__ __forceinline__ void accumulate(float* acc, int* cnt, const Row& r, i
   acc[28] += 1.f;
 }
 
+// The warp's sum of value `lane` (29 sums, then the 3 counts) in FP64: every
+// lane stores its FP32 partials in shared memory (rows padded to 33 words, so
+// the column reads hit 32 banks) and lane i adds column i over the 32 lanes in
+// lane order.  A shuffle tree would take 10 shuffles per double and 320 per
+// warp; with one problem per grid row and many problems per launch that tree
+// dominated the launch.
+__device__ __forceinline__ double warp_sum_fp64(const float* acc, const int* cnt,
+                                                float (*red)[33], int lane) {
+#pragma unroll
+  for (int i = 0; i < 29; ++i) red[lane][i] = acc[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) red[lane][29 + i] = (float)cnt[i];  // small, exact
+  __syncwarp();
+  double v = 0;
+#pragma unroll 8
+  for (int j = 0; j < 32; ++j) v += (double)red[j][lane];
+  return v;
+}
+
 // KIND 0: the camera problem; KIND 1: object problems (one instantiation each
 // keeps the kernel's code small).
 template <int KIND>
@@ -589,14 +648,9 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   }
   // FP64 from the warp level up
   __shared__ double sh[GN_THREADS / 32][32];
+  __shared__ float red[GN_THREADS / 32][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    double v = i < 29 ? (double)acc[i] : (double)cnt[i - 29];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sh[warp][i] = v;
-  }
+  sh[warp][lane] = warp_sum_fp64(acc, cnt, red[warp], lane);
   __syncthreads();
   __shared__ bool last;
   if (threadIdx.x < 32) {
@@ -798,7 +852,7 @@ static int render_reference(Context* ctx, const IdList& slots) {
   SlotPtrs sp{};
   for (int i = 0; i < slots.n; ++i) sp.D[i] = T.rD[slots.v[i]][0];
   render_depth_kernel<<<dim3(div_up(WH, 256), slots.n), 256, 0, ctx->stream>>>(
-      ctx->d_vertex, ctx->d_label, T.d_state, slots, sp, WH);
+      ctx->d_vertex, ctx->d_label, T.d_state, slots, sp, ctx->W, WH);
   MF_CUDA(cudaGetLastError());
   for (int l = 0; l < T.levels; ++l) {
     SlotPtrs q{};
@@ -1135,14 +1189,9 @@ gn_eval_static_kernel(GNArgs a, int s, int L, int set_pose, M4 Tf, M4 invTf,
     }
   }
   __shared__ double sh[GN_THREADS / 32][32];
+  __shared__ float red[GN_THREADS / 32][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int i = 0; i < 32; ++i) {
-    double v = i < 29 ? (double)acc[i] : (double)cnt[i - 29];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0) sh[warp][i] = v;
-  }
+  sh[warp][lane] = warp_sum_fp64(acc, cnt, red[warp], lane);
   __syncthreads();
   __shared__ bool last;
   if (threadIdx.x < 32) {
