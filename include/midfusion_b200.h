@@ -153,7 +153,7 @@ int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, doubl
  * 32 sums and a CTA ticket) is one static device array of 1 MiB + 512 B, so a
  * level may have at most 4096 x 512 pixels at level 0 and 4096 x 256 above
  * (larger levels return MF_E_ARG).  The pose is passed to the kernel by value
- * and the context's tracking state is not modified.  Same results as
+ * and the context's poses and sums are not modified.  Same results as
  * mf_track_eval, bit for bit.
  *  - The first call on a device looks up the scratch's device address; make
  *    it (for example once at start-up) before any stream capture.

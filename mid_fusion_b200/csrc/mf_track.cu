@@ -74,6 +74,7 @@ struct TrackState {
   GNState* d_state = nullptr;       // MAX_INSTANCES (slot 0: camera, slot i: object i)
   double* d_partials = nullptr;     // MAX_INSTANCES x max_tiles x 32
   int max_tiles = 0;
+  float2* d_zr = nullptr;           // MAX_PYR x max_tiles live depth range per CTA tile
   float* d_Twc_prev = nullptr;      // camera pose of the previous frame
   uint8_t* d_mask0 = nullptr;       // full-resolution ICP outlier mask
   float gaussian[5];
@@ -374,6 +375,7 @@ struct GNArgs {
   GNState* st;
   double* partials;
   int max_tiles;
+  const float2* zr;     // live depth range of each CTA tile, [level][tile]
   F4 kL;                // intrinsics at this level
   F4 k0;                // full resolution
   float inv_cov_rgb;
@@ -594,6 +596,90 @@ __device__ __forceinline__ void accumulate(float* acc, int* cnt, const Row& r, i
   acc[28] += 1.f;
 }
 
+// Range of live depths over the pixels of each GN tile (CTA) and level whose
+// ICP row gets past the validity checks (valid normal, nonzero vertex).
+__global__ void tile_depth_range_kernel(PyrPtrs pyr, int cur, float2* __restrict__ zr,
+                                        int max_tiles) {
+  const int L = blockIdx.y;
+  const int w = pyr.w[L], n = w * pyr.h[L];
+  const int ppt = gn_pix(L);
+  const int p0 = blockIdx.x * GN_THREADS * ppt;
+  if (p0 >= n) return;
+  float lo = INFINITY, hi = -INFINITY;
+  for (int k = 0; k < ppt; ++k) {
+    const int p = p0 + k * GN_THREADS + threadIdx.x;
+    if (p < n && pyr.N[L][p].x != INVALIDF) {
+      const F3 v = pyr.V[cur][L][p];
+      if (!(v.x == 0 && v.y == 0 && v.z == 0)) { lo = fminf(lo, v.z); hi = fmaxf(hi, v.z); }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  __shared__ float2 sw[GN_THREADS / 32];
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = make_float2(lo, hi);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < GN_THREADS / 32; ++i) { lo = fminf(lo, sw[i].x); hi = fmaxf(hi, sw[i].y); }
+    zr[L * max_tiles + blockIdx.x] = make_float2(lo, hi);
+  }
+}
+
+// Can any pixel of tile `tile` at level L give an object problem a valid row?
+// A `false` answer is exact for the 29 normal-equation sums (the tile's pixels
+// all end in a negative result code); only the diagnostic outlier counts
+// (sums 29-31, which the reference computes and never reads) then leave the
+// tile out.
+//  - photometric rows need the object's rendered reference: inside its label
+//    box, halved per level;
+//  - an ICP row needs a model tap with the object's label, i.e. a projection
+//    into the label box: the tile's live points lie in the frustum spanned by
+//    its pixel rectangle and depth range, whose projection lies in the hull
+//    of its 8 projected corners (2 px of slack for rounding);
+//  - or, with no such tap, the blended model vertex is 0, the world origin:
+//    rows then need a live point within 0.1 m of it (in object coordinates).
+__device__ bool object_tile_live(const GNArgs& a, const GNState& S, int L, int tile, int w,
+                                 int n) {
+  const int ppt = gn_pix(L);
+  const int p0 = tile * GN_THREADS * ppt, p1 = min(n, p0 + GN_THREADS * ppt);
+  const int ya = p0 / w, yb = (p1 - 1) / w;
+  const int xa = ya == yb ? p0 % w : 0, xb = ya == yb ? (p1 - 1) % w : w - 1;
+  const bool has_box = S.box[2] >= S.box[0];
+  if (a.use_rgb && has_box &&
+      !(xb < (S.box[0] >> L) || xa > (S.box[2] >> L) || yb < (S.box[1] >> L) ||
+        ya > (S.box[3] >> L)))
+    return true;
+  if (!a.use_icp) return false;
+  const float2 zr = a.zr[L * a.max_tiles + tile];
+  if (!(zr.x <= zr.y)) return false;  // no pixel of the tile reaches the projection
+  const M4 iK = inverse_camera_matrix(a.kL), K0 = camera_matrix(a.k0);
+  float qx0 = INFINITY, qx1 = -INFINITY, qy0 = INFINITY, qy1 = -INFINITY;
+  F3 lo = mk3(INFINITY), hi = mk3(-INFINITY);
+  for (int c = 0; c < 8; ++c) {
+    const float x = (float)((c & 1) ? xb : xa), y = (float)((c & 2) ? yb : ya);
+    const float z = (c & 4) ? zr.y : zr.x;
+    const F3 o2v = xform(S.invTf, z * rotate(iK, mk3(x, y, 1.f)));
+    lo = mk3(fminf(lo.x, o2v.x), fminf(lo.y, o2v.y), fminf(lo.z, o2v.z));
+    hi = mk3(fmaxf(hi.x, o2v.x), fmaxf(hi.y, o2v.y), fmaxf(hi.z, o2v.z));
+    const F3 c1v = xform(S.T_c1_o1, o2v);
+    if (!(c1v.z > 0.f)) return true;  // the frustum reaches behind camera 1: no bound
+    const F3 pr = rotate(K0, c1v);
+    const float qx = pr.x / pr.z, qy = pr.y / pr.z;
+    if (isnan(qx) || isnan(qy)) return true;
+    qx0 = fminf(qx0, qx); qx1 = fmaxf(qx1, qx);
+    qy0 = fminf(qy0, qy); qy1 = fmaxf(qy1, qy);
+  }
+  if (has_box && floorf(qx1) + 3.f >= (float)S.box[0] && floorf(qx0) - 2.f <= (float)S.box[2] &&
+      floorf(qy1) + 3.f >= (float)S.box[1] && floorf(qy0) - 2.f <= (float)S.box[3])
+    return true;
+  const F3 o = get_translation(S.inv_T_w_o1);
+  const float dx = fmaxf(fmaxf(lo.x - o.x, o.x - hi.x), 0.f);
+  const float dy = fmaxf(fmaxf(lo.y - o.y, o.y - hi.y), 0.f);
+  const float dz = fmaxf(fmaxf(lo.z - o.z, o.z - hi.z), 0.f);
+  return dx * dx + dy * dy + dz * dz <= 0.101f * 0.101f;
+}
+
 // The warp's sum of value `lane` (29 sums, then the 3 counts) in FP64: every
 // lane stores its FP32 partials in shared memory (rows padded to 33 words, so
 // the column reads hit 32 banks) and lane i adds column i over the 32 lanes in
@@ -623,34 +709,46 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   if (S.done) return;
   const int w = a.pyr.w[L], h = a.pyr.h[L];
   const int n = w * h;
-  float acc[29];
-#pragma unroll
-  for (int i = 0; i < 29; ++i) acc[i] = 0.f;
-  int cnt[3] = {0, 0, 0};
-  const F3* rV = a.rV[s];
-  const int ppt = gn_pix(L);
-#pragma unroll 1
-  for (int k = 0; k < ppt; ++k) {
-    const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
-    if (p >= n) break;
-    Row r;
-    if (a.use_icp) {
-      r.result = 0;
-      if (KIND == 0) icp_camera(a, S, L, p, r);
-      else icp_object(a, S, L, p, r);
-      accumulate(acc, cnt, r, a.robust);
-    }
-    if (a.use_rgb) {
-      r.result = 0;
-      rgb_row(a, S, rV, L, p, w, h, r);
-      accumulate(acc, cnt, r, a.robust);
-    }
+  // object problems: a tile that cannot hold a valid row skips its pixels
+  bool live = true;
+  if (KIND == 1) {
+    __shared__ int s_live;
+    if (threadIdx.x == 0) s_live = object_tile_live(a, S, L, blockIdx.x, w, n) ? 1 : 0;
+    __syncthreads();
+    live = s_live != 0;
   }
   // FP64 from the warp level up
   __shared__ double sh[GN_THREADS / 32][32];
   __shared__ float red[GN_THREADS / 32][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  sh[warp][lane] = warp_sum_fp64(acc, cnt, red[warp], lane);
+  if (live) {
+    float acc[29];
+#pragma unroll
+    for (int i = 0; i < 29; ++i) acc[i] = 0.f;
+    int cnt[3] = {0, 0, 0};
+    const F3* rV = a.rV[s];
+    const int ppt = gn_pix(L);
+#pragma unroll 1
+    for (int k = 0; k < ppt; ++k) {
+      const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
+      if (p >= n) break;
+      Row r;
+      if (a.use_icp) {
+        r.result = 0;
+        if (KIND == 0) icp_camera(a, S, L, p, r);
+        else icp_object(a, S, L, p, r);
+        accumulate(acc, cnt, r, a.robust);
+      }
+      if (a.use_rgb) {
+        r.result = 0;
+        rgb_row(a, S, rV, L, p, w, h, r);
+        accumulate(acc, cnt, r, a.robust);
+      }
+    }
+    sh[warp][lane] = warp_sum_fp64(acc, cnt, red[warp], lane);
+  } else {
+    sh[warp][lane] = 0.0;
+  }
   __syncthreads();
   __shared__ bool last;
   if (threadIdx.x < 32) {
@@ -739,6 +837,7 @@ int track_init(Context* ctx) {
     ts->max_tiles = std::max(ts->max_tiles, div_up((long long)P.w[l] * P.h[l], GN_THREADS * gn_pix(l)));
   if (talloc(ctx, &ts->d_state, MAX_INSTANCES)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_partials, (size_t)MAX_INSTANCES * ts->max_tiles * 32)) return MF_E_CUDA;
+  if (talloc(ctx, &ts->d_zr, (size_t)MAX_PYR * ts->max_tiles)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_Twc_prev, 16)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_mask0, (size_t)ctx->W * ctx->H)) return MF_E_CUDA;
   // Tracking::Tracking, tracking.cpp:77-84: gaussian[i] = expf(-(x*x) / (2 delta^2)),
@@ -890,6 +989,7 @@ static GNArgs make_args(Context* ctx, int L, int device_step) {
   a.st = T.d_state;
   a.partials = T.d_partials;
   a.max_tiles = T.max_tiles;
+  a.zr = T.d_zr;
   a.kL = kdiv(ctx->cfg, L);
   a.k0 = kdiv(ctx->cfg, 0);
   // obtainErrorParameters (TUM branch, tracking.cpp:766-772) keeps sigma_bright
@@ -901,6 +1001,18 @@ static GNArgs make_args(Context* ctx, int L, int device_step) {
   a.use_rgb = ctx->cfg.use_rgb;
   a.device_step = device_step;
   return a;
+}
+
+// Live depth range of every GN tile at every level (object problems read it to
+// skip tiles that cannot hold a valid row).  Recomputed before each object
+// evaluation, so it always matches the live vertex and normal maps.
+static int tile_depth_range(Context* ctx) {
+  TrackState& T = *ctx->track;
+  const int tiles = div_up((long long)T.pyr.w[0] * T.pyr.h[0], GN_THREADS * gn_pix(0));
+  tile_depth_range_kernel<<<dim3(tiles, T.levels), GN_THREADS, 0, ctx->stream>>>(
+      T.pyr, T.cur, T.d_zr, T.max_tiles);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
 }
 
 // Coarse-to-fine GN of every problem in `slots`, all on the device
@@ -994,6 +1106,7 @@ int track_objects(Context* ctx, const IdList& ids) {
                                                   ctx->d_Two, ctx->d_inst_label);
   MF_CUDA(cudaGetLastError());
   if (int rc = render_reference(ctx, ids)) return rc;
+  if (int rc = tile_depth_range(ctx)) return rc;
   if (ctx->cfg.batched) {
     if (int rc = gn_device(ctx, ids, 1)) return rc;
   } else {
@@ -1050,6 +1163,8 @@ int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums)
   one.v[0] = slot;
   const GNArgs a = make_args(ctx, L, 0);
   const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_THREADS * gn_pix(L));
+  if (S.kind == 1)
+    if (int rc = tile_depth_range(ctx)) return rc;
   if (S.kind == 0) gn_iter_kernel<0><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
   else gn_iter_kernel<1><<<dim3(tiles, 1), GN_THREADS, 0, ctx->stream>>>(a, one, L);
   MF_CUDA(cudaGetLastError());
@@ -1165,33 +1280,46 @@ gn_eval_static_kernel(GNArgs a, int s, int L, int set_pose, M4 Tf, M4 invTf,
 
   const int w = a.pyr.w[L], h = a.pyr.h[L];
   const int n = w * h;
-  float acc[29];
-#pragma unroll
-  for (int i = 0; i < 29; ++i) acc[i] = 0.f;
-  int cnt[3] = {0, 0, 0};
-  const F3* rV = a.rV[s];
-  const int ppt = gn_pix(L);
-#pragma unroll 1
-  for (int k = 0; k < ppt; ++k) {
-    const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
-    if (p >= n) break;
-    Row r;
-    if (a.use_icp) {
-      r.result = 0;
-      if (KIND == 0) icp_camera(a, S, L, p, r);
-      else icp_object(a, S, L, p, r);
-      accumulate(acc, cnt, r, a.robust);
-    }
-    if (a.use_rgb) {
-      r.result = 0;
-      rgb_row(a, S, rV, L, p, w, h, r);
-      accumulate(acc, cnt, r, a.robust);
-    }
+  // object problems: a tile that cannot hold a valid row skips its pixels
+  bool live = true;
+  if (KIND == 1) {
+    __shared__ int s_live;
+    if (threadIdx.x == 0) s_live = object_tile_live(a, S, L, blockIdx.x, w, n) ? 1 : 0;
+    __syncthreads();
+    live = s_live != 0;
   }
+  // FP64 from the warp level up
   __shared__ double sh[GN_THREADS / 32][32];
   __shared__ float red[GN_THREADS / 32][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  sh[warp][lane] = warp_sum_fp64(acc, cnt, red[warp], lane);
+  if (live) {
+    float acc[29];
+#pragma unroll
+    for (int i = 0; i < 29; ++i) acc[i] = 0.f;
+    int cnt[3] = {0, 0, 0};
+    const F3* rV = a.rV[s];
+    const int ppt = gn_pix(L);
+#pragma unroll 1
+    for (int k = 0; k < ppt; ++k) {
+      const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
+      if (p >= n) break;
+      Row r;
+      if (a.use_icp) {
+        r.result = 0;
+        if (KIND == 0) icp_camera(a, S, L, p, r);
+        else icp_object(a, S, L, p, r);
+        accumulate(acc, cnt, r, a.robust);
+      }
+      if (a.use_rgb) {
+        r.result = 0;
+        rgb_row(a, S, rV, L, p, w, h, r);
+        accumulate(acc, cnt, r, a.robust);
+      }
+    }
+    sh[warp][lane] = warp_sum_fp64(acc, cnt, red[warp], lane);
+  } else {
+    sh[warp][lane] = 0.0;
+  }
   __syncthreads();
   __shared__ bool last;
   if (threadIdx.x < 32) {
@@ -1273,6 +1401,8 @@ int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double
     invTf = inverse(Tf);
   }
   const GNArgs a = make_args(ctx, L, 0);
+  if (slot != 0)
+    if (int rc = tile_depth_range(ctx)) return rc;
   // the ticket must be zero when the launch starts (the last CTA also resets it)
   MF_CUDA(cudaMemsetAsync(scratch + EVAL_TICKET_OFF, 0, sizeof(unsigned), ctx->stream));
   if (slot == 0)
