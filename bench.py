@@ -44,8 +44,14 @@ UNEVEN = ("640x480 RGB-D, background 512^3@1cm + 12 objects with octrees of 32^3
 UNEVEN_STEPS = 8
 
 
+ADJ_PAIRS, ADJ_PAIRS_HD, HD = 64, 16, (1280, 720)
+
+
 def scene_for(rank, n_frames, workload="multi"):
     from mid_fusion_b200.scene import make_scene
+    if workload == "hd":  # the 1280x720 variant of the multi scene (fx = fy = 1050)
+        return make_scene("multi", HD[0], HD[1], n_frames=n_frames, seed=11 + rank, n_objects=3,
+                          bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512)
     if workload == "uneven":
         return make_scene("uneven", W, H, n_frames=n_frames, seed=23 + rank, n_objects=12)
     return make_scene("multi", W, H, n_frames=n_frames, seed=11 + rank, n_objects=3,
@@ -138,6 +144,7 @@ def run_ours(args, rank, world, local_rank):
     jobs = {main: n_frames}
     if do_uneven:
         jobs["uneven"] = n_uneven
+        jobs["hd"] = 3
     rendered = render_frames(rank, jobs, args.workers)  # before the first CUDA call
     frames = rendered[main]
     torch.cuda.set_device(local_rank)
@@ -247,6 +254,30 @@ def run_ours(args, rank, world, local_rank):
             c.close()
         del ins
 
+    # ---- adjoint of the camera cost: perturbed (pose, frame) pairs
+    adjoint = None
+    if do_uneven:
+        adjoint = {"640x480": run_adjoint(ctx_b, s, frames, [p[0] for p in poses_b], ADJ_PAIRS,
+                                          dev, torch),
+                   "1280x720": None}
+        sh = scene_for(rank, 3, "hd")
+        ctx_h = Context(HD[0], HD[1], k=sh.k, pool_blocks=args.pool_blocks, batched=True,
+                        robust="huber")
+        for inst, T in zip(sh.instances, sh.volume_poses(0)):
+            ctx_h.add_instance(inst.size, inst.dim, T, inst.label)
+        from mid_fusion_b200.scene import generalize_masks
+        hd_frames = rendered["hd"]
+        for f in range(2):
+            d, rgb, lab = hd_frames[f]
+            for i, P in enumerate(sh.volume_poses(f)):
+                ctx_h.set_instance_pose(i, P)
+            ctx_h.set_camera_pose(sh.cam_poses[f])
+            ctx_h.upload(d, rgb, generalize_masks(lab, [i.label for i in sh.instances]))
+            ctx_h.integrate(list(range(len(sh.instances))))
+        adjoint["1280x720"] = run_adjoint(ctx_h, sh, hd_frames, sh.cam_poses, ADJ_PAIRS_HD, dev,
+                                          torch)
+        ctx_h.close()
+
     # ---- e2e through the C ABI from pinned host buffers
     import ctypes
     ctx_e = make_ctx(True)
@@ -290,7 +321,47 @@ def run_ours(args, rank, world, local_rank):
     return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
                 status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
                 ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
-                n_inst=len(s.instances), uneven=uneven)
+                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint)
+
+
+def run_adjoint(ctx, scene, frames, poses, pairs, dev, torch):
+    """Cost + dE/d twist + dE/d tsdf (mf_camera_cost) over `pairs` (reference
+    frame, live frame) pairs of consecutive frames, the live pose perturbed by
+    N(0, 5 mm) per axis and N(0, 0.5 deg) per axis; device time per pair with
+    CUDA events (the frames' preprocessing outside the timed region)."""
+    from mid_fusion_b200.scene import se3_exp
+    rng = np.random.default_rng(5)
+    _, n = ctx.pool_tsdf()
+    grad = torch.zeros(n, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    times, rows = [], []
+    for b in range(pairs):
+        f = 1 + b % (len(frames) - 1)
+        ctx.set_camera_pose(poses[f - 1])
+        ctx.upload(frames[f - 1][0], frames[f - 1][1], None)
+        ctx.preprocess()
+        ctx.set_ref_from_current()
+        ctx.upload(frames[f][0], frames[f][1], None)
+        ctx.preprocess()
+        xi = np.concatenate([rng.normal(size=3) * 0.005,
+                             rng.normal(size=3) * np.radians(0.5)])
+        T = (se3_exp(xi) @ np.asarray(poses[f], np.float64)).astype(np.float32)
+        grad.zero_()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, _, nr = ctx.camera_cost(T, grad.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        rows.append(nr)
+    ms = float(np.mean(times[2:] if len(times) > 4 else times))
+    return {"pairs": pairs, "frame": [scene.width, scene.height],
+            "ms_per_pair": round(ms, 4), "pairs_per_s": round(1e3 / ms, 2),
+            "rows_per_pair": int(np.mean(rows)),
+            "what": "raycast of every instance, level-0 camera ICP + photometric Huber cost, "
+                    "dE/d twist, dE/d tsdf through the raycast (FP32, FP64 sums)",
+            "status_flags": ctx.status()}
 
 
 def run_reference(args):
@@ -452,6 +523,7 @@ def main():
                   "ms_per_step": round(1e3 * total_p / args.steps, 4)},
         "batched_over_plain": round(total_p / total_b, 3),
         "uneven12": r.get("uneven"),
+        "adjoint": r.get("adjoint"),
         "pose_diff_batched_vs_plain_m": r["dpos"],
         "camera_err_vs_gt_m": r["gt_err"],
         "e2e": {"value": round(value_e, 2), "unit": "frames/s",

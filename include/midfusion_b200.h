@@ -38,6 +38,7 @@ extern "C" {
 #define MF_STATUS_ALLOC_OVERFLOW 2  /* more keys than the reference's list holds */
 #define MF_STATUS_RAY_GUARD 4
 #define MF_STATUS_GN_FALLBACK 8     /* a 6x6 system used the truncated eigen solve */
+#define MF_STATUS_ADJOINT 16        /* mf_camera_cost skipped the TSDF adjoint of a ray */
 
 /* Robust kernels of Tracking::calc_robust_weight,
  * apps/kfusion/src/cpp/tracking/tracking.cpp:1504-1532 (enum RobustW,
@@ -163,6 +164,26 @@ int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, doubl
  *    Calls from one thread are serialised, because the call synchronises. */
 int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose,
                          double* sums);
+/* No counterpart in the reference: the camera-tracking cost and its adjoint.
+ * Raycasts every instance at the current camera pose, which is the reference
+ * pose T_w_r (the model maps are replaced), then evaluates at pyramid level 0
+ *   E = sum_p rho(e_icp(p)) + rho(e_rgb(p))
+ * with the camera rows of mf_track_camera (robust kernel of the config) for
+ * the live frame of the last mf_preprocess at pose T_live, against the
+ * reference frame of mf_set_ref_from_current.  out[0] = E; out[1..6] =
+ * dE/d(twist) for T_live <- exp(twist) T_live, twist = (v, w), at twist = 0;
+ * out[7] = the number of valid rows.  When d_grad_tsdf is not NULL (device
+ * memory, one float per pool voxel, indexed like mf_pool_tsdf) dE/d(tsdf) is
+ * ADDED to it: through the model vertex, the model normal and the rendered
+ * photometric reference depth of every pixel.  Voxel colours do not enter E.
+ * The camera GN problem's state is overwritten.  Synchronises. */
+int mf_camera_cost(mf_context* ctx, const float T_live[16], double* out, float* d_grad_tsdf);
+/* The pool's TSDF values: a device pointer to pool capacity x 512 floats
+ * (voxel v of pool slot s at s * 512 + v). */
+int mf_pool_tsdf(mf_context* ctx, float** d_tsdf, long long* n);
+/* Which block each used pool slot holds: 4 ints per slot (corner voxel x, y,
+ * z and the instance id), for slots 0 .. *n - 1 (at most `cap` written). */
+int mf_pool_slots(mf_context* ctx, int32_t* meta, long long cap, long long* n);
 /* Pyramid planes of the current frame: which 0 depth, 1 intensity, 2 vertex,
  * 3 normal, 4 x-gradient, 5 y-gradient, 6 ICP covariance, 7 camera reference
  * vertex (float3 planes are 3 floats per pixel). */

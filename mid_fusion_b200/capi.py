@@ -34,7 +34,7 @@ EXPORTS = [
     "mf_preprocess", "mf_set_ref_from_current", "mf_track_camera", "mf_track_objects",
     "mf_track_info", "mf_track_eval", "mf_download_pyramid", "mf_process_frame",
     "mf_process_frame_device", "mf_get_poses", "mf_frame_stats", "mf_set_graphs",
-    "mf_profile", "mf_track_eval_static",
+    "mf_profile", "mf_track_eval_static", "mf_camera_cost", "mf_pool_tsdf", "mf_pool_slots",
 ]
 
 
@@ -239,6 +239,31 @@ class Context:
         self._check(self.lib.mf_track_eval(self.h, slot, level, _ptr(p, np.float32),
                                            _ptr(sums, np.float64)))
         return sums
+
+    def camera_cost(self, T_live, grad_tsdf_ptr=None):
+        """E, dE/d twist (6) and the number of rows (mf_camera_cost); when
+        grad_tsdf_ptr (a device address of pool_size() floats) is given,
+        dE/d tsdf is added there."""
+        out = np.zeros(8, np.float64)
+        self._check(self.lib.mf_camera_cost(self.h, _ptr(_m4(T_live), np.float32),
+                                            _ptr(out, np.float64),
+                                            C.c_void_p(grad_tsdf_ptr) if grad_tsdf_ptr else None))
+        return out[0], out[1:7].copy(), int(out[7])
+
+    def pool_slots(self):
+        """(n, 4) int32: corner voxel x, y, z and instance of each used pool slot."""
+        n = C.c_longlong()
+        self._check(self.lib.mf_pool_slots(self.h, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 4), np.int32)
+        self._check(self.lib.mf_pool_slots(self.h, _ptr(out, np.int32), n.value, C.byref(n)))
+        return out[:n.value]
+
+    def pool_tsdf(self):
+        """(device address, length) of the pool's TSDF values."""
+        p = C.c_void_p()
+        n = C.c_longlong()
+        self._check(self.lib.mf_pool_tsdf(self.h, C.byref(p), C.byref(n)))
+        return p.value, n.value
 
     def track_eval_static(self, slot, level, pose=None):
         """mf_track_eval with static device scratch (allocates nothing)."""

@@ -555,6 +555,35 @@ int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose
   return track_eval_static(ctx, slot, level, pose, sums);
 }
 
+int mf_camera_cost(mf_context* ctx, const float* T_live, double* out, float* d_grad_tsdf) {
+  if (check(ctx) || !T_live || !out) return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  return camera_cost(ctx, T_live, d_grad_tsdf ? 1 : 0, out, d_grad_tsdf);
+}
+
+int mf_pool_slots(mf_context* ctx, int32_t* meta, long long cap, long long* n) {
+  if (check(ctx) || !n || (cap > 0 && !meta)) return MF_E_ARG;
+  int used = 0;
+  MF_CUDA(cudaMemcpyAsync(&used, ctx->pool.count, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  used = std::min(used, ctx->pool.cap);
+  *n = used;
+  const long long m = std::min<long long>(used, cap);
+  if (m > 0)
+    MF_CUDA(cudaMemcpyAsync(meta, ctx->pool.meta, sizeof(int4) * m, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+int mf_pool_tsdf(mf_context* ctx, float** d_tsdf, long long* n) {
+  if (check(ctx) || !d_tsdf || !n) return MF_E_ARG;
+  *d_tsdf = ctx->pool.tsdf;
+  *n = (long long)ctx->pool.cap * 512;
+  return MF_OK;
+}
+
 int mf_download_pyramid(mf_context* ctx, int level, int which, float* out) {
   if (check(ctx) || !out || level < 0 || level >= ctx->cfg.pyramid_levels) return MF_E_ARG;
   return track_download_level(ctx, level, which, out);

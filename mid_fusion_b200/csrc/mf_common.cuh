@@ -199,6 +199,7 @@ enum Status : int {
   ST_ALLOC_OVERFLOW = 2,   // more samples emitted than the reference list holds
   ST_RAY_GUARD = 4,        // ray iterator hit its iteration guard
   ST_GN_SINGULAR = 8,      // a normal-equation system fell back to the eigen solve
+  ST_ADJOINT = 16,         // a raycast adjoint skipped a ray (too many samples) or its replay differed
 };
 
 // ----------------------------------------------------------------- layout

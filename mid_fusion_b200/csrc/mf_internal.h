@@ -127,6 +127,9 @@ int track_objects(Context* ctx, const IdList& ids);
 int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double* sums);
+int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8, float* d_grad);
+int stage_raycast_adjoint(Context* ctx, const IdList& ids, const double* gV, const double* gN,
+                          float* d_grad);
 int track_download_level(Context* ctx, int L, int which, float* out);
 void track_save_prev_camera(Context* ctx);
 bool track_has_ref(Context* ctx);

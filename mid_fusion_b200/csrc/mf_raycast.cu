@@ -261,4 +261,291 @@ int stage_raycast(Context* ctx, const IdList& ids, float epsilon) {
   return MF_OK;
 }
 
+// ------------------------------------------------------------------------
+// Adjoint of the composite raycast (no reference counterpart): carries
+// dE/d(model vertex) and dE/d(model normal) of a pixel back to the TSDF values
+// of the winning instance's voxels.  The vertex is T_w_o (o + d t*), where the
+// march (raycast_volume) ends with the secant step
+//   t* = t_k + s_{k-1} f_k / (f_{k-1} - f_k),
+// every sample position depends on the earlier step lengths
+// s_j = max(mu f_j, voxel), and every sample value f_j is a voxel read (get) or
+// a trilinear interpolation.  The backward sweep needs the samples in reverse:
+// the forward march is replayed once with a checkpoint of the sample position
+// every ADJ_SEG samples, and each segment is replayed again, from its checkpoint,
+// just before it is swept; no per-sample state is stored beyond one segment.
+// The normal is normalize(R grad(tsdf, hit)); its adjoint reaches the 32 taps
+// of the central differences and, through their trilinear weights, the hit.
+constexpr int ADJ_SEG = 32;      // samples per checkpoint
+constexpr int ADJ_MAX_CP = 64;   // checkpoints: rays of up to 2048 samples
+
+// Scatters g * d f / d tsdf of the trilinear interpolation at `pos`
+// (volume_interp_m) and returns d f / d t along `dir`.
+__device__ float interp_adjoint(const Pool& P, const Volume& V, BlockMemo& m, F3 pos, F3 dir,
+                                float g, float* __restrict__ grad) {
+  const float inv = V.size / V.dim;
+  const F3 pv = mk3(pos.x * inv, pos.y * inv, pos.z * inv);
+  const F3 fl = floor3(pv);
+  const I3 base = to_i3(fl);
+  const F3 f = mk3(pv.x - fl.x, pv.y - fl.y, pv.z - fl.z);
+  const int lx = imx(base.x, 0), ly = imx(base.y, 0), lz = imx(base.z, 0);
+  float dfx = 0.f, dfy = 0.f, dfz = 0.f;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int x = lx + (i & 1), y = ly + ((i >> 1) & 1), z = lz + (i >> 2);
+    const int ts = memo_slot(V, m, x, y, z);
+    const float val = ts < 0 ? 1.f : __ldg(P.tsdf + (size_t)ts * 512 + voxel_index(x, y, z));
+    const float wx = (i & 1) ? f.x : 1.f - f.x, wy = (i & 2) ? f.y : 1.f - f.y,
+                wz = (i & 4) ? f.z : 1.f - f.z;
+    if (ts >= 0 && g != 0.f)
+      atomicAdd(grad + (size_t)ts * 512 + voxel_index(x, y, z), g * wx * wy * wz);
+    dfx += val * ((i & 1) ? 1.f : -1.f) * wy * wz;
+    dfy += val * ((i & 2) ? 1.f : -1.f) * wx * wz;
+    dfz += val * ((i & 4) ? 1.f : -1.f) * wx * wy;
+  }
+  return inv * (dfx * dir.x + dfy * dir.y + dfz * dir.z);
+}
+
+// The same for one sample of raycast_volume's loop: a voxel read, or the
+// interpolation when the read lies in [-0.5, 0.1).
+__device__ float sample_adjoint(const Pool& P, const Volume& V, BlockMemo& m, F3 pos, F3 dir,
+                                float g, float* __restrict__ grad) {
+  const float inv = V.size / V.dim;
+  const I3 s = to_i3(mk3(pos.x * inv, pos.y * inv, pos.z * inv));
+  const int sl = memo_slot(V, m, s.x, s.y, s.z);
+  const float fv = sl < 0 ? 1.f : __ldg(P.tsdf + (size_t)sl * 512 + voxel_index(s.x, s.y, s.z));
+  if (fv < 0.1f && fv >= -0.5f) return interp_adjoint(P, V, m, pos, dir, g, grad);
+  if (sl >= 0 && g != 0.f) atomicAdd(grad + (size_t)sl * 512 + voxel_index(s.x, s.y, s.z), g);
+  return 0.f;
+}
+
+// The sample value of raycast_volume's loop at `pos`.
+__device__ __forceinline__ float march_value(const Pool& P, const Volume& V, BlockMemo& m,
+                                             F3 pos) {
+  const float inv = V.size / V.dim;
+  const I3 s = to_i3(mk3(pos.x * inv, pos.y * inv, pos.z * inv));
+  float f = tsdf_at_m(P, V, m, s.x, s.y, s.z);
+  if (f < 0.1f && f >= -0.5f) f = volume_interp_m<0>(P, V, pos, m);
+  return f;
+}
+
+// Replays raycast_volume and sweeps its march backwards with dE/dt* = g_t.
+// Returns 1 when done, 0 when the replay found no hit (nothing to do), -1 when
+// the march is longer than the checkpoints cover (the ray is skipped).
+__device__ __noinline__ int march_adjoint(const Pool& P, const Volume& V, F3 origin,
+                                          F3 direction, float nearPlane, float farPlane,
+                                          float mu, float step, float largestep, float g_t,
+                                          float* __restrict__ grad, F3* hit) {
+  const F3 invR = mk3(1.0f / direction.x, 1.0f / direction.y, 1.0f / direction.z);
+  const F3 tbot = (-1.f * invR) * origin;
+  const F3 ttop = invR * (V.dim - origin);
+  const F3 tmin = mk3(fmn(ttop.x, tbot.x), fmn(ttop.y, tbot.y), fmn(ttop.z, tbot.z));
+  const F3 tmax = mk3(fmx(ttop.x, tbot.x), fmx(ttop.y, tbot.y), fmx(ttop.z, tbot.z));
+  const float largest_tmin = fmx(fmx(tmin.x, tmin.y), fmx(tmin.x, tmin.z));
+  const float smallest_tmax = fmn(fmn(tmax.x, tmax.y), fmn(tmax.x, tmax.z));
+  const float tnear = fmx(largest_tmin, nearPlane);
+  const float tfar = fmn(smallest_tmax, farPlane);
+  const float inv = V.size / V.dim;
+  if (!(tnear < tfar)) return 0;
+  BlockMemo memo;
+  float t = tnear, stepsize = largestep;
+  F3 position = origin + direction * t;
+  float f_t = volume_interp_m<0>(P, V, position, memo), f_tt = 0;
+  if (!(f_t > 0)) return 0;
+  const F3 p0 = position;
+  F3 cp_p[ADJ_MAX_CP];  // sample position at each checkpoint
+  int k = 0;
+  for (int guard = 0; t < tfar && guard < (1 << 20); t += stepsize, ++guard) {
+    if (k % ADJ_SEG == 0) {
+      const int c = k / ADJ_SEG;
+      if (c >= ADJ_MAX_CP) return -1;
+      cp_p[c] = position;
+    }
+    const I3 s = to_i3(mk3(position.x * inv, position.y * inv, position.z * inv));
+    f_tt = tsdf_at_m(P, V, memo, s.x, s.y, s.z);
+    if (f_tt < 0.1f && f_tt >= -0.5f) f_tt = volume_interp_m<0>(P, V, position, memo);
+    if (f_tt < 0) break;
+    stepsize = fmx(f_tt * mu, step);
+    position = position + stepsize * direction;
+    f_t = f_tt;
+    ++k;
+  }
+  if (!(f_tt < 0)) return 0;
+  {
+    const float th = t + stepsize * f_tt / (f_t - f_tt);
+    *hit = origin + direction * th;
+  }
+  // t* = t_k + s f_k / (a - f_k) with s = s_{k-1} and a = f_{k-1} (for k = 0 the
+  // constant largestep and the interpolation that opened the march)
+  const float den = f_t - f_tt;
+  const float g_fk = g_t * stepsize * f_t / (den * den);
+  const float g_s = g_t * f_tt / den;
+  const float g_a = -g_t * stepsize * f_tt / (den * den);
+  float GT = g_t;  // dE/dt_j, carried backwards
+  float seg_f[ADJ_SEG];
+  F3 seg_p[ADJ_SEG];
+  for (int c = k / ADJ_SEG; c >= 0; --c) {
+    // replay samples j0 .. j1 of this segment from its checkpoint
+    const int j0 = c * ADJ_SEG, j1 = min(j0 + ADJ_SEG - 1, k);
+    F3 pos = cp_p[c];
+    for (int j = j0; j <= j1; ++j) {
+      seg_p[j - j0] = pos;
+      const float f = march_value(P, V, memo, pos);
+      seg_f[j - j0] = f;
+      if (j < j1) pos = pos + fmx(f * mu, step) * direction;
+    }
+    for (int j = j1; j >= j0; --j) {
+      float gf;
+      if (j == k) {
+        gf = g_fk;
+      } else {
+        // t_{j+1} = t_j + s_j, s_j = max(mu f_j, voxel)
+        const float gsj = GT + (j == k - 1 ? g_s : 0.f);
+        gf = (seg_f[j - j0] * mu > step ? mu * gsj : 0.f) + (j == k - 1 ? g_a : 0.f);
+      }
+      GT += gf * sample_adjoint(P, V, memo, seg_p[j - j0], direction, gf, grad);
+    }
+  }
+  if (k == 0)  // the opening interpolation was the secant's other end
+    (void)interp_adjoint(P, V, memo, p0, direction, g_a, grad);
+  return 1;
+}
+
+// Adjoint of volume_grad at pos: scatters the 32 taps' share of gG (dE/dG)
+// and returns dE/d pos through the trilinear weights.
+__device__ F3 grad_adjoint(const Pool& P, const Volume& V, F3 pos_m, F3 gG,
+                           float* __restrict__ grad) {
+  const float inv = V.size / V.dim;
+  const F3 pos = mk3(pos_m.x * inv, pos_m.y * inv, pos_m.z * inv);
+  const F3 fl = floor3(pos);
+  const I3 base = to_i3(fl);
+  const F3 f = mk3(pos.x - fl.x, pos.y - fl.y, pos.z - fl.z);
+  const int s1 = V.size - 1;
+  const int cx[4] = {imx(base.x - 1, 0), imx(base.x, 0), imn(base.x + 1, s1), imn(base.x + 2, s1)};
+  const int cy[4] = {imx(base.y - 1, 0), imx(base.y, 0), imn(base.y + 1, s1), imn(base.y + 2, s1)};
+  const int cz[4] = {imx(base.z - 1, 0), imx(base.z, 0), imn(base.z + 1, s1), imn(base.z + 2, s1)};
+  const float sc = V.dim / V.size * 0.5f;
+  const F3 gr = gG * sc;  // dE / d(gr) before the scale
+  auto slot = [&](int a, int b, int c) { return block_slot(V, cx[a], cy[b], cz[c]); };
+  auto val = [&](int a, int b, int c) {
+    const int sl = slot(a, b, c);
+    return sl < 0 ? 1.f : __ldg(P.tsdf + (size_t)sl * 512 + voxel_index(cx[a], cy[b], cz[c]));
+  };
+  auto add = [&](int a, int b, int c, float g) {
+    const int sl = slot(a, b, c);
+    if (sl >= 0 && g != 0.f) atomicAdd(grad + (size_t)sl * 512 + voxel_index(cx[a], cy[b], cz[c]), g);
+  };
+  const float wx[2] = {1.f - f.x, f.x}, wy[2] = {1.f - f.y, f.y}, wz[2] = {1.f - f.z, f.z};
+  F3 gf = mk3(0.f);  // dE/d(fractional position)
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b)
+      for (int c = 0; c < 2; ++c) {
+        const float w = wx[a] * wy[b] * wz[c];
+        const float sx = a ? 1.f : -1.f, sy = b ? 1.f : -1.f, sz = c ? 1.f : -1.f;
+        const float dx = val(2 + a, 1 + b, 1 + c) - val(a, 1 + b, 1 + c);
+        const float dy = val(1 + a, 2 + b, 1 + c) - val(1 + a, b, 1 + c);
+        const float dz = val(1 + a, 1 + b, 2 + c) - val(1 + a, 1 + b, c);
+        add(2 + a, 1 + b, 1 + c, gr.x * w); add(a, 1 + b, 1 + c, -gr.x * w);
+        add(1 + a, 2 + b, 1 + c, gr.y * w); add(1 + a, b, 1 + c, -gr.y * w);
+        add(1 + a, 1 + b, 2 + c, gr.z * w); add(1 + a, 1 + b, c, -gr.z * w);
+        const float s = gr.x * dx + gr.y * dy + gr.z * dz;
+        gf.x += s * sx * wy[b] * wz[c];
+        gf.y += s * sy * wx[a] * wz[c];
+        gf.z += s * sz * wx[a] * wy[b];
+      }
+  return gf * inv;
+}
+
+// One thread per model pixel; pixels whose map adjoints are zero return.
+__global__ void __launch_bounds__(128)
+raycast_adjoint_kernel(Pool pool, const Volume* __restrict__ vols,
+                       const InstFrame* __restrict__ frames, IdList ids, RayArgs a,
+                       const double* __restrict__ gV, const double* __restrict__ gN,
+                       float* __restrict__ grad, int* __restrict__ status) {
+  const int x = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
+  if (x >= a.W || y >= a.H) return;
+  const int p = x + y * a.W;
+  const F3 gv = mk3((float)gV[3 * p], (float)gV[3 * p + 1], (float)gV[3 * p + 2]);
+  const F3 gn = mk3((float)gN[3 * p], (float)gN[3 * p + 1], (float)gN[3 * p + 2]);
+  if (gv.x == 0.f && gv.y == 0.f && gv.z == 0.f && gn.x == 0.f && gn.y == 0.f && gn.z == 0.f)
+    return;
+  __shared__ int s_slot[8 * 128];
+  // replay the composite (raycast_objects_kernel) to find the winner
+  float nearest = 1.0e3f;
+  double high_fg = 0.f;
+  int win = -1;
+  F4 whit{0, 0, 0, 0};
+  float wnfar = 0.f, wtmin = 0.f;
+  F3 wdir = mk3(0.f);
+  const M4 view = frames[ids.v[0]].view;
+  const F3 w_dir = rotate(view, mk3((float)x, (float)y, 1.f));
+  for (int o = 0; o < ids.n; ++o) {
+    const int i = ids.v[o];
+    const Volume& V = vols[i];
+    const InstFrame& F = frames[i];
+    const float step = V.dim / V.size;
+    const F3 o_dir = normalize(rotate(F.inv_T_w_o, w_dir));
+    const float nfar = fmn(nearest, a.farPlane);
+    const float t_min = ray_first_block(V, F.o_origin, o_dir, a.nearPlane, nfar, a.epsilon, status);
+    const F4 hit = t_min > 0.f
+                       ? raycast_volume(pool, V, F.o_origin, o_dir,
+                                        t_min * V.dim / (unsigned)V.size, nfar, a.mu, step,
+                                        step * 8)
+                       : F4{0, 0, 0, 0};
+    const float hd = F.label == 0 ? hit.w + 0.05f : hit.w;
+    if (hd > nearest) continue;
+    const double fg = volume_interp(pool, V, mk3(hit.x, hit.y, hit.z), 1);
+    if (fg <= 0.5f) continue;
+    if (hd == nearest) {
+      if (!(fg > high_fg)) continue;
+    } else if (hd < nearest) {
+      nearest = hd;
+    } else {
+      continue;
+    }
+    high_fg = fg;
+    win = i; whit = hit; wnfar = nfar; wtmin = t_min; wdir = o_dir;
+  }
+  if (win < 0) return;
+  const Volume& V = vols[win];
+  const InstFrame& F = frames[win];
+  const F3 X = mk3(whit.x, whit.y, whit.z);
+  const F3 vm = xform(F.T_w_o, X);
+  const F3 mv = a.vertex[p];
+  if (vm.x != mv.x || vm.y != mv.y || vm.z != mv.z) {  // the replay must be exact
+    atomicOr(status, ST_ADJOINT);
+    return;
+  }
+  F3 gX = rotate_t(gv, F.T_w_o);  // dE/dX from the vertex
+  if (gn.x != 0.f || gn.y != 0.f || gn.z != 0.f) {
+    const F3 G = volume_grad(pool, V, X, s_slot + threadIdx.x, 128);
+    const float gl = length(G);
+    if (gl > 0.f) {
+      const F3 n = normalize(rotate(F.T_w_o, G));
+      const F3 gRG = (gn - dot(n, gn) * n) * (1.f / gl);
+      gX = gX + grad_adjoint(pool, V, X, rotate_t(gRG, F.T_w_o), grad);
+    }
+  }
+  if (whit.w == 0.f) return;  // a miss claimed by the corner's foreground: no march
+  const float step = V.dim / V.size;
+  F3 rep;
+  const int r = march_adjoint(pool, V, F.o_origin, wdir, wtmin * V.dim / (unsigned)V.size,
+                              wnfar, a.mu, step, step * 8, dot(wdir, gX), grad, &rep);
+  if (r < 0 || (r == 1 && (rep.x != X.x || rep.y != X.y || rep.z != X.z)))
+    atomicOr(status, ST_ADJOINT);
+}
+
+int stage_raycast_adjoint(Context* ctx, const IdList& ids, const double* gV, const double* gN,
+                          float* d_grad) {
+  if (ids.n == 0) return MF_OK;
+  const mf_config& c = ctx->cfg;
+  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H,
+            c.near_plane, c.far_plane, c.mu, ctx->ray_epsilon};
+  dim3 grid((ctx->W + 15) / 16, (ctx->H + 7) / 8);
+  raycast_adjoint_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
+                                                        ids, a, gV, gN, d_grad, ctx->d_status);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
 }  // namespace mf

@@ -79,6 +79,11 @@ struct TrackState {
   uint8_t* d_mask0 = nullptr;       // full-resolution ICP outlier mask
   float gaussian[5];
   std::vector<void*> allocs;
+  // camera cost and adjoint (allocated on first use)
+  double* d_gmodel = nullptr;       // 2 x 3 x W x H: dE/d model vertex, dE/d model normal
+  double* d_cost_part = nullptr;    // per-CTA partials of the cost rows, 8 each
+  double* d_cost = nullptr;         // 8: cost, dE/d twist (6), rows
+  int cost_blocks = 0;
 };
 
 // ------------------------------------------------------------------ preprocessing
@@ -1417,5 +1422,221 @@ int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
   return MF_OK;
 }
+
+// ------------------------------------------------------------------------
+// Camera cost at level 0 and its adjoint (no reference counterpart).
+//
+//   E(T_live, tsdf) = sum_p rho(e_icp(p)) + rho(e_rgb(p))
+//
+// with the camera rows of gn_iter_kernel (the same validity tests, residuals,
+// whitening and robust kernel) at level 0.  Per valid row the kernel adds
+// rho'(e) de/d(twist) -- the exact derivative for a left perturbation
+// T <- exp(twist) T_live, with the bilinear image gradient of the photometric
+// lookup -- and, when asked, rho'(e) de/d(model vertex, normal) into per
+// model-pixel FP64 buffers, which the raycast adjoint then carries back to the
+// TSDF voxels.  ICP: e = ic n.(v_m - T v) with ic = (n^T P n)^(-1/2).
+// Photometric: e = ic_rgb (I_ref(p) - I_live(pi(K T^-1 T_w_r rv(p)))), where
+// the reference vertex rv(p) = d(p) K^-1 (x, y, 1) and d(p) is the depth of the
+// model vertex at p in the reference camera.
+struct CostOut {
+  double* partials;  // 8 per CTA: loss, dE/d twist (6), rows
+  double* gV;        // 3 per model pixel (may be null)
+  double* gN;
+  int want_grad;
+};
+
+__device__ __forceinline__ void atomic_add3(double* p, F3 v) {
+  atomicAdd(p, (double)v.x);
+  atomicAdd(p + 1, (double)v.y);
+  atomicAdd(p + 2, (double)v.z);
+}
+
+__global__ void __launch_bounds__(256)
+camera_cost_kernel(GNArgs a, CostOut c) {
+  const GNState& S = a.st[0];
+  const int w = a.pyr.w[0], h = a.pyr.h[0];
+  const int p = blockIdx.x * 256 + threadIdx.x;
+  float v[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // loss, grad[6], rows
+  if (p < w * h) {
+    // ---- ICP (icp_camera)
+    if (a.use_icp && !a.pyr.MASK[0][p]) {
+      const F3 nl = a.pyr.N[0][p];
+      if (nl.x != INVALIDF) {
+        const F3 pv = xform(S.Tf, a.pyr.V[a.cur][0][p]);
+        const F3 pp = xform(S.view, pv);
+        const float px = pp.x / pp.z, py = pp.y / pp.z;
+        if (!(px < 1 || px > (float)(unsigned)(a.W - 2) || py < 1 ||
+              py > (float)(unsigned)(a.H - 2) || isnan(px) || isnan(py))) {
+          const int q = (int)((unsigned)px + (unsigned)py * a.W);
+          const F3 rn = a.mnormal[q];
+          if (rn.x != INVALIDF) {
+            const F3 diff = a.mvertex[q] - pv;
+            const F3 pn = rotate(S.Tf, nl);
+            if (!(length(diff) > 0.1f) && !(dot(pn, rn) < 0.8f)) {
+              const F3 P = a.pyr.COV[0][p];
+              const float sig = rn.x * rn.x * P.x + rn.y * rn.y * P.y + rn.z * rn.z * P.z;
+              const float ic = sqrtf((float)(1.0 / (double)sig));
+              const float e = ic * dot(rn, diff);
+              float wt, loss;
+              robust(e, a.robust, wt, loss);
+              const float de = wt * e;  // rho'(e)
+              v[0] += loss;
+              v[7] += 1.f;
+              // de/d(v, w) = -ic (n, pv x n)
+              const F3 j1 = cross(pv, rn);
+              v[1] -= de * ic * rn.x; v[2] -= de * ic * rn.y; v[3] -= de * ic * rn.z;
+              v[4] -= de * ic * j1.x; v[5] -= de * ic * j1.y; v[6] -= de * ic * j1.z;
+              if (c.want_grad) {
+                atomic_add3(c.gV + 3 * (size_t)q, (de * ic) * rn);
+                // d ic / d n = -ic^3 (n * P)
+                const float ic3 = ic * ic * ic;
+                const F3 dic = mk3(-ic3 * rn.x * P.x, -ic3 * rn.y * P.y, -ic3 * rn.z * P.z);
+                atomic_add3(c.gN + 3 * (size_t)q, de * (ic * diff + dot(rn, diff) * dic));
+              }
+            }
+          }
+        }
+      }
+    }
+    // ---- photometric (rgb_row, camera, level 0)
+    if (a.use_rgb) {
+      const F3 rv = a.rV[0][p];
+      const F3 rl = a.pyr.V[1 - a.cur][0][p];
+      if (!(rv.z <= 0.f || rv.z == INVALIDF) && !(length(rv - rl) > 0.1f && rl.z > 0.f)) {
+        const M4 KL = camera_matrix(a.kL);
+        const F3 wv = xform(S.T_w_r, rv);
+        const F3 lv = xform(S.invTf, wv);
+        const F3 pr = rotate(KL, lv);
+        const float px = pr.x / pr.z, py = pr.y / pr.z;
+        if (!(px < 1 || px > (float)(unsigned)(w - 2) || py < 1 || py > (float)(unsigned)(h - 2) ||
+              isnan(px) || isnan(py))) {
+          const float* IL = a.pyr.I[a.cur][0];
+          const float fx0 = floorf(px), fy0 = floorf(py);
+          const int bx = (int)fx0, by = (int)fy0;
+          const float ax = px - fx0, ay = py - fy0;
+          const float i00 = IL[bx + by * w], i10 = IL[bx + 1 + by * w];
+          const float i01 = IL[bx + (by + 1) * w], i11 = IL[bx + 1 + (by + 1) * w];
+          const float residual = a.pyr.I[1 - a.cur][0][p] - bil(IL, w, px, py);
+          const float ic = a.inv_cov_rgb;
+          const float e = ic * residual;
+          float wt, loss;
+          robust(e, a.robust, wt, loss);
+          const float de = wt * e;
+          v[0] += loss;
+          v[7] += 1.f;
+          // d bil / d(px, py) of the bilinear interpolation itself
+          const float gx = (i10 - i00) * (1.f - ay) + (i11 - i01) * ay;
+          const float gy = (i01 - i00) * (1.f - ax) + (i11 - i10) * ax;
+          const float fxk = KL.r[0].x, fyk = KL.r[1].y, iz = 1.f / lv.z;
+          // de/d lv = -ic (gx dpx/dlv + gy dpy/dlv)
+          const F3 g_lv = -ic * mk3(gx * fxk * iz, gy * fyk * iz,
+                                     -(gx * fxk * lv.x + gy * fyk * lv.y) * iz * iz);
+          const F3 g3 = rotate_t(g_lv, S.invTf);  // in world coordinates
+          const F3 j1 = cross(wv, g3);
+          // lv = T^-1 exp(-twist) wv: de/d(v, w) = -(g3, wv x g3)
+          v[1] -= de * g3.x; v[2] -= de * g3.y; v[3] -= de * g3.z;
+          v[4] -= de * j1.x; v[5] -= de * j1.y; v[6] -= de * j1.z;
+          if (c.want_grad) {
+            // rv = d K^-1 (x, y, 1), d = (T_w_r^-1 v_m).z
+            const int x = p % w, y = p / w;
+            const F3 ray = rotate(inverse_camera_matrix(a.kL), mk3((float)x, (float)y, 1.f));
+            const float g_d = dot(rotate_t(g3, S.T_w_r), ray);
+            atomic_add3(c.gV + 3 * (size_t)p, (de * g_d) * xyz(S.inv_T_w_r.r[2]));
+          }
+        }
+      }
+    }
+  }
+  // FP64 block sums, fixed order
+  __shared__ double sh[8][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    double d = v[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_down_sync(0xffffffffu, d, o);
+    if (lane == 0) sh[warp][i] = d;
+  }
+  __syncthreads();
+  if (threadIdx.x < 8) {
+    double d = 0;
+    for (int i = 0; i < 8; ++i) d += sh[i][threadIdx.x];
+    c.partials[(size_t)blockIdx.x * 8 + threadIdx.x] = d;
+  }
+}
+
+__global__ void cost_sum_kernel(const double* __restrict__ partials, int n, double* out) {
+  if (threadIdx.x >= 8) return;
+  double d = 0;
+#pragma unroll 8
+  for (int b = 0; b < n; ++b) d += partials[(size_t)b * 8 + threadIdx.x];
+  out[threadIdx.x] = d;
+}
+
+// Camera problem (slot 0) for a cost evaluation: reference pose = the current
+// camera pose, live pose = T_live.
+__global__ void cost_setup_kernel(GNState* st, const float* __restrict__ Twc, F4 k, M4 Tl,
+                                  M4 iTl) {
+  GNState& S = st[0];
+  const M4 T = load_m4(Twc);
+  S.kind = 0; S.label = 0; S.inst = 0; S.done = 0; S.ticket = 0;
+  S.T_w_r = T;
+  S.inv_T_w_r = inverse(T);
+  S.view = mul(camera_matrix(k), S.inv_T_w_r);
+  S.Tf = Tl;
+  S.invTf = iTl;
+}
+
+int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8,
+                float* d_grad) {
+  if (!ctx->track || !ctx->track->have_ref) {
+    ctx->last_error = "mf_camera_cost: needs a reference frame (mf_set_ref_from_current) "
+                      "and a preprocessed live frame";
+    return MF_E_STATE;
+  }
+  TrackState& T = *ctx->track;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  const int nb = (int)((WH + 255) / 256);
+  if (!T.d_cost) {
+    MF_CUDA(cudaMalloc(&T.d_gmodel, sizeof(double) * 6 * WH));
+    MF_CUDA(cudaMalloc(&T.d_cost_part, sizeof(double) * 8 * nb));
+    MF_CUDA(cudaMalloc(&T.d_cost, sizeof(double) * 8));
+    T.allocs.push_back(T.d_gmodel);
+    T.allocs.push_back(T.d_cost_part);
+    T.allocs.push_back(T.d_cost);
+    T.cost_blocks = nb;
+  }
+  // the model maps of the current TSDF at the current (reference) camera pose
+  IdList all;
+  all.n = (int)ctx->inst.size();
+  for (int i = 0; i < all.n; ++i) all.v[i] = i;
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  if (int rc = stage_raycast(ctx, all, ctx->ray_epsilon)) return rc;
+  M4 Tl;
+  std::memcpy(&Tl, T_live16, 64);
+  const mf_config& c = ctx->cfg;
+  cost_setup_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc,
+                                              F4{c.k[0], c.k[1], c.k[2], c.k[3]}, Tl,
+                                              inverse(Tl));
+  MF_CUDA(cudaGetLastError());
+  IdList cam;
+  cam.n = 1;
+  cam.v[0] = 0;
+  if (int rc = render_reference(ctx, cam)) return rc;
+  double* gV = want_grad ? T.d_gmodel : nullptr;
+  double* gN = want_grad ? T.d_gmodel + 3 * WH : nullptr;
+  if (want_grad) MF_CUDA(cudaMemsetAsync(T.d_gmodel, 0, sizeof(double) * 6 * WH, ctx->stream));
+  const GNArgs a = make_args(ctx, 0, 0);
+  camera_cost_kernel<<<nb, 256, 0, ctx->stream>>>(a, CostOut{T.d_cost_part, gV, gN, want_grad});
+  cost_sum_kernel<<<1, 32, 0, ctx->stream>>>(T.d_cost_part, nb, T.d_cost);
+  MF_CUDA(cudaGetLastError());
+  if (want_grad && d_grad)
+    if (int rc = stage_raycast_adjoint(ctx, all, gV, gN, d_grad)) return rc;
+  MF_CUDA(cudaMemcpyAsync(out8, T.d_cost, sizeof(double) * 8, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
 
 }  // namespace mf

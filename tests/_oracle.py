@@ -191,6 +191,38 @@ class Impl:
         return mask.astype(bool)
 
 
+def camera_cost(vols, poses, labels, T_w_r, T_live, k, W, H, live, use_icp=True, use_rgb=True,
+                fp64=True, pert=(), near=0.1, far=4.0, mu=0.1, eps_size=None):
+    """The camera cost at level 0 (oracle/or_adjoint.cpp) for central
+    differences: vols are oracle volumes, live = dict of level-0 float arrays
+    vertex, normal, cov, intensity, ref_intensity, ref_vertex; pert = iterable
+    of (instance, x, y, z, delta) added to voxel TSDF values.  Returns (E, rows)."""
+    lib = oracle().lib
+    F64 = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+    f = lib.oa_camera_cost
+    f.restype = C.c_double
+    f.argtypes = [C.POINTER(P), FP, I32P, C.c_int, FP, F64, FP, C.c_int, C.c_int, C.c_float,
+                  C.c_float, C.c_float, C.c_float, FP, FP, FP, FP, FP, FP, C.c_int, C.c_int,
+                  C.c_int, I32P, F64, C.c_int, F64]
+    n = len(vols)
+    arr = (P * n)(*[v.h for v in vols])
+    pert = list(pert)
+    pidx = np.array([[p[0], p[1], p[2], p[3]] for p in pert], np.int32).reshape(-1, 4)
+    pval = np.array([p[4] for p in pert], np.float64)
+    if len(pert) == 0:
+        pidx = np.zeros((1, 4), np.int32)
+        pval = np.zeros(1, np.float64)
+    rows = np.zeros(1, np.float64)
+    eps = float(np.float32(2.0 ** -np.log2(eps_size or vols[0].size)))
+    E = f(arr, _f32(np.stack(poses).reshape(n, 16)), np.ascontiguousarray(labels, np.int32), n,
+          _f32(T_w_r), np.ascontiguousarray(np.asarray(T_live, np.float64).reshape(16)),
+          _f32(k), W, H, near, far, mu, eps, _f32(live["vertex"]), _f32(live["normal"]),
+          _f32(live["cov"]), _f32(live["intensity"]), _f32(live["ref_intensity"]),
+          _f32(live["ref_vertex"]), int(use_icp), int(use_rgb), int(fp64),
+          np.ascontiguousarray(pidx), np.ascontiguousarray(pval), len(pert), rows)
+    return float(E), int(rows[0])
+
+
 _cache = {}
 
 

@@ -1,0 +1,167 @@
+"""The camera cost and its hand-written adjoint (mf_camera_cost) against the
+oracle's FP64 cost (oracle/or_adjoint.cpp):
+
+* the cost itself (FP32 rows, FP64 sums) against FP64;
+* dE/d(twist) against FP64 central differences, and, for the ICP term alone,
+  against -J^T W r of the Gauss-Newton system (mf_track_eval);
+* dE/d(tsdf) through the composite raycast against FP64 central differences
+  on the voxels with the largest and on randomly chosen nonzero gradients.
+
+The cost is piecewise smooth: the ICP model lookup is the nearest pixel and
+every row has validity thresholds, so a step of 1e-6 already moves ~20 of
+30 000 rows to another model pixel and the difference quotient measures those
+jumps.  The central differences therefore use steps of 1e-8 .. 1e-9 in FP64
+(the median over three steps, against an occasional jump), where the quotient
+is stable to ~1e-6 relative.
+"""
+import numpy as np
+import pytest
+
+import _oracle as O
+from mid_fusion_b200 import build
+from mid_fusion_b200.capi import Context
+from mid_fusion_b200.scene import generalize_masks, make_scene, se3_exp
+
+pytestmark = pytest.mark.gpu
+
+W, H = 160, 120
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    build.build()
+
+
+def _setup(use_icp=True, use_rgb=True, seed=3):
+    import torch  # noqa: F401  (CUDA context for the gradient buffer)
+    s = make_scene("multi", W, H, n_frames=2, seed=seed, bg_size=256, obj_size=64, n_objects=2)
+    labels = [i.label for i in s.instances]
+    ctx = Context(W, H, k=s.k, pool_blocks=1 << 13, robust="huber", use_icp=use_icp,
+                  use_rgb=use_rgb)
+    orc = O.oracle()
+    vols = []
+    for inst, T in zip(s.instances, s.volume_poses(0)):
+        ctx.add_instance(inst.size, inst.dim, T, inst.label)
+        vols.append(orc.volume(inst.size, inst.dim))
+    T0 = s.cam_poses[0].astype(np.float32)
+    d, rgb, lab = s.render(0)
+    masks = generalize_masks(lab, labels)
+    ctx.set_camera_pose(T0)
+    ctx.upload(d, rgb, masks)
+    ctx.integrate(list(range(len(labels))))
+    rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+    for i, v in enumerate(vols):
+        v.integrate(d, rgb3, masks[i], T0, s.volume_poses(0)[i], s.k, 0.1)
+    ctx.preprocess()
+    live = {"ref_intensity": ctx.pyramid(0, 1).copy(), "ref_vertex": ctx.pyramid(0, 2).copy()}
+    ctx.set_ref_from_current()
+    d1, rgb1, lab1 = s.render(1)
+    ctx.upload(d1, rgb1, generalize_masks(lab1, labels))
+    ctx.preprocess()
+    live.update(vertex=ctx.pyramid(0, 2).copy(), normal=ctx.pyramid(0, 3).copy(),
+                cov=ctx.pyramid(0, 6).copy(), intensity=ctx.pyramid(0, 1).copy())
+    return s, ctx, vols, labels, T0, live
+
+
+def _oracle_cost(s, vols, labels, T0, T_live, live, use_icp=True, use_rgb=True, pert=()):
+    return O.camera_cost(vols, s.volume_poses(0), labels, T0, T_live, s.k, W, H, live,
+                         use_icp=use_icp, use_rgb=use_rgb, pert=pert)
+
+
+STEPS = (1e-8, 3e-9, 1e-9)
+
+
+def _central(f):
+    """Median over STEPS of (f(h) - f(-h)) / 2h."""
+    return float(np.median([(f(h) - f(-h)) / (2 * h) for h in STEPS]))
+
+
+def _live_pose(s):
+    rng = np.random.default_rng(7)
+    xi = np.concatenate([rng.normal(size=3) * 0.004, rng.normal(size=3) * 0.004])
+    return (se3_exp(xi) @ s.cam_poses[1]).astype(np.float32)
+
+
+@pytest.mark.parametrize("terms", ["icp+rgb", "icp", "rgb"])
+def test_cost_and_twist_gradient_match_fp64(terms):
+    use_icp, use_rgb = "icp" in terms, "rgb" in terms
+    s, ctx, vols, labels, T0, live = _setup(use_icp, use_rgb)
+    T = _live_pose(s)
+    E, g, rows = ctx.camera_cost(T)
+    E64, rows64 = _oracle_cost(s, vols, labels, T0, T.astype(np.float64), live, use_icp,
+                               use_rgb)
+    assert rows > 100
+    assert abs(rows - rows64) <= max(2, 2e-3 * rows64), (rows, rows64)
+    assert abs(E - E64) <= 2e-3 * E64, (E, E64)
+    fd = np.zeros(6)
+    T64 = T.astype(np.float64)
+    for i in range(6):
+        def f(h, i=i):
+            xi = np.zeros(6)
+            xi[i] = h
+            return _oracle_cost(s, vols, labels, T0, se3_exp(xi) @ T64, live, use_icp,
+                                use_rgb)[0]
+        fd[i] = _central(f)
+    scale = np.abs(fd).max()
+    np.testing.assert_allclose(g, fd, rtol=0, atol=2e-3 * scale, err_msg=f"{g} vs {fd}")
+    if terms == "icp":
+        # the ICP rows' J is the exact derivative: dE/d twist = -J^T W r
+        sums = ctx.track_eval(0, 0, T)
+        np.testing.assert_allclose(g, -sums[1:7], rtol=1e-5, atol=1e-6 * np.abs(g).max())
+    assert ctx.status() == 0
+    ctx.close()
+
+
+def test_tsdf_gradient_matches_fp64_central_differences():
+    import torch
+    s, ctx, vols, labels, T0, live = _setup()
+    T = _live_pose(s)
+    _, n = ctx.pool_tsdf()
+    grad = torch.zeros(n, dtype=torch.float32, device="cuda")
+    E, g, rows = ctx.camera_cost(T, grad.data_ptr())
+    assert ctx.status() == 0, "adjoint replay differed or skipped a ray"
+    gh = grad.cpu().numpy()
+    nz = np.flatnonzero(gh)
+    assert len(nz) > 100
+    slots = ctx.pool_slots()
+    rng = np.random.default_rng(0)
+    pick = list(nz[np.argsort(-np.abs(gh[nz]))[:8]]) + list(rng.choice(nz, 8, replace=False))
+    gmax = np.abs(gh).max()
+    for idx in pick:
+        slot, v = divmod(int(idx), 512)
+        cx, cy, cz, inst = slots[slot]
+        x, y, z = cx + (v & 7), cy + ((v >> 3) & 7), cz + (v >> 6)
+        fd = _central(lambda h: _oracle_cost(s, vols, labels, T0, T.astype(np.float64), live,
+                                             pert=[(inst, x, y, z, h)])[0])
+        assert abs(gh[idx] - fd) <= 0.02 * abs(fd) + 2e-3 * gmax, (inst, x, y, z, gh[idx], fd)
+    ctx.close()
+
+
+def test_autograd_function_matches_adjoint_and_fp64():
+    import torch
+    from mid_fusion_b200.autograd import CameraCost, pool_tsdf_tensor
+    s, ctx, vols, labels, T0, live = _setup()
+    base = _live_pose(s).astype(np.float64)
+    tsdf = pool_tsdf_tensor(ctx).requires_grad_()
+    twist = torch.tensor([0.002, -0.001, 0.0015, 0.003, -0.002, 0.001], dtype=torch.float64,
+                         requires_grad=True)
+    E = CameraCost.apply(twist, tsdf, ctx, base)
+    E.backward()
+    # the same pose through the direct entry point
+    T = (se3_exp(twist.detach().numpy()) @ base).astype(np.float32)
+    _, n = ctx.pool_tsdf()
+    ref = torch.zeros(n, dtype=torch.float32, device="cuda")
+    E2, _, _ = ctx.camera_cost(T, ref.data_ptr())
+    assert float(E.detach()) == E2
+    torch.testing.assert_close(tsdf.grad, ref, rtol=0, atol=1e-6 * float(ref.abs().max()))
+    # d E / d twist at a nonzero twist against FP64 central differences in twist
+    tw = twist.detach().numpy()
+    fd = np.zeros(6)
+    for i in range(6):
+        def f(h, i=i):
+            d = np.zeros(6)
+            d[i] = h
+            return _oracle_cost(s, vols, labels, T0, se3_exp(tw + d) @ base, live)[0]
+        fd[i] = _central(f)
+    np.testing.assert_allclose(twist.grad.numpy(), fd, rtol=0, atol=2e-3 * np.abs(fd).max())
+    ctx.close()
