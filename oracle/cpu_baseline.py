@@ -33,7 +33,7 @@ def _tests_path():
 
 
 class CpuPipeline:
-    def __init__(self, scene, use_reference=True):
+    def __init__(self, scene, use_reference=True, fp64=False):
         _tests_path()
         import _oracle as O
         self.O = O
@@ -48,7 +48,10 @@ class CpuPipeline:
         s = scene
         self.vols = [impl.volume(i.size, i.dim) for i in s.instances]
         self.labels = [i.label for i in s.instances]
-        self.trk = O.Tracker(s.width, s.height, s.k, robust=1, fp64=False)
+        self.trk = O.Tracker(s.width, s.height, s.k, robust=1, fp64=fp64)
+        # labels of the object instances: their model pixels are ICP outliers
+        # of the camera (trackLiveFrame's mask variant, tracking.cpp:1750-1879)
+        self.moving = [i.label for i in s.instances[1:]]
         H, W = s.height, s.width
         self.vertex = np.zeros((H, W, 3), np.float32)
         self.normal = np.zeros((H, W, 3), np.float32)
@@ -63,6 +66,7 @@ class CpuPipeline:
         self.trk.set_frame(rgb, depth)
         if self.frame > 0:
             T_prev = self.T
+            self.trk.set_mask((np.isin(self.label_img, self.moving) * 255).astype(np.uint8))
             self.T = self.trk.track_camera(T_prev, T_prev, self.vertex,
                                            self.normal).astype(np.float32)
             for i in range(1, len(self.vols)):
