@@ -134,6 +134,12 @@ int mf_set_ref_from_current(mf_context* ctx);
  * updated in place on the device.  Pixels whose model label has its bit set in
  * `moving_labels` are excluded from ICP (the dynamic-object mask); 0 = none. */
 int mf_track_camera(mf_context* ctx, uint32_t moving_labels);
+/* The second trackLiveFrame of a frame with moving objects (kfusion.cpp:
+ * 347-373): from the current (tracked) camera pose, against the reference pose
+ * and model maps of this frame's mf_track_camera, with the pixels of the
+ * `moving_labels` objects excluded from ICP.  MF_E_STATE without an
+ * mf_track_camera since the last mf_set_ref_from_current. */
+int mf_retrack_camera(mf_context* ctx, uint32_t moving_labels);
 /* Tracking::trackEachObject (tracking.cpp:580-708) for each id (>= 1) against
  * its own model map; T_w_c1 is the camera pose before the last camera update
  * (mf_track_camera or mf_set_camera_pose), T_w_c2 the current one.  The volume
@@ -178,6 +184,53 @@ int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose
  * photometric reference depth of every pixel.  Voxel colours do not enter E.
  * The camera GN problem's state is overwritten.  Synchronises. */
 int mf_camera_cost(mf_context* ctx, const float T_live[16], double* out, float* d_grad_tsdf);
+
+/* --- motion segmentation ------------------------------------------------
+ * Tracking::compute_residuals (tracking/tracking.cpp:1535-1747) with the
+ * moving-object test of kfusion.cpp:287-338 (check_static_state,
+ * rendering/rendering.cpp:907-947).  Call after mf_track_camera: T_w_l is the
+ * current camera pose, T_w_r the pose the model maps of the last mf_raycast
+ * were rendered at.  Raycasts every instance at T_w_l (objects at their
+ * current poses) into a second set of maps (the model maps stay), then
+ * computes per pixel of level 0 an ICP row (live vertex against the model
+ * maps) and a photometric row (the rendered live depth, seen from T_w_r,
+ * warped into the reference intensity) with result codes 1 (inlier), -1 no
+ * data, -2 outside the image, -3 no model point, -4 over the distance or
+ * residual threshold, -5 normal / occlusion test.
+ * inlier_ratio[i] (optional, one per instance): for objects i >= 1 with
+ * pixels in the live render, the share of those pixels whose rows are all
+ * > -3; -1 for the background and for objects out of view.
+ * moving_labels (optional): bit `label` set for each object with
+ * 0.05 < ratio < moved_threshold (the reference's defaults: residual
+ * threshold 1.5, kernels.h:95; moved threshold 0.9, config --obj-moved).
+ * The bits can be passed to mf_track_camera.  Synchronises. */
+int mf_motion_residuals(mf_context* ctx, float residual_threshold, float moved_threshold,
+                        float* inlier_ratio, uint32_t* moving_labels);
+/* Host copies of the last mf_motion_residuals (each pointer optional):
+ * results int8[2][H][W] (ICP rows, then photometric rows), errors
+ * float[2][H][W] (valid where the result is 1, else 0), the live render's
+ * vertex float[H][W][3] and label int32[H][W].  Synchronises. */
+int mf_motion_download(mf_context* ctx, int8_t* results, float* errors, float* live_vertex,
+                       int32_t* live_label);
+/* The result codes (device int8[2][H][W], ICP then photometric) of instance
+ * id's tracking rows at level 0 from its last GN iteration: the camera
+ * (id 0, mf_track_camera) or object id (mf_track_objects) -- what the
+ * reference copies into Object::trackresult_ (kfusion.cpp:282-283, 397-405)
+ * for Object::refine_mask_use_motion.  pose_eval (optional, host float[16]):
+ * the pose those rows were evaluated at (the camera's T_w_l, or the object's
+ * T_c2_o2 = inverse(T_w_c2) T_w_o2); given, the call synchronises, else it
+ * is asynchronous on the context stream. */
+int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* pose_eval);
+/* Object::refine_mask_use_motion (object/object.cpp:255-315, outliers not
+ * absorbed into the background) on instance id's generalized mask of the
+ * current frame: where the mask is >= 0, an ICP row of -4 or -6 or a
+ * photometric row below -3 in d_results (device int8[2][H][W]) sets it to -1
+ * (not integrated).  d_results NULL = the planes of the last
+ * mf_motion_residuals.  Asynchronous on the context stream. */
+int mf_refine_mask_use_motion(mf_context* ctx, int id, const int8_t* d_results);
+/* Host copy (float[H][W]) of instance id's generalized mask of the current
+ * frame, as uploaded and refined.  Synchronises. */
+int mf_download_mask(mf_context* ctx, int id, float* out);
 /* The pool's TSDF values: a device pointer to pool capacity x 512 floats
  * (voxel v of pool slot s at s * 512 + v). */
 int mf_pool_tsdf(mf_context* ctx, float** d_tsdf, long long* n);

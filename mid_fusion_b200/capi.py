@@ -35,6 +35,8 @@ EXPORTS = [
     "mf_track_info", "mf_track_eval", "mf_download_pyramid", "mf_process_frame",
     "mf_process_frame_device", "mf_get_poses", "mf_frame_stats", "mf_set_graphs",
     "mf_profile", "mf_track_eval_static", "mf_camera_cost", "mf_pool_tsdf", "mf_pool_slots",
+    "mf_motion_residuals", "mf_motion_download", "mf_track_results",
+    "mf_refine_mask_use_motion", "mf_download_mask", "mf_retrack_camera",
 ]
 
 
@@ -221,6 +223,10 @@ class Context:
             bits |= 1 << int(l)
         self._check(self.lib.mf_track_camera(self.h, C.c_uint32(bits)))
 
+    def retrack_camera(self, moving_bits):
+        """mf_retrack_camera with label bits (as motion_residuals returns)."""
+        self._check(self.lib.mf_retrack_camera(self.h, C.c_uint32(int(moving_bits))))
+
     def track_objects(self, ids):
         ids = np.ascontiguousarray(ids, np.int32)
         self._check(self.lib.mf_track_objects(self.h, _ptr(ids, np.int32), len(ids)))
@@ -264,6 +270,46 @@ class Context:
         n = C.c_longlong()
         self._check(self.lib.mf_pool_tsdf(self.h, C.byref(p), C.byref(n)))
         return p.value, n.value
+
+    def motion_residuals(self, threshold=1.5, moved=0.9):
+        """Per-instance inlier ratios and the moving-label bits
+        (mf_motion_residuals)."""
+        ratio = np.zeros(max(self.n_instances, 1), np.float32)
+        bits = C.c_uint32()
+        self._check(self.lib.mf_motion_residuals(self.h, C.c_float(threshold), C.c_float(moved),
+                                                 _ptr(ratio, np.float32), C.byref(bits)))
+        return ratio[:self.n_instances], bits.value
+
+    def motion_download(self):
+        """(results int8 (2, H, W), errors (2, H, W), live vertex (H, W, 3),
+        live label (H, W)) of the last motion_residuals."""
+        res = np.zeros((2, self.H, self.W), np.int8)
+        err = np.zeros((2, self.H, self.W), np.float32)
+        vert = np.zeros((self.H, self.W, 3), np.float32)
+        lab = np.zeros((self.H, self.W), np.int32)
+        self._check(self.lib.mf_motion_download(self.h, _ptr(res, np.int8), _ptr(err, np.float32),
+                                                _ptr(vert, np.float32), _ptr(lab, np.int32)))
+        return res, err, vert, lab
+
+    def track_results(self, i, d_ptr):
+        """Result codes of instance i's last level-0 GN rows into device
+        memory at d_ptr (2 * H * W int8); returns the pose they were
+        evaluated at."""
+        pose = np.zeros(16, np.float32)
+        self._check(self.lib.mf_track_results(self.h, int(i), C.c_void_p(d_ptr),
+                                              _ptr(pose, np.float32)))
+        return pose.reshape(4, 4)
+
+    def refine_mask_use_motion(self, i, d_ptr=None):
+        """Refine instance i's mask with result planes at d_ptr (device), or
+        with the last motion_residuals planes."""
+        self._check(self.lib.mf_refine_mask_use_motion(self.h, int(i),
+                                                       C.c_void_p(d_ptr) if d_ptr else None))
+
+    def mask(self, i):
+        out = np.zeros((self.H, self.W), np.float32)
+        self._check(self.lib.mf_download_mask(self.h, int(i), _ptr(out, np.float32)))
+        return out
 
     def track_eval_static(self, slot, level, pose=None):
         """mf_track_eval with static device scratch (allocates nothing)."""

@@ -523,6 +523,12 @@ int mf_track_camera(mf_context* ctx, uint32_t moving_labels) {
   return track_camera(ctx, moving_labels);
 }
 
+int mf_retrack_camera(mf_context* ctx, uint32_t moving_labels) {
+  if (check(ctx)) return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  return track_camera(ctx, moving_labels, 1);
+}
+
 int mf_track_objects(mf_context* ctx, const int* ids, int n) {
   if (check(ctx) || n < 0 || n > 31 || (n > 0 && !ids)) return MF_E_ARG;
   IdList l;
@@ -587,6 +593,41 @@ int mf_pool_tsdf(mf_context* ctx, float** d_tsdf, long long* n) {
 int mf_download_pyramid(mf_context* ctx, int level, int which, float* out) {
   if (check(ctx) || !out || level < 0 || level >= ctx->cfg.pyramid_levels) return MF_E_ARG;
   return track_download_level(ctx, level, which, out);
+}
+
+int mf_motion_residuals(mf_context* ctx, float residual_threshold, float moved_threshold,
+                        float* inlier_ratio, uint32_t* moving_labels) {
+  if (check(ctx) || !(residual_threshold > 0)) return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  return motion_residuals(ctx, residual_threshold, moved_threshold, inlier_ratio, moving_labels);
+}
+
+int mf_motion_download(mf_context* ctx, int8_t* results, float* errors, float* live_vertex,
+                       int32_t* live_label) {
+  if (check(ctx)) return MF_E_ARG;
+  return motion_download(ctx, results, errors, live_vertex, live_label);
+}
+
+int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* pose_eval) {
+  if (check(ctx) || !d_results || id < 0) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return track_results(ctx, id, d_results, pose_eval);
+}
+
+int mf_refine_mask_use_motion(mf_context* ctx, int id, const int8_t* d_results) {
+  if (check(ctx) || id < 0) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return refine_mask_use_motion(ctx, id, d_results, ctx->cfg.use_icp, ctx->cfg.use_rgb);
+}
+
+int mf_download_mask(mf_context* ctx, int id, float* out) {
+  if (check(ctx) || !out || id < 0) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  MF_CUDA(cudaMemcpyAsync(out, ctx->d_masks + id * WH, 4 * WH, cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
 }
 
 }  // extern "C"

@@ -111,6 +111,9 @@ int stage_prepare(Context* ctx, const IdList& ids);
 int stage_alloc(Context* ctx, const IdList& ids);
 int stage_integrate(Context* ctx, const IdList& ids);
 int stage_raycast(Context* ctx, const IdList& ids, float epsilon);
+// The same raycast into other map buffers.
+int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex, F3* normal,
+                     int* label);
 int alloc_keys(Context* ctx, int id, const uint64_t* keys, int n);
 int export_blocks(Context* ctx, int id, uint64_t* keys, int32_t* coords, uint8_t* active,
                   void* voxels, int cap, int* n);
@@ -122,12 +125,17 @@ int track_init(Context* ctx);
 void track_free(Context* ctx);
 int track_preprocess(Context* ctx);
 int track_set_ref(Context* ctx);
-int track_camera(Context* ctx, uint32_t moving);
+int track_camera(Context* ctx, uint32_t moving, int retrack = 0);
 int track_objects(Context* ctx, const IdList& ids);
 int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8, float* d_grad);
+int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
+                     uint32_t* moving);
+int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t* llabel);
+int track_results(Context* ctx, int slot, int8_t* d_out, float* pose_eval);
+int refine_mask_use_motion(Context* ctx, int id, const int8_t* d_res, int use_icp, int use_rgb);
 int stage_raycast_adjoint(Context* ctx, const IdList& ids, const double* gV, const double* gN,
                           float* d_grad);
 int track_download_level(Context* ctx, int L, int which, float* out);

@@ -250,10 +250,14 @@ int profile_raycast(Context* ctx, int reps, double* us) {
 }
 
 int stage_raycast(Context* ctx, const IdList& ids, float epsilon) {
+  return stage_raycast_to(ctx, ids, epsilon, ctx->d_vertex, ctx->d_normal, ctx->d_label);
+}
+
+int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex, F3* normal,
+                     int* label) {
   if (ids.n == 0) return MF_OK;
   const mf_config& c = ctx->cfg;
-  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H,
-            c.near_plane, c.far_plane, c.mu, epsilon};
+  RayArgs a{vertex, normal, label, ctx->W, ctx->H, c.near_plane, c.far_plane, c.mu, epsilon};
   dim3 grid((ctx->W + 15) / 16, (ctx->H + 7) / 8);
   raycast_objects_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
                                                         ids, a, ctx->d_status);

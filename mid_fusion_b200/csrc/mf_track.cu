@@ -47,6 +47,7 @@ struct GNState {
   // full-resolution model label map; empty when x1 < x0
   int box[4];
   M4 Tf, invTf;      // float pose (and inverse) seen by the per-pixel kernels
+  M4 evalTf;         // the pose of the last GN evaluation (Tf when gn_step ran)
   M4 T_w_r, inv_T_w_r, view;               // camera: reference pose, K * inverse(T_w_r)
   M4 T_c1_o1, inv_T_c1_o1, inv_T_w_o1, T_w_c2;  // object constants
   double sums[MAX_PYR][32];
@@ -69,6 +70,7 @@ struct TrackState {
   PyrPtrs pyr{};
   int cur = 0;                      // live set; 1 - cur holds the reference frame
   bool have_ref = false;
+  bool tracked = false;             // the reference pose of this frame is saved
   float* rD[MAX_INSTANCES][MAX_PYR] = {};
   F3* rV[MAX_INSTANCES][MAX_PYR] = {};
   GNState* d_state = nullptr;       // MAX_INSTANCES (slot 0: camera, slot i: object i)
@@ -84,6 +86,13 @@ struct TrackState {
   double* d_cost_part = nullptr;    // per-CTA partials of the cost rows, 8 each
   double* d_cost = nullptr;         // 8: cost, dE/d twist (6), rows
   int cost_blocks = 0;
+  // motion residuals (allocated on first use)
+  int8_t* d_mres = nullptr;         // 2 x W x H result codes: ICP rows, then photometric
+  float* d_merr = nullptr;          // 2 x W x H errors
+  F3* d_lvert = nullptr;            // model raycast at the live pose: vertex, normal, label
+  F3* d_lnorm = nullptr;
+  int* d_llabel = nullptr;
+  int* d_mcount = nullptr;          // 2 x MAX_INSTANCES: object pixels, inliers
 };
 
 // ------------------------------------------------------------------ preprocessing
@@ -249,22 +258,26 @@ __global__ void depth2vertex_slots_kernel(SlotPtrs sp, int w, int h, M4 invK) {
 }
 
 // ------------------------------------------------------------------ GN setup
+// retrack: the second trackLiveFrame of a frame (kfusion.cpp:370-373), from
+// the tracked pose against the same reference pose, which stays saved.
 __global__ void setup_camera_kernel(GNState* st, const float* __restrict__ Twc,
-                                    float* __restrict__ Twc_prev, F4 k) {
+                                    float* __restrict__ Twc_prev, F4 k, int retrack) {
   GNState& S = st[0];
   const M4 T = load_m4(Twc);
-  store_m4(Twc_prev, T);
+  const M4 Tr = retrack ? load_m4(Twc_prev) : T;
+  if (!retrack) store_m4(Twc_prev, T);
   for (int i = 0; i < 16; ++i) {
     S.T[i] = (double)Twc[i];
     S.prevT[i] = S.T[i];
   }
   S.kind = 0; S.label = 0; S.inst = 0; S.done = 0; S.ticket = 0; S.fallback = 0;
   for (int l = 0; l < MAX_PYR; ++l) S.iters[l] = 0;
-  S.T_w_r = T;
-  S.inv_T_w_r = inverse(T);
+  S.T_w_r = Tr;
+  S.inv_T_w_r = inverse(Tr);
   S.view = mul(camera_matrix(k), S.inv_T_w_r);  // tracking.cpp:258
   S.Tf = T;
   S.invTf = inverse(T);
+  S.evalTf = T;
 }
 
 // trackEachObject setup, tracking.cpp:586-593: T_c1_o1 = inverse(T_w_c1) T_wo1,
@@ -293,6 +306,7 @@ __global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __r
   }
   S.Tf = T0;
   S.invTf = inverse(T0);
+  S.evalTf = T0;
 }
 
 __global__ void level_start_kernel(GNState* st, IdList slots) {
@@ -324,6 +338,7 @@ MF_HD void gn_step(GNState& S, const double* s, int level) {
   double T[16], P[16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) { T[i] = S.T[i]; P[i] = S.prevT[i]; }
+  S.evalTf = S.Tf;   // the rows just summed were evaluated here
   const double prev_err = S.prev_err;
   const double err = s[0] / s[28];
   int done = 0, fallback = 0;
@@ -904,6 +919,7 @@ int track_set_ref(Context* ctx) {
   if (int rc = track_init(ctx)) return rc;
   ctx->track->cur = 1 - ctx->track->cur;
   ctx->track->have_ref = true;
+  ctx->track->tracked = false;
   return MF_OK;
 }
 
@@ -1074,12 +1090,17 @@ static int gn_host(Context* ctx, int slot) {
 // Tracking::trackLiveFrame with the current model maps; the camera pose is read
 // from and written back to the device.  `moving` (bit per label) selects the
 // pixels excluded from ICP (trackLiveFrame(..., mask)); 0 = no mask.
-int track_camera(Context* ctx, uint32_t moving) {
+int track_camera(Context* ctx, uint32_t moving, int retrack) {
   if (int rc = track_init(ctx)) return rc;
   TrackState& T = *ctx->track;
   const mf_config& c = ctx->cfg;
+  if (retrack && !T.tracked) {
+    ctx->last_error = "mf_retrack_camera: no mf_track_camera on this frame";
+    return MF_E_STATE;
+  }
+  T.tracked = true;
   setup_camera_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc, T.d_Twc_prev,
-                                                F4{c.k[0], c.k[1], c.k[2], c.k[3]});
+                                                F4{c.k[0], c.k[1], c.k[2], c.k[3]}, retrack);
   MF_CUDA(cudaGetLastError());
   if (moving) {
     label_mask_kernel<<<div_up((long long)ctx->W * ctx->H, 256), 256, 0, ctx->stream>>>(
@@ -1635,6 +1656,300 @@ int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8
   MF_CUDA(cudaMemcpyAsync(out8, T.d_cost, sizeof(double) * 8, cudaMemcpyDeviceToHost,
                           ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+
+// ------------------------------------------------------------------------
+// Motion residuals (Tracking::compute_residuals, tracking.cpp:1535-1553,
+// compute_residual_kernel :1555-1612, compute_icp_residual_kernel :1615-1677,
+// compute_rgb_residual_kernel :1680-1747) and the moving-object test
+// (check_static_state, rendering/rendering.cpp:907-947, and the inlier ratio
+// of kfusion.cpp:312-341).  T_w_l is the freshly tracked camera pose, T_w_r
+// the reference pose of the model maps; the photometric reference vertices
+// come from the model raycast at T_w_l with the objects at their last poses,
+// turned into depth relative to T_w_r (vertex2depth with T_w_r, as the
+// reference passes it, preprocessing.cpp:292-309) and back into vertices.
+struct MotionArgs {
+  PyrPtrs pyr;
+  int cur, W, H;
+  const F3* mvertex; const F3* mnormal;   // model maps at T_w_r
+  const F3* lvert;                          // model vertices raycast at T_w_l
+  const int* llabel;
+  M4 T_w_l, T_w_r, inv_T_w_r, K, invK;
+  float sigma_bright, threshold;
+  int use_icp, use_rgb;
+  int8_t* res; float* err;
+  int* count;                               // [label]: object pixels, [32 + label]: inliers
+};
+
+__global__ void motion_residual_kernel(MotionArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.W * a.H;
+  if (p >= n) return;
+  const int x = p % a.W, y = p / a.W;
+  int8_t ri = 0, rr = 0;
+  float ei = 0.f, er = 0.f;
+  // the outlier-mask test of :1586-1590 never fires: the reference's
+  // outlier_mask_ stays the all-zero mask of set_params_frame (:170), since
+  // the mask variant of trackLiveFrame keeps its pyramid local (:1781-1787)
+  {
+    if (a.use_icp) {
+      const F3 ln = a.pyr.N[0][p];
+      if (ln.x == INVALIDF) {
+        ri = -1;
+      } else {
+        const F3 w_vertex = xform(a.T_w_l, a.pyr.V[a.cur][0][p]);
+        const F3 r_vertex = xform(a.inv_T_w_r, w_vertex);
+        const F3 proj = rotate(a.K, r_vertex);
+        const float px = proj.x / proj.z, py = proj.y / proj.z;
+        if (px < 1 || px > (float)(unsigned)(a.W - 2) || py < 1 || py > (float)(unsigned)(a.H - 2) ||
+            isnan(px) || isnan(py)) {
+          ri = -2;
+        } else {
+          const int q = (int)((unsigned)px + (unsigned)py * a.W);
+          const F3 rn = a.mnormal[q];
+          const F3 rv = a.mvertex[q];
+          if (rn.x == INVALIDF) {
+            ri = -3;
+          } else {
+            const F3 diff = rv - w_vertex;
+            const F3 wn = rotate(a.T_w_l, ln);
+            if (length(diff) > 0.1f) ri = -4;
+            else if (dot(wn, rn) < 0.8f) ri = -5;
+            else {
+              const F3 P = a.pyr.COV[0][p];
+              const double sig = rn.x * rn.x * P.x + rn.y * rn.y * P.y + rn.z * rn.z * P.z;
+              const double e = sqrt(1.0 / sig) * dot(rn, diff);
+              if (fabs(e) > a.threshold) ri = -4;
+              else { ri = 1; ei = (float)e; }
+            }
+          }
+        }
+      }
+    }
+    if (a.use_rgb) {
+      // rendered live vertex -> depth relative to T_w_r -> vertex
+      const F3 vl = a.lvert[p];
+      const float d = vl.z > 0.0 ? xform(a.inv_T_w_r, vl).z : 0.f;
+      const F3 ref = d > 0 ? d * rotate(a.invK, mk3((float)x, (float)y, 1.f)) : mk3(0.f);
+      const F3 live = a.pyr.V[a.cur][0][p];
+      if (ref.z <= 0.f || ref.z == INVALIDF) {
+        rr = -1;
+      } else if (length(ref - live) > 0.1f && live.z > 0.f) {
+        rr = -5;
+      } else {
+        const F3 w_vertex = xform(a.T_w_l, ref);
+        const F3 r_vertex = xform(a.inv_T_w_r, w_vertex);
+        const F3 proj = rotate(a.K, r_vertex);
+        const float px = proj.x / proj.z, py = proj.y / proj.z;
+        if (px < 1 || px > (float)(unsigned)(a.W - 2) || py < 1 || py > (float)(unsigned)(a.H - 2) ||
+            isnan(px) || isnan(py)) {
+          rr = -2;
+        } else {
+          const float residual = a.pyr.I[a.cur][0][p] - bil(a.pyr.I[1 - a.cur][0], a.W, px, py);
+          const double e = (1.0 / a.sigma_bright) * residual;
+          if (fabs(e) > a.threshold) rr = -4;
+          else { rr = 1; er = (float)e; }
+        }
+      }
+    }
+  }
+  a.res[p] = ri; a.res[n + p] = rr;
+  a.err[p] = ei; a.err[n + p] = er;
+  // check_static_state: an object pixel of the live render is an inlier when
+  // its rows' results are > -3
+  const int l = a.llabel[p];
+  if (l >= 1 && l < 32) {
+    bool inl;
+    if (a.use_icp && a.use_rgb) inl = ri > -3 && rr > -3;
+    else if (a.use_icp) inl = ri > -3;
+    else inl = a.use_rgb && rr > -3;
+    atomicAdd(a.count + l, 1);
+    if (inl) atomicAdd(a.count + 32 + l, 1);
+  }
+}
+
+// Object::refine_mask_use_motion (object/object.cpp:255-315, outliers not
+// absorbed into the background): inside the band, pixels whose ICP row is -4
+// or -6, or whose photometric row is below -3, leave the object's mask.
+__global__ void refine_mask_kernel(float* __restrict__ mask, const int8_t* __restrict__ res,
+                                   int n, int use_icp, int use_rgb) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n || !(mask[p] >= 0)) return;
+  if (use_icp && (res[p] == -4 || res[p] == -6)) { mask[p] = -1; return; }
+  if (use_rgb && res[n + p] < -3) mask[p] = -1;
+}
+
+int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
+                     uint32_t* moving) {
+  if (!ctx->track || !ctx->track->have_ref) {
+    ctx->last_error = "mf_motion_residuals: needs a reference frame and a tracked live frame";
+    return MF_E_STATE;
+  }
+  TrackState& T = *ctx->track;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  if (!T.d_mres) {
+    MF_CUDA(cudaMalloc(&T.d_mres, 2 * WH));
+    T.allocs.push_back(T.d_mres);
+    MF_CUDA(cudaMalloc(&T.d_merr, sizeof(float) * 2 * WH));
+    T.allocs.push_back(T.d_merr);
+    MF_CUDA(cudaMalloc(&T.d_lvert, sizeof(F3) * WH));
+    T.allocs.push_back(T.d_lvert);
+    MF_CUDA(cudaMalloc(&T.d_lnorm, sizeof(F3) * WH));
+    T.allocs.push_back(T.d_lnorm);
+    MF_CUDA(cudaMalloc(&T.d_llabel, sizeof(int) * WH));
+    T.allocs.push_back(T.d_llabel);
+    MF_CUDA(cudaMalloc(&T.d_mcount, sizeof(int) * 64));
+    T.allocs.push_back(T.d_mcount);
+    // like the reference's persistent render buffers, the maps start zeroed
+    // and keep what a later raycast does not overwrite
+    MF_CUDA(cudaMemsetAsync(T.d_lvert, 0, sizeof(F3) * WH, ctx->stream));
+    MF_CUDA(cudaMemsetAsync(T.d_lnorm, 0, sizeof(F3) * WH, ctx->stream));
+    MF_CUDA(cudaMemsetAsync(T.d_llabel, 0, sizeof(int) * WH, ctx->stream));
+  }
+  // the model raycast at the live pose, objects at their last poses
+  // (kfusion.cpp:291-296)
+  IdList all;
+  all.n = (int)ctx->inst.size();
+  for (int i = 0; i < all.n; ++i) all.v[i] = i;
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  if (int rc = stage_raycast_to(ctx, all, ctx->ray_epsilon, T.d_lvert, T.d_lnorm, T.d_llabel))
+    return rc;
+  float Tl[16], Tr[16];
+  MF_CUDA(cudaMemcpyAsync(Tl, ctx->d_Twc, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(Tr, T.d_Twc_prev, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaMemsetAsync(T.d_mcount, 0, sizeof(int) * 64, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  const mf_config& c = ctx->cfg;
+  const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
+  MotionArgs a;
+  a.pyr = T.pyr;
+  a.cur = T.cur;
+  a.W = ctx->W;
+  a.H = ctx->H;
+  a.mvertex = ctx->d_vertex;
+  a.mnormal = ctx->d_normal;
+  a.lvert = T.d_lvert;
+  a.llabel = T.d_llabel;
+  a.T_w_l = load_m4(Tl);
+  a.T_w_r = load_m4(Tr);
+  a.inv_T_w_r = inverse(a.T_w_r);
+  a.K = camera_matrix(k);
+  a.invK = inverse_camera_matrix(k);
+  a.sigma_bright = (float)(sqrtf(100.0f) / 255.0);  // tracking.cpp:766-772
+  a.threshold = threshold;
+  a.use_icp = c.use_icp;
+  a.use_rgb = c.use_rgb;
+  a.res = T.d_mres;
+  a.err = T.d_merr;
+  a.count = T.d_mcount;
+  motion_residual_kernel<<<div_up((long long)WH, 256), 256, 0, ctx->stream>>>(a);
+  MF_CUDA(cudaGetLastError());
+  int cnt[64];
+  MF_CUDA(cudaMemcpyAsync(cnt, T.d_mcount, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  // kfusion.cpp:312-338: an object in view (with pixels in the live render)
+  // moves when move-out threshold 0.05 < inliers / pixels < `moved`
+  uint32_t mv = 0;
+  for (int i = 0; i < (int)ctx->inst.size(); ++i) {
+    const int l = ctx->inst[i].label;
+    float r = -1.f;
+    if (i >= 1 && l >= 1 && l < 32 && cnt[l] > 0) {
+      r = static_cast<float>(cnt[32 + l]) / (cnt[l]);
+      if (r < moved && r > 0.05f) mv |= 1u << l;
+    }
+    if (ratio) ratio[i] = r;
+  }
+  if (moving) *moving = mv;
+  return MF_OK;
+}
+
+int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t* llabel) {
+  TrackState* T = ctx->track;
+  if (!T || !T->d_mres) {
+    ctx->last_error = "mf_motion_download: no motion residuals yet";
+    return MF_E_STATE;
+  }
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  if (res) MF_CUDA(cudaMemcpyAsync(res, T->d_mres, 2 * WH, cudaMemcpyDeviceToHost, ctx->stream));
+  if (err)
+    MF_CUDA(cudaMemcpyAsync(err, T->d_merr, sizeof(float) * 2 * WH, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  if (lvert)
+    MF_CUDA(cudaMemcpyAsync(lvert, T->d_lvert, sizeof(F3) * WH, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  if (llabel)
+    MF_CUDA(cudaMemcpyAsync(llabel, T->d_llabel, sizeof(int) * WH, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+// The result codes of problem `slot`'s rows at level 0, evaluated at the pose
+// of its last level-0 GN iteration: Tracking::trackingResult_[0] after
+// trackLiveFrame / trackEachObject, which kfusion.cpp:282-283 and :397-405
+// copy into Object::trackresult_.  ICP rows first, then photometric rows; a
+// term that is switched off leaves 0.
+__global__ void row_codes_kernel(GNArgs a, int slot, int8_t* __restrict__ out) {
+  __shared__ GNState S;
+  if (threadIdx.x == 0) {
+    S = a.st[slot];
+    S.Tf = S.evalTf;
+    S.invTf = inverse(S.evalTf);
+  }
+  __syncthreads();
+  const int w = a.pyr.w[0], h = a.pyr.h[0], n = w * h;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  Row r;
+  int8_t ci = 0, cr = 0;
+  if (a.use_icp) {
+    r.result = 0;
+    if (S.kind == 0) icp_camera(a, S, 0, p, r);
+    else icp_object(a, S, 0, p, r);
+    ci = (int8_t)r.result;
+  }
+  if (a.use_rgb) {
+    r.result = 0;
+    rgb_row(a, S, a.rV[slot], 0, p, w, h, r);
+    cr = (int8_t)r.result;
+  }
+  out[p] = ci;
+  out[n + p] = cr;
+}
+
+int track_results(Context* ctx, int slot, int8_t* d_out, float* pose_eval) {
+  if (!ctx->track || !ctx->track->have_ref) {
+    ctx->last_error = "mf_track_results: no tracking has run";
+    return MF_E_STATE;
+  }
+  const int n = ctx->W * ctx->H;
+  GNArgs a = make_args(ctx, 0, 0);
+  row_codes_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(a, slot, d_out);
+  MF_CUDA(cudaGetLastError());
+  if (pose_eval) {
+    static_assert(sizeof(M4) == 64, "M4 is 16 row-major floats");
+    MF_CUDA(cudaMemcpyAsync(pose_eval, &ctx->track->d_state[slot].evalTf, sizeof(M4),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  return MF_OK;
+}
+
+int refine_mask_use_motion(Context* ctx, int id, const int8_t* d_res, int use_icp, int use_rgb) {
+  TrackState* T = ctx->track;
+  if (!d_res) {
+    if (!T || !T->d_mres) {
+      ctx->last_error = "mf_refine_mask_use_motion: no motion residuals yet";
+      return MF_E_STATE;
+    }
+    d_res = T->d_mres;
+  }
+  const int n = ctx->W * ctx->H;
+  refine_mask_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(ctx->d_masks + (size_t)id * n,
+                                                              d_res, n, use_icp, use_rgb);
+  MF_CUDA(cudaGetLastError());
   return MF_OK;
 }
 

@@ -381,6 +381,18 @@ static bool solve_pose(const std::vector<double>& s, M4<T>& update) {
   return nx < (double)1e-05f && (double)std::sqrt(ratio) < 2e-3;
 }
 
+// trackingResult_[0] after the last level-0 evaluation: the codes of the
+// ICP rows, then of the photometric rows (0 for a term that is off)
+static void keep_codes(std::vector<int8_t>& out, const std::vector<Row>& icp,
+                       const std::vector<Row>& rgb, bool use_icp, bool use_rgb) {
+  const size_t n = icp.size();
+  out.assign(2 * n, 0);
+  for (size_t i = 0; i < n; ++i) {
+    out[i] = use_icp ? (int8_t)icp[i].result : 0;
+    out[n + i] = use_rgb ? (int8_t)rgb[i].result : 0;
+  }
+}
+
 template <typename T>
 void Tracker<T>::camera_sums(int level, const M4<T>& T_w_l, const M4<T>& T_w_r,
                              const std::vector<V3<T>>& MV, const std::vector<V3<T>>& MN,
@@ -454,6 +466,7 @@ void Tracker<T>::camera_sums(int level, const M4<T>& T_w_l, const M4<T>& T_w_r,
       g.error = inv_cov_rgb * residual;
       g.result = 1;
     }
+  if (level == 0) keep_codes(last_result, icp, rgb, p.use_icp, p.use_rgb);
   reduce<T>(s, icp, rgb, w, h, p.robust, p.use_icp, p.use_rgb);
 }
 
@@ -578,6 +591,7 @@ void Tracker<T>::object_sums(int level, const M4<T>& T_c2_o2, const M4<T>& T_c1_
       g.error = inv_cov_rgb * residual;
       g.result = 1;
     }
+  if (level == 0) keep_codes(last_result, icp, rgb, p.use_icp, p.use_rgb);
   reduce<T>(s, icp, rgb, w, h, p.robust, p.use_icp, p.use_rgb);
 }
 
@@ -608,6 +622,108 @@ M4<T> Tracker<T>::track_object(const M4<T>& T_wo1, const M4<T>& T_w_c2, const M4
     }
   }
   return mul(T_w_c2, T_c2_o2);
+}
+
+template <typename T>
+void Tracker<T>::motion_residuals(const M4<T>& T_w_l, const M4<T>& T_w_r,
+                                  const float* model_vertex, const float* model_normal,
+                                  const float* live_render_vertex, float threshold,
+                                  int8_t* result, float* error) const {
+  const int W = p.W, H = p.H, n = W * H;
+  const M4<T> K = camera_matrix<T>(p.k[0], p.k[1], p.k[2], p.k[3]);
+  const M4<T> invK = inverse_camera_matrix<T>(p.k[0], p.k[1], p.k[2], p.k[3]);
+  const M4<T> inv_r = inverse(T_w_r);
+  auto at = [](const float* a, int q) { return v3<T>(a[3 * q], a[3 * q + 1], a[3 * q + 2]); };
+  // warp (tracking.cpp:1114-1121) with T_w_l for the world transform and
+  // inverse(T_w_r) for the reference frame; false for pixels outside
+  // [1, W-2] x [1, H-2] (and, where the reference's conversion of a NaN
+  // coordinate to a pixel index is undefined, for NaN)
+  auto warp = [&](V3<T> v, V3<T>& w, T& px, T& py) {
+    w = xform(T_w_l, v);
+    const V3<T> pr = rotate(K, xform(inv_r, w));
+    px = pr.x / pr.z; py = pr.y / pr.z;
+    return !(px < 1 || px > (T)(unsigned)(W - 2) || py < 1 || py > (T)(unsigned)(H - 2) ||
+             std::isnan(px) || std::isnan(py));
+  };
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      const int i = x + y * W;
+      int8_t ri = 0, rr = 0;
+      float ei = 0.f, er = 0.f;
+      // no row is -6: the reference's outlier_mask_ stays the all-zero mask of
+      // set_params_frame (tracking.cpp:170); the mask variant of
+      // trackLiveFrame keeps its mask pyramid local (:1781-1787)
+      {
+        if (p.use_icp) {  // compute_icp_residual_kernel, tracking.cpp:1615-1677
+          V3<T> w;
+          T px, py;
+          if (l_normal[0][i].x == INVALID) ri = -1;
+          else if (!warp(l_vertex[0][i], w, px, py)) ri = -2;
+          else {
+            const int q = (int)((unsigned)px + (unsigned)py * W);
+            const V3<T> rn = at(model_normal, q), rv = at(model_vertex, q);
+            if (rn.x == INVALID) ri = -3;
+            else {
+              const V3<T> diff = rv - w;
+              const V3<T> wn = rotate(T_w_l, l_normal[0][i]);
+              if (length(diff) > T(0.1f)) ri = -4;
+              else if (dot(wn, rn) < T(0.8f)) ri = -5;
+              else {
+                const V3<T> P = cov[0][i];
+                const double sig = rn.x * rn.x * P.x + rn.y * rn.y * P.y + rn.z * rn.z * P.z;
+                const double e = std::sqrt(1.0 / sig) * dot(rn, diff);
+                if (std::fabs(e) > threshold) ri = -4;
+                else { ri = 1; ei = (float)e; }
+              }
+            }
+          }
+        }
+        if (p.use_rgb) {  // compute_rgb_residual_kernel, tracking.cpp:1680-1747
+          // vertex2depth with T_w_r (preprocessing.cpp:292-309), depth2vertexKernel
+          const V3<T> vl = at(live_render_vertex, i);
+          const T d = vl.z > 0.0 ? xform(inv_r, vl).z : T(0);
+          const V3<T> ref = d > 0 ? d * rotate(invK, v3<T>((T)x, (T)y, T(1))) : v3<T>(0, 0, 0);
+          const V3<T> live = l_vertex[0][i];
+          V3<T> w;
+          T px, py;
+          if (ref.z <= 0 || ref.z == INVALID) rr = -1;
+          else if (length(ref - live) > T(0.1f) && live.z > 0) rr = -5;
+          else if (!warp(ref, w, px, py)) rr = -2;
+          else {
+            const T residual = l_I[0][i] - bil(r_I[0].data(), W, px, py);
+            const double e = (1.0 / (double)sigma_bright) * residual;
+            if (std::fabs(e) > threshold) rr = -4;
+            else { rr = 1; er = (float)e; }
+          }
+        }
+      }
+      result[i] = ri; result[n + i] = rr;
+      error[i] = ei; error[n + i] = er;
+    }
+}
+
+float inlier_ratio(const int8_t* result, const int* labels, int label, int n, bool use_icp,
+                   bool use_rgb) {
+  int all = 0, inl = 0;
+  for (int i = 0; i < n; ++i) {
+    if (labels[i] != label) continue;
+    ++all;
+    bool ok = false;
+    if (use_icp && use_rgb) ok = result[i] > -3 && result[n + i] > -3;
+    else if (use_icp) ok = result[i] > -3;
+    else if (use_rgb) ok = result[n + i] > -3;
+    inl += ok;
+  }
+  return all ? static_cast<float>(inl) / all : -1.f;
+}
+
+void refine_mask_use_motion(float* mask, const int8_t* result, int n, bool use_icp,
+                            bool use_rgb) {
+  for (int i = 0; i < n; ++i) {
+    if (!(mask[i] >= 0)) continue;
+    if (use_icp && (result[i] == -4 || result[i] == -6)) { mask[i] = -1; continue; }
+    if (use_rgb && result[n + i] < -3) mask[i] = -1;
+  }
 }
 
 template struct Tracker<float>;

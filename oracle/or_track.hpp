@@ -115,6 +115,7 @@ struct Tracker {
   // last reduction per level (for tests), 32 values
   std::vector<std::vector<double>> last_sums;
   int last_iterations[4];
+  std::vector<int8_t> last_result;  // level-0 row codes of the last evaluation
 
   void init(const TrackParams& prm);
   void set_frame(const uint8_t* rgb, const float* depth);   // rgb2intensity + set_params_frame
@@ -136,6 +137,23 @@ struct Tracker {
   // trackEachObject: returns the new volume pose T_w_o2
   M4<T> track_object(const M4<T>& T_w_o1, const M4<T>& T_w_c2, const M4<T>& T_w_c1,
                      const float* vertex, const float* normal, const int* labels, int label);
+  // Tracking::compute_residuals at level 0 (tracking.cpp:1535-1747): result
+  // codes and errors of the ICP rows (first W*H) and photometric rows (next
+  // W*H).  model_*: the model maps raycast at T_w_r; live_render_vertex: the
+  // model vertices raycast at T_w_l.  Rows that are not computed keep result
+  // 0 and error 0.
+  void motion_residuals(const M4<T>& T_w_l, const M4<T>& T_w_r, const float* model_vertex,
+                        const float* model_normal, const float* live_render_vertex,
+                        float threshold, int8_t* result, float* error) const;
 };
+
+// check_static_state (rendering.cpp:907-947) and the inlier ratio of
+// kfusion.cpp:312-320 for the pixels of `labels` equal to `label`: -1 when
+// the label holds no pixel (the reference computes no ratio then).
+float inlier_ratio(const int8_t* result, const int* labels, int label, int n, bool use_icp,
+                   bool use_rgb);
+// Object::refine_mask_use_motion (object.cpp:255-315), outliers not absorbed.
+void refine_mask_use_motion(float* mask, const int8_t* result, int n, bool use_icp,
+                            bool use_rgb);
 
 }  // namespace ort

@@ -155,4 +155,62 @@ int ot_get_level(void* hh, int level, int which, float* out) {
   return h->fp64 ? get(h->d) : get(h->f);
 }
 
+// Tracking::compute_residuals at level 0 with the single-precision tracker
+// (the reference's arithmetic); -1 for an all-FP64 tracker.
+int ot_motion_residuals(void* hh, const float* T_w_l, const float* T_w_r, const float* vertex,
+                        const float* normal, const float* live_render_vertex, float threshold,
+                        signed char* result, float* error) {
+  Handle* h = (Handle*)hh;
+  if (h->fp64) return -1;
+  h->f.motion_residuals(ld<float>(T_w_l), ld<float>(T_w_r), vertex, normal, live_render_vertex,
+                        threshold, (int8_t*)result, error);
+  return 0;
+}
+float ot_inlier_ratio(const signed char* result, const int* labels, int label, int n, int use_icp,
+                      int use_rgb) {
+  return inlier_ratio((const int8_t*)result, labels, label, n, use_icp != 0, use_rgb != 0);
+}
+void ot_refine_mask_use_motion(float* mask, const signed char* result, int n, int use_icp,
+                               int use_rgb) {
+  refine_mask_use_motion(mask, (const int8_t*)result, n, use_icp != 0, use_rgb != 0);
+}
+
+// The level-0 row result codes of the last camera or object evaluation
+// (2 * W * H int8); returns the count written (0 before any evaluation).
+int ot_last_results(void* hh, signed char* out) {
+  Handle* h = (Handle*)hh;
+  const std::vector<int8_t>& r = h->fp64 ? h->d.last_result : h->f.last_result;
+  std::memcpy(out, r.data(), r.size());
+  return (int)r.size();
+}
+
+// Overwrites one plane of a pyramid level (test input injection): `which` as
+// in ot_get_level for the live frame, 8 = reference intensity, 9 = reference
+// (live) vertex.
+int ot_set_level(void* hh, int level, int which, const float* in) {
+  Handle* h = (Handle*)hh;
+  auto set = [&](auto& t, auto zero) {
+    using T = decltype(zero);
+    const size_t n = (size_t)t.lw[level] * t.lh[level];
+    auto plane = [&](std::vector<T>& d) { for (size_t i = 0; i < n; ++i) d[i] = (T)in[i]; };
+    auto vec = [&](std::vector<V3<T>>& d) {
+      for (size_t i = 0; i < n; ++i) d[i] = v3<T>(in[3 * i], in[3 * i + 1], in[3 * i + 2]);
+    };
+    switch (which) {
+      case 0: plane(t.l_D[level]); break;
+      case 1: plane(t.l_I[level]); break;
+      case 2: vec(t.l_vertex[level]); break;
+      case 3: vec(t.l_normal[level]); break;
+      case 4: plane(t.gx[level]); break;
+      case 5: plane(t.gy[level]); break;
+      case 6: vec(t.cov[level]); break;
+      case 8: plane(t.r_I[level]); break;
+      case 9: vec(t.r_vertex_live[level]); break;
+      default: return -1;
+    }
+    return (int)n;
+  };
+  return h->fp64 ? set(h->d, 0.0) : set(h->f, 0.0f);
+}
+
 }  // extern "C"

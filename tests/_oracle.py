@@ -226,6 +226,28 @@ def camera_cost(vols, poses, labels, T_w_r, T_live, k, W, H, live, use_icp=True,
 _cache = {}
 
 
+def inlier_ratio(results, labels, label, use_icp=True, use_rgb=True):
+    """check_static_state + the inlier ratio of kfusion.cpp:312-320 (-1 when
+    the label has no pixel)."""
+    lib = oracle().lib
+    lib.ot_inlier_ratio.restype = C.c_float
+    res = np.ascontiguousarray(results, np.int8)
+    lab = np.ascontiguousarray(labels, np.int32)
+    return float(lib.ot_inlier_ratio(res.ctypes.data_as(C.c_void_p),
+                                     lab.ctypes.data_as(C.c_void_p), int(label), lab.size,
+                                     int(use_icp), int(use_rgb)))
+
+
+def refine_mask_use_motion(mask, results, use_icp=True, use_rgb=True):
+    """Object::refine_mask_use_motion on a copy of mask."""
+    lib = oracle().lib
+    out = np.array(mask, np.float32, copy=True, order="C")
+    res = np.ascontiguousarray(results, np.int8)
+    lib.ot_refine_mask_use_motion(out.ctypes.data_as(C.c_void_p), res.ctypes.data_as(C.c_void_p),
+                                  out.size, int(use_icp), int(use_rgb))
+    return out
+
+
 def oracle():
     if "or" not in _cache:
         _cache["or"] = Impl(ORACLE_SO, "or_")
@@ -268,6 +290,13 @@ class Tracker:
         lib.ot_last_iterations.argtypes = [P, C.c_int]
         lib.ot_get_level.restype = C.c_int
         lib.ot_get_level.argtypes = [P, C.c_int, C.c_int, FP]
+        I8 = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+        lib.ot_motion_residuals.restype = C.c_int
+        lib.ot_motion_residuals.argtypes = [P, FP, FP, FP, FP, FP, C.c_float, I8, FP]
+        lib.ot_last_results.restype = C.c_int
+        lib.ot_last_results.argtypes = [P, I8]
+        lib.ot_set_level.restype = C.c_int
+        lib.ot_set_level.argtypes = [P, C.c_int, C.c_int, FP]
         it = np.zeros(4, np.int32)
         it[:len(iters)] = iters
         self.levels = len(iters)
@@ -317,6 +346,29 @@ class Tracker:
                                 _f32(T_w_c1).reshape(16), _f32(vertex), _f32(normal),
                                 np.ascontiguousarray(labels, np.int32), int(label), out)
         return out
+
+    def motion_residuals(self, T_w_l, T_w_r, vertex, normal, live_vertex, threshold=1.5):
+        """Tracking::compute_residuals at level 0: (results int8 (2, H, W),
+        errors (2, H, W)); single-precision tracker only."""
+        res = np.zeros((2, self.H, self.W), np.int8)
+        err = np.zeros((2, self.H, self.W), np.float32)
+        rc = self.lib.ot_motion_residuals(self.h, _f32(T_w_l).reshape(16),
+                                          _f32(T_w_r).reshape(16), _f32(vertex), _f32(normal),
+                                          _f32(live_vertex), threshold, res, err)
+        assert rc == 0, "motion residuals need the single-precision tracker"
+        return res, err
+
+    def set_level(self, level, which, data):
+        """Overwrite a pyramid plane (which as in level(); 8 = reference
+        intensity, 9 = reference vertex)."""
+        assert self.lib.ot_set_level(self.h, level, which, _f32(data).reshape(-1)) > 0
+
+    def last_results(self):
+        """Level-0 row codes (2, H, W) of the last camera / object evaluation."""
+        out = np.zeros(2 * self.W * self.H, np.int8)
+        n = self.lib.ot_last_results(self.h, out)
+        assert n == out.size
+        return out.reshape(2, self.H, self.W)
 
     def iterations(self):
         return [self.lib.ot_last_iterations(self.h, l) for l in range(self.levels)]
