@@ -45,6 +45,7 @@ UNEVEN_STEPS = 8
 
 
 ADJ_PAIRS, ADJ_PAIRS_HD, HD = 64, 16, (1280, 720)
+MOTION_FRAMES = 16
 
 
 def scene_for(rank, n_frames, workload="multi"):
@@ -278,6 +279,11 @@ def run_ours(args, rank, world, local_rank):
                                           torch)
         ctx_h.close()
 
+    # ---- motion segmentation after camera tracking
+    motion = None
+    if do_uneven:
+        motion = run_motion(ctx_b, frames, [p[0] for p in poses_b], MOTION_FRAMES, dev, torch)
+
     # ---- e2e through the C ABI from pinned host buffers
     import ctypes
     ctx_e = make_ctx(True)
@@ -321,7 +327,50 @@ def run_ours(args, rank, world, local_rank):
     return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
                 status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
                 ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
-                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint)
+                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint, motion=motion)
+
+
+def run_motion(ctx, frames, poses, n, dev, torch):
+    """Motion segmentation after camera tracking (mf_motion_residuals: the
+    live raycast of every instance, level-0 ICP + photometric residual codes,
+    per-object inlier ratios, moving bits to the host), then the row codes of
+    every object's last GN evaluation (mf_track_results) and the refinement
+    of every instance's mask; device time per frame with CUDA events (camera
+    and object tracking outside the timed region)."""
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    codes = torch.zeros(2 * W * H, dtype=torch.int8, device=dev)
+    times, moving = [], []
+    for b in range(n):
+        f = 1 + b % (len(frames) - 1)
+        ctx.set_camera_pose(poses[f - 1])
+        ctx.upload(frames[f - 1][0], frames[f - 1][1], None)
+        ctx.preprocess()
+        ctx.raycast()
+        ctx.set_ref_from_current()
+        ctx.upload(frames[f][0], frames[f][1], None)
+        ctx.upload_labels(frames[f][2])
+        ctx.preprocess()
+        ctx.track_camera()
+        ctx.track_objects(list(range(1, ctx.n_instances)))
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, bits = ctx.motion_residuals(1.5, 0.9)
+        ctx.refine_mask_use_motion(0)  # the background: the motion residual rows
+        for i in range(1, ctx.n_instances):  # objects: their own GN rows
+            ctx.track_results(i, codes.data_ptr())
+            ctx.refine_mask_use_motion(i, codes.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        moving.append(bin(bits).count("1"))
+    ms = float(np.mean(times[2:] if len(times) > 4 else times))
+    return {"frames": n, "ms_per_frame": round(ms, 4),
+            "moving_objects_mean": round(float(np.mean(moving)), 2),
+            "what": "mf_motion_residuals (live raycast, residual codes, inlier ratios, moving "
+                    "bits to the host) + mf_track_results of every object + "
+                    "mf_refine_mask_use_motion of every instance",
+            "status_flags": ctx.status()}
 
 
 def run_adjoint(ctx, scene, frames, poses, pairs, dev, torch):
@@ -524,6 +573,7 @@ def main():
         "batched_over_plain": round(total_p / total_b, 3),
         "uneven12": r.get("uneven"),
         "adjoint": r.get("adjoint"),
+        "motion": r.get("motion"),
         "pose_diff_batched_vs_plain_m": r["dpos"],
         "camera_err_vs_gt_m": r["gt_err"],
         "e2e": {"value": round(value_e, 2), "unit": "frames/s",
