@@ -219,8 +219,10 @@ int mf_motion_download(mf_context* ctx, int8_t* results, float* errors, float* l
  * for Object::refine_mask_use_motion.  pose_eval (optional, host float[16]):
  * the pose those rows were evaluated at (the camera's T_w_l, or the object's
  * T_c2_o2 = inverse(T_w_c2) T_w_o2); given, the call synchronises, else it
- * is asynchronous on the context stream. */
-int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* pose_eval);
+ * is asynchronous on the context stream.  d_errors (optional, device
+ * float[2][H][W]): TrackData::error of the rows with result 1, else 0. */
+int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* d_errors,
+                     float* pose_eval);
 /* Object::refine_mask_use_motion (object/object.cpp:255-315, outliers not
  * absorbed into the background) on instance id's generalized mask of the
  * current frame: where the mask is >= 0, an ICP row of -4 or -6 or a
@@ -231,6 +233,50 @@ int mf_refine_mask_use_motion(mf_context* ctx, int id, const int8_t* d_results);
 /* Host copy (float[H][W]) of instance id's generalized mask of the current
  * frame, as uploaded and refined.  Synchronises. */
 int mf_download_mask(mf_context* ctx, int id, float* out);
+
+/* --- headless renders ---------------------------------------------------
+ * The reference's visualisation kernels (rendering/rendering.cpp) into
+ * uchar4 images of W x H (mf_render_normal: uchar3).  `out` may be device
+ * memory (written asynchronously on the context stream) or host memory
+ * (rendered into a context scratch image and copied; the call synchronises).
+ * Float-to-byte conversions keep the low byte of the 32-bit integer value,
+ * as the reference does when built with gcc for x86-64.
+ *
+ * renderVolume_many_Kernel (rendering.cpp:489-646) as Kfusion::renderVolume
+ * calls it (kfusion.cpp:1303-1309: near plane, 2 x far plane).  T_w_c: the
+ * view pose to raycast every instance from, with that kernel's own
+ * composite rules; NULL = shade the maps of the last mf_raycast (the
+ * reference's doraycast == false).  render_color: shade with the
+ * interpolated voxel colour, else with colors[label] (the background white).
+ * largestep: the march step outside the band (the reference's benchmark
+ * passes 0.75 mu).  ambient: float[3] or NULL for (0.1, 0.1, 0.1)
+ * (constant_parameters.h:24).  colors: n_colors RGBA entries indexed by
+ * instance label; labels outside the table render black. */
+int mf_render_volume(mf_context* ctx, const float* T_w_c, int render_color, float largestep,
+                     const float* ambient, const uint8_t* colors, int n_colors, uint8_t* out);
+/* renderDepthKernel (rendering.cpp:366-393) of the current input depth with
+ * the config's near and far planes. */
+int mf_render_depth(mf_context* ctx, uint8_t* out);
+/* renderIntensityKernel (rendering.cpp:648-664) of the current grey input. */
+int mf_render_intensity(mf_context* ctx, uint8_t* out);
+/* renderNormalKernel (rendering.cpp:346-364) of the model normal map (uchar3). */
+int mf_render_normal(mf_context* ctx, uint8_t* out);
+/* Track renders of result rows (device int8[2][H][W], errors float[2][H][W]
+ * from mf_track_results; both NULL = the last mf_motion_residuals): mode 0
+ * renderTrackKernel (rendering.cpp:395-432) of the ICP rows, 1
+ * renderRGBTrackKernel (:434-487) of the photometric rows, 2
+ * render_RGBD_TrackKernel (:183-237) of both. */
+int mf_render_track(mf_context* ctx, int mode, const int8_t* d_results, const float* d_errors,
+                    uint8_t* out);
+/* Label renders of a label image (device int32[H][W]; NULL = the last
+ * mf_raycast's): mode 0 renderInstanceMaskKernel (rendering.cpp:797-820;
+ * pass colours indexed by class for renderClassMaskKernel :822-847), 1
+ * renderMaskWithImageKernel (:679-723) over the current RGB input, 2
+ * renderMaskMotionWithImageKernel (:725-795), which also reads each label's
+ * result rows: d_rows[label] (a host array of n_rows device pointers, each
+ * int8[2][H][W] or NULL), the Object::trackresult_ of that instance. */
+int mf_render_mask(mf_context* ctx, int mode, const int32_t* d_labels, const uint8_t* colors,
+                   int n_colors, const int8_t* const* d_rows, int n_rows, uint8_t* out);
 /* The pool's TSDF values: a device pointer to pool capacity x 512 floats
  * (voxel v of pool slot s at s * 512 + v). */
 int mf_pool_tsdf(mf_context* ctx, float** d_tsdf, long long* n);
@@ -286,7 +332,8 @@ int mf_export_nodes(mf_context* ctx, int id, uint64_t* keys, uint32_t* side,
                     uint8_t* children_mask, void* values, int cap, int* n);
 int mf_root_children(mf_context* ctx, int id, uint8_t* mask);
 /* Volume::interp (continuous/volume_template.hpp:97-104) at n points
- * (metres, volume frame); field 0 = tsdf, 1 = foreground probability. */
+ * (metres, volume frame); field 0 = tsdf, 1 = foreground probability,
+ * 2, 3, 4 = colour r, g, b. */
 int mf_interp(mf_context* ctx, int id, const float* pos, int n, int field, float* out);
 
 #ifdef __cplusplus

@@ -37,6 +37,8 @@ EXPORTS = [
     "mf_profile", "mf_track_eval_static", "mf_camera_cost", "mf_pool_tsdf", "mf_pool_slots",
     "mf_motion_residuals", "mf_motion_download", "mf_track_results",
     "mf_refine_mask_use_motion", "mf_download_mask", "mf_retrack_camera",
+    "mf_render_volume", "mf_render_depth", "mf_render_intensity", "mf_render_normal",
+    "mf_render_track", "mf_render_mask",
 ]
 
 
@@ -291,14 +293,57 @@ class Context:
                                                 _ptr(vert, np.float32), _ptr(lab, np.int32)))
         return res, err, vert, lab
 
-    def track_results(self, i, d_ptr):
+    def track_results(self, i, d_ptr, d_err=None):
         """Result codes of instance i's last level-0 GN rows into device
-        memory at d_ptr (2 * H * W int8); returns the pose they were
-        evaluated at."""
+        memory at d_ptr (2 * H * W int8), errors at d_err (2 * H * W float,
+        optional); returns the pose they were evaluated at."""
         pose = np.zeros(16, np.float32)
         self._check(self.lib.mf_track_results(self.h, int(i), C.c_void_p(d_ptr),
+                                              C.c_void_p(d_err) if d_err else None,
                                               _ptr(pose, np.float32)))
         return pose.reshape(4, 4)
+
+    # ---------------------------------------------------------------- renders
+    def render_volume(self, T_w_c=None, render_color=True, largestep=0.075, ambient=None,
+                      colors=None):
+        """(H, W, 4) uint8 shaded render (mf_render_volume); T_w_c None shades
+        the last raycast's maps."""
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        col = None if colors is None else np.ascontiguousarray(colors, np.uint8).reshape(-1, 4)
+        amb = None if ambient is None else np.ascontiguousarray(ambient, np.float32)
+        self._check(self.lib.mf_render_volume(
+            self.h, None if T_w_c is None else _ptr(_m4(T_w_c), np.float32),
+            int(render_color), C.c_float(largestep), _ptr(amb, np.float32),
+            _ptr(col, np.uint8), 0 if col is None else len(col), _ptr(out, np.uint8)))
+        return out
+
+    def render_image(self, which):
+        """which: "depth", "intensity" (H, W, 4) or "normal" (H, W, 3)."""
+        out = np.zeros((self.H, self.W, 3 if which == "normal" else 4), np.uint8)
+        fn = {"depth": self.lib.mf_render_depth, "intensity": self.lib.mf_render_intensity,
+              "normal": self.lib.mf_render_normal}[which]
+        self._check(fn(self.h, _ptr(out, np.uint8)))
+        return out
+
+    def render_track(self, mode, d_res=None, d_err=None):
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        self._check(self.lib.mf_render_track(self.h, int(mode),
+                                             C.c_void_p(d_res) if d_res else None,
+                                             C.c_void_p(d_err) if d_err else None,
+                                             _ptr(out, np.uint8)))
+        return out
+
+    def render_mask(self, mode, colors, d_labels=None, d_rows=()):
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        col = np.ascontiguousarray(colors, np.uint8).reshape(-1, 4)
+        rows = (C.c_void_p * max(len(d_rows), 1))(*[C.c_void_p(p) if p else None
+                                                    for p in d_rows])
+        self._check(self.lib.mf_render_mask(self.h, int(mode),
+                                            C.c_void_p(d_labels) if d_labels else None,
+                                            _ptr(col, np.uint8), len(col),
+                                            rows if len(d_rows) else None, len(d_rows),
+                                            _ptr(out, np.uint8)))
+        return out
 
     def refine_mask_use_motion(self, i, d_ptr=None):
         """Refine instance i's mask with result planes at d_ptr (device), or

@@ -195,7 +195,8 @@ int mf_destroy(mf_context* ctx) {
                 ctx->d_vols, ctx->d_Two, ctx->d_Twc, ctx->d_frames, ctx->d_status,
                 ctx->d_reserved, ctx->d_inst_label, ctx->d_visit, ctx->d_visit_count,
                 ctx->d_depth, ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, ctx->d_masks,
-                ctx->d_labels, ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->d_export};
+                ctx->d_labels, ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->d_export,
+                ctx->d_render, ctx->d_render_small};
   for (void* p : ps) if (p) cudaFree(p);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -430,7 +431,7 @@ int mf_root_children(mf_context* ctx, int id, uint8_t* mask) {
 }
 
 int mf_interp(mf_context* ctx, int id, const float* pos, int n, int field, float* out) {
-  if (check(ctx) || n < 0 || (n > 0 && (!pos || !out)) || field < 0 || field > 1)
+  if (check(ctx) || n < 0 || (n > 0 && (!pos || !out)) || field < 0 || field > 4)
     return MF_E_ARG;
   if (id < 0 || id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
   return interp_points(ctx, id, pos, n, field, out);
@@ -608,10 +609,11 @@ int mf_motion_download(mf_context* ctx, int8_t* results, float* errors, float* l
   return motion_download(ctx, results, errors, live_vertex, live_label);
 }
 
-int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* pose_eval) {
+int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* d_errors,
+                     float* pose_eval) {
   if (check(ctx) || !d_results || id < 0) return MF_E_ARG;
   if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
-  return track_results(ctx, id, d_results, pose_eval);
+  return track_results(ctx, id, d_results, d_errors, pose_eval);
 }
 
 int mf_refine_mask_use_motion(mf_context* ctx, int id, const int8_t* d_results) {
@@ -628,6 +630,51 @@ int mf_download_mask(mf_context* ctx, int id, float* out) {
                           ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
   return MF_OK;
+}
+
+int mf_render_volume(mf_context* ctx, const float* T_w_c, int render_color, float largestep,
+                     const float* ambient, const uint8_t* colors, int n_colors, uint8_t* out) {
+  if (check(ctx) || !out || !(largestep > 0) || n_colors < 0 || (n_colors > 0 && !colors))
+    return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  return render_volume(ctx, T_w_c, render_color, largestep, ambient, colors, n_colors, out);
+}
+
+int mf_render_depth(mf_context* ctx, uint8_t* out) {
+  if (check(ctx) || !out) return MF_E_ARG;
+  return render_image(ctx, 0, out);
+}
+
+int mf_render_intensity(mf_context* ctx, uint8_t* out) {
+  if (check(ctx) || !out) return MF_E_ARG;
+  return render_image(ctx, 1, out);
+}
+
+int mf_render_normal(mf_context* ctx, uint8_t* out) {
+  if (check(ctx) || !out) return MF_E_ARG;
+  return render_image(ctx, 2, out);
+}
+
+int mf_render_track(mf_context* ctx, int mode, const int8_t* d_results, const float* d_errors,
+                    uint8_t* out) {
+  if (check(ctx) || !out || mode < 0 || mode > 2) return MF_E_ARG;
+  if (!d_results) {
+    const int8_t* r = nullptr;
+    const float* e = nullptr;
+    if (int rc = motion_planes(ctx, &r, &e)) return rc;
+    d_results = r;
+    d_errors = e;
+  }
+  if (mode != 0 && !d_errors) return MF_E_ARG;
+  return render_track(ctx, mode, d_results, d_errors, out);
+}
+
+int mf_render_mask(mf_context* ctx, int mode, const int32_t* d_labels, const uint8_t* colors,
+                   int n_colors, const int8_t* const* d_rows, int n_rows, uint8_t* out) {
+  if (check(ctx) || !out || mode < 0 || mode > 2 || n_colors < 0 || (n_colors > 0 && !colors) ||
+      n_rows < 0 || (n_rows > 0 && !d_rows))
+    return MF_E_ARG;
+  return render_mask(ctx, mode, d_labels, colors, n_colors, d_rows, n_rows, out);
 }
 
 }  // extern "C"

@@ -22,6 +22,17 @@ MF_HD float fmx(float a, float b) { return a > b ? a : b; }
 MF_HD int imn(int a, int b) { return a < b ? a : b; }
 MF_HD int imx(int a, int b) { return a > b ? a : b; }
 MF_HD float clampf(float f, float a, float b) { return fmx(a, fmn(f, b)); }  // cutil_math.h:981
+// The reference converts float (or double) colour values to unsigned char
+// implicitly (make_uchar4(float, ...)).  Out of range that is undefined
+// behaviour; built with gcc for x86-64 the value goes through a 32-bit integer
+// and the low byte is kept.  to_u8 does the same, so renders agree with the
+// reference as built there (a direct float-to-u8 conversion on the device
+// would saturate instead).
+MF_HD unsigned char to_u8(float v) { return (unsigned char)(int)v; }
+MF_HD unsigned char to_u8d(double v) { return (unsigned char)(int)v; }
+MF_HD uchar4 u4(float x, float y, float z, float w) {
+  return make_uchar4(to_u8(x), to_u8(y), to_u8(z), to_u8(w));
+}
 MF_HD float sq(float r) { return r * r; }
 
 struct F3 { float x, y, z; };

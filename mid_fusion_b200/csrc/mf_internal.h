@@ -95,6 +95,9 @@ struct Context {
   void* graphs = nullptr;           // captured frame graphs (mf_pipeline.cu)
   bool use_graphs = true;
   TrackState* track = nullptr;
+  uint8_t* d_render = nullptr;      // W*H*4 render scratch for host destinations
+  void* d_render_small = nullptr;   // colour / pointer tables of a render
+  size_t render_small_bytes = 0;
 };
 
 #define MF_CUDA(call)                                                          \
@@ -134,7 +137,18 @@ int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8
 int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
                      uint32_t* moving);
 int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t* llabel);
-int track_results(Context* ctx, int slot, int8_t* d_out, float* pose_eval);
+int track_results(Context* ctx, int slot, int8_t* d_out, float* d_err, float* pose_eval);
+int motion_planes(Context* ctx, const int8_t** res, const float** err);
+// headless renders (mf_render.cu; the shaded volume render in mf_raycast.cu)
+int render_target(Context* ctx, void* out, size_t bytes, void** target);
+int render_finish(Context* ctx, void* out, void* target, size_t bytes);
+int render_stage_small(Context* ctx, const void* src, size_t bytes, void** dst);
+int render_volume(Context* ctx, const float* T_w_c, int render_color, float largestep,
+                  const float* ambient, const uint8_t* colors, int n_colors, uint8_t* out);
+int render_image(Context* ctx, int which, uint8_t* out);
+int render_track(Context* ctx, int mode, const int8_t* d_res, const float* d_err, uint8_t* out);
+int render_mask(Context* ctx, int mode, const int32_t* d_labels, const uint8_t* colors,
+                int n_colors, const int8_t* const* d_rows, int n_rows, uint8_t* out);
 int refine_mask_use_motion(Context* ctx, int id, const int8_t* d_res, int use_icp, int use_rgb);
 int stage_raycast_adjoint(Context* ctx, const IdList& ids, const double* gV, const double* gN,
                           float* d_grad);

@@ -1,3 +1,4 @@
+#include <cstring>
 // Multi-instance octree raycasting on the device.
 //
 // raycastObjectList (apps/kfusion/src/cpp/rendering/rendering.cpp:9-181): per
@@ -550,6 +551,174 @@ int stage_raycast_adjoint(Context* ctx, const IdList& ids, const double* gV, con
                                                         ids, a, gV, gN, d_grad, ctx->d_status);
   MF_CUDA(cudaGetLastError());
   return MF_OK;
+}
+
+// ------------------------------------------------------------------------
+// The shaded volume render (headless).
+struct RenderArgs {
+  Pool pool;
+  const Volume* vols;
+  const InstFrame* frames;   // T_w_o, inverse(T_w_o), label of every instance
+  IdList ids;                // instances in list order
+  int W, H;
+  M4 view;                   // T_w_c * inverse(K) of the render pose
+  F3 w_origin;               // get_translation(T_w_c)
+  float nearPlane, farPlane, mu, largestep, epsilon;
+  F3 ambient;
+  int render_color, do_raycast;
+  const uchar4* colors;      // label colours
+  int n_colors;
+  const F3* vertex; const F3* normal; const int* label;  // maps for do_raycast == 0
+  uchar4* out;
+  int* status;
+};
+
+// renderVolume_many_Kernel, rendering.cpp:489-646.  With do_raycast the
+// composite hit is found again with this function's own rules (the tie and
+// the zero-gradient cases differ from raycastObjectList); otherwise the maps
+// of the last raycast are shaded.
+__global__ void __launch_bounds__(128) render_volume_kernel(RenderArgs a) {
+  const int x = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
+  if (x >= a.W || y >= a.H) return;
+  const int p = x + y * a.W;
+  __shared__ int s_slot[8 * 128];
+  F3 w_hit = mk3(0.f), w_norm = mk3(0.f);
+  int w_label = 0;
+  if (a.do_raycast) {
+    float nearest = 1.0e10f;
+    double high_fg = 0.f;
+    int miss = 0;
+    const F3 w_dir = rotate(a.view, mk3((float)x, (float)y, 1.f));
+    for (int o = 0; o < a.ids.n; ++o) {
+      const int i = a.ids.v[o];
+      const Volume& V = a.vols[i];
+      const InstFrame& F = a.frames[i];
+      const float step = V.dim / V.size;
+      const F3 o_origin = xform(F.inv_T_w_o, a.w_origin);
+      const F3 o_dir = normalize(rotate(F.inv_T_w_o, w_dir));
+      const float nfar = fmn(nearest, a.farPlane);
+      const float t_min = ray_first_block(V, o_origin, o_dir, a.nearPlane, nfar, a.epsilon,
+                                          a.status);
+      const F4 hit = t_min > 0.f
+                         ? raycast_volume(a.pool, V, o_origin, o_dir,
+                                          t_min * V.dim / (unsigned)V.size, nfar, a.mu, step,
+                                          a.largestep)
+                         : F4{0, 0, 0, 0};
+      const float hd = F.label == 0 ? hit.w + 0.05f : hit.w;
+      if (hd > nearest) { miss++; continue; }
+      const double fg = volume_interp(a.pool, V, mk3(hit.x, hit.y, hit.z), 1);
+      if (fg <= 0.5f) { miss++; continue; }
+      if (hd == nearest) {
+        if (fg > high_fg) high_fg = fg;
+        else { miss++; continue; }
+      }
+      if (hit.w > 0) {
+        nearest = hd;
+        const F3 o_hit = mk3(hit.x, hit.y, hit.z);
+        const F3 g = volume_grad(a.pool, V, o_hit, s_slot + threadIdx.x, 128);
+        if (length(g) > 0) {
+          w_norm = rotate(F.T_w_o, g);
+          w_hit = xform(F.T_w_o, o_hit);
+          w_label = F.label;
+        }
+      } else {
+        miss++;
+      }
+    }
+    if (miss == a.ids.n) {
+      a.out[p] = make_uchar4(0, 0, 0, 0);
+      return;
+    }
+  } else {
+    w_hit = a.vertex[p];
+    w_norm = a.normal[p];
+    w_label = a.label[p];
+  }
+  F3 col = mk3(0.f);
+  for (int o = 0; o < a.ids.n; ++o) {
+    const int i = a.ids.v[o];
+    const InstFrame& F = a.frames[i];
+    if (w_label != F.label) continue;
+    const F3 o_hit = xform(F.inv_T_w_o, w_hit);
+    const F3 diff = normalize(a.w_origin - w_hit);
+    const float dir = fmx(dot(normalize(w_norm), diff), 0.f);
+    F3 rgb;
+    if (a.render_color) {
+      const Volume& V = a.vols[i];
+      rgb = mk3(volume_interp(a.pool, V, o_hit, 2), volume_interp(a.pool, V, o_hit, 3),
+                volume_interp(a.pool, V, o_hit, 4));
+    } else if (w_label == 0) {
+      rgb = mk3(1.f);
+    } else {
+      const uchar4 c = (w_label >= 0 && w_label < a.n_colors) ? a.colors[w_label]
+                                                               : make_uchar4(0, 0, 0, 0);
+      rgb = mk3((float)c.x, (float)c.y, (float)c.z);
+      rgb = mk3(rgb.x / 255, rgb.y / 255, rgb.z / 255);
+    }
+    // clamp(make_float3(dir) * rgb + ambient, 0, 1) * 255; the background's
+    // label colour path has no product (make_float3(dir) + ambient)
+    const F3 lit = (a.render_color || w_label != 0)
+                       ? mk3(dir * rgb.x, dir * rgb.y, dir * rgb.z)
+                       : mk3(dir);
+    col = mk3(fmx(0.f, fmn(lit.x + a.ambient.x, 1.f)), fmx(0.f, fmn(lit.y + a.ambient.y, 1.f)),
+              fmx(0.f, fmn(lit.z + a.ambient.z, 1.f)));
+    col = col * 255.f;
+  }
+  a.out[p] = u4(col.x, col.y, col.z, 0.f);
+}
+
+int render_volume(Context* ctx, const float* T_w_c, int render_color, float largestep,
+                  const float* ambient, const uint8_t* colors, int n_colors, uint8_t* out) {
+  const mf_config& c = ctx->cfg;
+  const size_t bytes = (size_t)ctx->W * ctx->H * 4;
+  void* target = nullptr;
+  if (int rc = render_target(ctx, out, bytes, &target)) return rc;
+  IdList all;
+  all.n = (int)ctx->inst.size();
+  for (int i = 0; i < all.n; ++i) all.v[i] = i;
+  // the instances' T_w_o and inverse; the camera frame of the current pose
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  float Tc[16];
+  if (T_w_c) {
+    std::memcpy(Tc, T_w_c, sizeof(Tc));
+  } else {
+    MF_CUDA(cudaMemcpyAsync(Tc, ctx->d_Twc, 64, cudaMemcpyDeviceToHost, ctx->stream));
+    MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  }
+  void* d_colors = nullptr;
+  if (n_colors > 0) {
+    if (int rc = render_stage_small(ctx, colors, 4 * (size_t)n_colors, &d_colors)) return rc;
+  }
+  const M4 T = load_m4(Tc);
+  RenderArgs a;
+  a.pool = ctx->pool;
+  a.vols = ctx->d_vols;
+  a.frames = ctx->d_frames;
+  a.ids = all;
+  a.W = ctx->W;
+  a.H = ctx->H;
+  a.view = mul(T, inverse_camera_matrix(F4{c.k[0], c.k[1], c.k[2], c.k[3]}));
+  a.w_origin = get_translation(T);
+  // Kfusion::renderVolume passes farPlane * 2 (kfusion.cpp:1303-1304)
+  a.nearPlane = c.near_plane;
+  a.farPlane = c.far_plane * 2.0f;
+  a.mu = c.mu;
+  a.largestep = largestep;
+  a.epsilon = ctx->ray_epsilon;
+  a.ambient = ambient ? mk3(ambient[0], ambient[1], ambient[2]) : mk3(0.1f);
+  a.render_color = render_color;
+  a.do_raycast = T_w_c != nullptr;
+  a.colors = (const uchar4*)d_colors;
+  a.n_colors = n_colors;
+  a.vertex = ctx->d_vertex;
+  a.normal = ctx->d_normal;
+  a.label = ctx->d_label;
+  a.out = (uchar4*)target;
+  a.status = ctx->d_status;
+  dim3 grid((ctx->W + 15) / 16, (ctx->H + 7) / 8);
+  render_volume_kernel<<<grid, 128, 0, ctx->stream>>>(a);
+  return render_finish(ctx, out, target, bytes);
 }
 
 }  // namespace mf

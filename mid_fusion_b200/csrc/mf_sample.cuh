@@ -30,11 +30,19 @@ __device__ __forceinline__ int memo_slot(const Volume& V, BlockMemo& m, int x, i
 // every tap reads the block voxel when the block exists and the init / empty
 // value (tsdf 1, fg 0) otherwise.  When the 2x2x2 cell lies inside one block
 // (gather_points' "all local" case) a single block lookup serves all taps.
+// FIELD: 0 tsdf, 1 foreground probability, 2-4 colour r, g, b; an
+// unallocated voxel reads its initial value (tsdf 1, the rest 0).
 template <int FIELD>
 __device__ __forceinline__ float tap_val(const Pool& P, int slot, int v) {
   if (slot < 0) return FIELD == 0 ? 1.f : 0.f;
   const size_t o = (size_t)slot * 512 + v;
-  return FIELD == 0 ? __ldg(P.tsdf + o) : (float)__ldg(P.fg + o);
+  switch (FIELD) {
+    case 0: return __ldg(P.tsdf + o);
+    case 1: return (float)__ldg(P.fg + o);
+    case 2: return __ldg(P.r + o);
+    case 3: return __ldg(P.g + o);
+    default: return __ldg(P.b + o);
+  }
 }
 
 template <int FIELD>
@@ -70,7 +78,13 @@ __device__ __noinline__ float volume_interp_m(const Pool& P, const Volume& V, F3
 __device__ __forceinline__ float volume_interp(const Pool& P, const Volume& V, F3 pos_m,
                                                int field) {
   BlockMemo m;
-  return field == 0 ? volume_interp_m<0>(P, V, pos_m, m) : volume_interp_m<1>(P, V, pos_m, m);
+  switch (field) {
+    case 0: return volume_interp_m<0>(P, V, pos_m, m);
+    case 1: return volume_interp_m<1>(P, V, pos_m, m);
+    case 2: return volume_interp_m<2>(P, V, pos_m, m);
+    case 3: return volume_interp_m<3>(P, V, pos_m, m);
+    default: return volume_interp_m<4>(P, V, pos_m, m);
+  }
 }
 
 __device__ __forceinline__ float tsdf_at(const Pool& P, const Volume& V, int x, int y, int z) {

@@ -1891,7 +1891,8 @@ int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t
 // trackLiveFrame / trackEachObject, which kfusion.cpp:282-283 and :397-405
 // copy into Object::trackresult_.  ICP rows first, then photometric rows; a
 // term that is switched off leaves 0.
-__global__ void row_codes_kernel(GNArgs a, int slot, int8_t* __restrict__ out) {
+__global__ void row_codes_kernel(GNArgs a, int slot, int8_t* __restrict__ out,
+                                 float* __restrict__ out_err) {
   __shared__ GNState S;
   if (threadIdx.x == 0) {
     S = a.st[slot];
@@ -1904,29 +1905,36 @@ __global__ void row_codes_kernel(GNArgs a, int slot, int8_t* __restrict__ out) {
   if (p >= n) return;
   Row r;
   int8_t ci = 0, cr = 0;
+  float ei = 0.f, er = 0.f;  // TrackData::error of rows with result 1
   if (a.use_icp) {
     r.result = 0;
     if (S.kind == 0) icp_camera(a, S, 0, p, r);
     else icp_object(a, S, 0, p, r);
     ci = (int8_t)r.result;
+    if (ci == 1) ei = r.e;
   }
   if (a.use_rgb) {
     r.result = 0;
     rgb_row(a, S, a.rV[slot], 0, p, w, h, r);
     cr = (int8_t)r.result;
+    if (cr == 1) er = r.e;
   }
   out[p] = ci;
   out[n + p] = cr;
+  if (out_err) {
+    out_err[p] = ei;
+    out_err[n + p] = er;
+  }
 }
 
-int track_results(Context* ctx, int slot, int8_t* d_out, float* pose_eval) {
+int track_results(Context* ctx, int slot, int8_t* d_out, float* d_err, float* pose_eval) {
   if (!ctx->track || !ctx->track->have_ref) {
     ctx->last_error = "mf_track_results: no tracking has run";
     return MF_E_STATE;
   }
   const int n = ctx->W * ctx->H;
   GNArgs a = make_args(ctx, 0, 0);
-  row_codes_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(a, slot, d_out);
+  row_codes_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(a, slot, d_out, d_err);
   MF_CUDA(cudaGetLastError());
   if (pose_eval) {
     static_assert(sizeof(M4) == 64, "M4 is 16 row-major floats");
@@ -1953,5 +1961,16 @@ int refine_mask_use_motion(Context* ctx, int id, const int8_t* d_res, int use_ic
   return MF_OK;
 }
 
+
+// The planes of the last mf_motion_residuals (for renders), or MF_E_STATE.
+int motion_planes(Context* ctx, const int8_t** res, const float** err) {
+  if (!ctx->track || !ctx->track->d_mres) {
+    ctx->last_error = "no motion residuals yet";
+    return MF_E_STATE;
+  }
+  *res = ctx->track->d_mres;
+  *err = ctx->track->d_merr;
+  return MF_OK;
+}
 
 }  // namespace mf

@@ -297,7 +297,13 @@ float get_fine_tsdf(const Volume& v, int x, int y, int z) {
 static float sample_field(const Volume& v, int x, int y, int z, int field) {
   const Voxel* p = v.voxel(x, y, z);
   if (!p) return field == 0 ? 1.f : 0.f;
-  return field == 0 ? p->x : (float)p->fg;
+  switch (field) {
+    case 0: return p->x;
+    case 1: return (float)p->fg;
+    case 2: return p->r;
+    case 3: return p->g;
+    default: return p->b;
+  }
 }
 float interp(const Volume& v, F3 pos_m, int field) {
   const float inv = v.size / v.dim;  // volume_template.hpp:97-104

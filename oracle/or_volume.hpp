@@ -107,7 +107,7 @@ unsigned integrate_volume_kernel(Volume& vol, const float* depth, const F3* rgb,
                                  const M4& T_w_o, F4 k, float mu);
 
 float get_fine_tsdf(const Volume& v, int x, int y, int z);
-float interp(const Volume& v, F3 pos_m, int field);   // field 0: tsdf, 1: fg
+float interp(const Volume& v, F3 pos_m, int field);   // 0 tsdf, 1 fg, 2-4 r, g, b
 F3 grad_tsdf(const Volume& v, F3 pos_m);
 float ray_first_block(const Volume& v, F3 origin, F3 dir, float nearp, float farp,
                       float epsilon);

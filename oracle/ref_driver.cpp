@@ -120,8 +120,14 @@ void ref_export_nodes(void* h, refkey_t* keys, unsigned* side, unsigned char* cm
 
 float ref_interp(void* h, const float* p, int field) {
   const float3 pos = make_float3(p[0], p[1], p[2]);
-  if (field == 0) return ((RefVol*)h)->vol.interp(pos, [](const auto& v) { return v.x; });
-  return ((RefVol*)h)->vol.interp(pos, [](const auto& v) { return v.fg; });
+  auto& vol = ((RefVol*)h)->vol;
+  switch (field) {
+    case 0: return vol.interp(pos, [](const auto& v) { return v.x; });
+    case 1: return vol.interp(pos, [](const auto& v) { return v.fg; });
+    case 2: return vol.interp(pos, [](const auto& v) { return v.r; });
+    case 3: return vol.interp(pos, [](const auto& v) { return v.g; });
+    default: return vol.interp(pos, [](const auto& v) { return v.b; });
+  }
 }
 void ref_grad(void* h, const float* p, float* out) {
   const float3 g = ((RefVol*)h)->vol.grad(make_float3(p[0], p[1], p[2]),

@@ -248,6 +248,83 @@ def refine_mask_use_motion(mask, results, use_icp=True, use_rgb=True):
     return out
 
 
+class Render:
+    """The oracle's restatement of the reference's render kernels
+    (oracle/or_render.cpp); images as numpy uint8 arrays."""
+
+    def __init__(self, W, H):
+        self.lib = oracle().lib
+        self.W, self.H = W, H
+
+    def _out(self, c=4):
+        return np.zeros((self.H, self.W, c), np.uint8)
+
+    def volume(self, vols, poses, labels, T_w_c, k, near, far, mu, largestep, epsilon,
+               render_color, colors, maps=None, T_shade=None, ambient=(0.1, 0.1, 0.1)):
+        """renderVolume_many_Kernel; T_w_c None shades `maps` = (vertex,
+        normal, label) from T_shade."""
+        n = len(vols)
+        arr = (P * n)(*[v.h for v in vols])
+        out = self._out()
+        col = np.ascontiguousarray(colors, np.uint8).reshape(-1, 4)
+        if maps is None:
+            v = nr = np.zeros((self.H, self.W, 3), np.float32)
+            lab = np.zeros((self.H, self.W), np.int32)
+        else:
+            v, nr, lab = (_f32(maps[0]), _f32(maps[1]), np.ascontiguousarray(maps[2], np.int32))
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)
+        self.lib.or_render_volume(
+            arr, vp(_f32(np.stack(poses).reshape(n, 16))),
+            vp(np.ascontiguousarray(labels, np.int32)), n,
+            None if T_w_c is None else vp(_f32(T_w_c).reshape(16)), vp(_f32(k)), self.W, self.H,
+            C.c_float(near), C.c_float(far), C.c_float(mu), C.c_float(largestep),
+            C.c_float(epsilon), vp(_f32(ambient)), int(render_color), vp(col), len(col), vp(v),
+            vp(nr), vp(lab), None if T_shade is None else vp(_f32(T_shade).reshape(16)), vp(out))
+        return out
+
+    def depth(self, depth, near, far):
+        out = self._out()
+        d = _f32(depth)
+        self.lib.or_render_depth(d.ctypes.data_as(C.c_void_p), d.size, C.c_float(near),
+                                 C.c_float(far), out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def intensity(self, grey):
+        out = self._out()
+        g = _f32(grey)
+        self.lib.or_render_intensity(g.ctypes.data_as(C.c_void_p), g.size,
+                                     out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def normal(self, normal):
+        out = self._out(3)
+        nr = _f32(normal)
+        self.lib.or_render_normal(nr.ctypes.data_as(C.c_void_p), nr.size // 3,
+                                  out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def track(self, res, err, mode):
+        out = self._out()
+        r = np.ascontiguousarray(res, np.int8)
+        e = _f32(err)
+        self.lib.or_render_track(r.ctypes.data_as(C.c_void_p), e.ctypes.data_as(C.c_void_p),
+                                 self.W * self.H, int(mode), out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def mask(self, label, rgb3, mode, colors, rows=()):
+        out = self._out()
+        lab = np.ascontiguousarray(label, np.int32)
+        rgb = _f32(rgb3)
+        col = np.ascontiguousarray(colors, np.uint8).reshape(-1, 4)
+        keep = [None if r is None else np.ascontiguousarray(r, np.int8) for r in rows]
+        ptrs = (C.c_void_p * max(len(keep), 1))(
+            *[None if r is None else r.ctypes.data_as(C.c_void_p).value for r in keep])
+        self.lib.or_render_mask(lab.ctypes.data_as(C.c_void_p), rgb.ctypes.data_as(C.c_void_p),
+                                lab.size, int(mode), col.ctypes.data_as(C.c_void_p), len(col),
+                                ptrs, len(keep), out.ctypes.data_as(C.c_void_p))
+        return out
+
+
 def oracle():
     if "or" not in _cache:
         _cache["or"] = Impl(ORACLE_SO, "or_")

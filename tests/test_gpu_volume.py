@@ -130,7 +130,7 @@ def test_interp_matches_oracle():
                   s.volume_poses(0)[0], s.k, 0.1)
     rng = np.random.default_rng(0)
     pts = rng.uniform(0, inst.dim, size=(2000, 3)).astype(np.float32)
-    for field in (0, 1):
+    for field in range(5):  # tsdf, fg, r, g, b
         g = ctx.interp(0, pts, field)
         o = np.array([vol.interp(p, field) for p in pts], np.float32)
         assert np.array_equal(g, o)

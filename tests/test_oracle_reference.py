@@ -93,6 +93,6 @@ def test_interp_and_grad_match_reference():
         v.integrate(d, rgb3, m, s.cam_poses[0], np.eye(4), s.k, 0.1)
     rng = np.random.default_rng(1)
     for p in rng.uniform(0.5, 4.6, size=(400, 3)).astype(np.float32):
-        assert a.interp(p, 0) == b.interp(p, 0)
-        assert a.interp(p, 1) == b.interp(p, 1)
+        for field in range(5):  # tsdf, fg, r, g, b
+            assert a.interp(p, field) == b.interp(p, field), field
         assert np.array_equal(a.grad(p), b.grad(p))
