@@ -234,6 +234,36 @@ int mf_refine_mask_use_motion(mf_context* ctx, int id, const int8_t* d_results);
  * frame, as uploaded and refined.  Synchronises. */
 int mf_download_mask(mf_context* ctx, int id, float* out);
 
+/* --- object spawning and semantics -------------------------------------
+ * Kfusion::spawnNewObjectKernel (kfusion.cpp:1080-1150): the placement of a
+ * new object's volume from the current depth frame and camera pose.  mask:
+ * uint8[H][W] (host or device), nonzero on the new object's pixels.  Every
+ * masked pixel's vertex (zero where the depth is 0) goes to the world frame;
+ * their bounding box and mean (float sums in row-major order, as the
+ * reference accumulates them) give volume_size = min(2.5 max(dx, dy, dz / 2),
+ * 5) and T_w_o = identity with the translation mean - size / 2;
+ * volume_resol = 256 / 512 / 1024 / 2048 for sizes below 0.64 / 1.28 / 2.56 /
+ * 5.12 m (0 where the reference leaves it unset).  n_pixels (optional): the
+ * masked pixel count.  The caller adds the instance (mf_instance_add) and
+ * integrates it, as Kfusion::generate_new_objects does.  Synchronises. */
+int mf_spawn_object(mf_context* ctx, const uint8_t* mask, float T_w_o[16], float* volume_size,
+                    int* volume_resol, int* n_pixels);
+/* Object::Object's semantic state (object.cpp:11-34): class id, the class
+ * probabilities of the segmentation that created it (n_classes, 80 in the
+ * reference) and a fused count of 1. */
+int mf_instance_set_semantics(mf_context* ctx, int id, int class_id, const float* probs,
+                              int n_classes);
+/* Object::fuse_semantic_kernel / fuseSemanticLabel (object.cpp:197-252): for
+ * class_id != 0, the running mean (probs * recog_times + fused * fused_time) /
+ * (fused_time + recog_times) in float; the object's class becomes 1 + the
+ * first index of the largest fused probability.  MF_E_ARG when n_classes
+ * differs from the object's (the reference exits). */
+int mf_fuse_semantics(mf_context* ctx, int id, int class_id, const float* probs, int n_classes,
+                      int recog_times);
+/* The object's class id, fused count and (up to cap) fused probabilities. */
+int mf_instance_semantics(mf_context* ctx, int id, int* class_id, int* fused_time, float* probs,
+                          int cap);
+
 /* --- headless renders ---------------------------------------------------
  * The reference's visualisation kernels (rendering/rendering.cpp) into
  * uchar4 images of W x H (mf_render_normal: uchar3).  `out` may be device

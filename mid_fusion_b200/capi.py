@@ -38,7 +38,8 @@ EXPORTS = [
     "mf_motion_residuals", "mf_motion_download", "mf_track_results",
     "mf_refine_mask_use_motion", "mf_download_mask", "mf_retrack_camera",
     "mf_render_volume", "mf_render_depth", "mf_render_intensity", "mf_render_normal",
-    "mf_render_track", "mf_render_mask",
+    "mf_render_track", "mf_render_mask", "mf_spawn_object", "mf_instance_set_semantics",
+    "mf_fuse_semantics", "mf_instance_semantics",
 ]
 
 
@@ -302,6 +303,34 @@ class Context:
                                               C.c_void_p(d_err) if d_err else None,
                                               _ptr(pose, np.float32)))
         return pose.reshape(4, 4)
+
+    # ---------------------------------------------------------------- objects
+    def spawn_object(self, mask):
+        """(T_w_o, volume_size, volume_resol, n_pixels) of mf_spawn_object."""
+        m = np.ascontiguousarray(mask, np.uint8)
+        T = np.zeros(16, np.float32)
+        size, resol, n = C.c_float(), C.c_int(), C.c_int()
+        self._check(self.lib.mf_spawn_object(self.h, _ptr(m, np.uint8), _ptr(T, np.float32),
+                                             C.byref(size), C.byref(resol), C.byref(n)))
+        return T.reshape(4, 4), size.value, resol.value, n.value
+
+    def set_semantics(self, i, class_id, probs):
+        p = np.ascontiguousarray(probs, np.float32)
+        self._check(self.lib.mf_instance_set_semantics(self.h, int(i), int(class_id),
+                                                       _ptr(p, np.float32), p.size))
+
+    def fuse_semantics(self, i, class_id, probs, recog_times=1):
+        p = np.ascontiguousarray(probs, np.float32)
+        self._check(self.lib.mf_fuse_semantics(self.h, int(i), int(class_id), _ptr(p, np.float32),
+                                               p.size, int(recog_times)))
+
+    def semantics(self, i, n=80):
+        """(class id, fused count, fused probabilities)."""
+        cid, ft = C.c_int(), C.c_int()
+        p = np.zeros(n, np.float32)
+        self._check(self.lib.mf_instance_semantics(self.h, int(i), C.byref(cid), C.byref(ft),
+                                                   _ptr(p, np.float32), n))
+        return cid.value, ft.value, p
 
     # ---------------------------------------------------------------- renders
     def render_volume(self, T_w_c=None, render_color=True, largestep=0.075, ambient=None,

@@ -677,4 +677,40 @@ int mf_render_mask(mf_context* ctx, int mode, const int32_t* d_labels, const uin
   return render_mask(ctx, mode, d_labels, colors, n_colors, d_rows, n_rows, out);
 }
 
+int mf_spawn_object(mf_context* ctx, const uint8_t* mask, float* T_w_o, float* volume_size,
+                    int* volume_resol, int* n_pixels) {
+  if (check(ctx) || !mask || !T_w_o || !volume_size || !volume_resol) return MF_E_ARG;
+  const int n = spawn_object(ctx, mask, T_w_o, volume_size, volume_resol);
+  if (n < 0) return n;
+  if (n_pixels) *n_pixels = n;
+  return MF_OK;
+}
+
+int mf_instance_set_semantics(mf_context* ctx, int id, int class_id, const float* probs,
+                              int n_classes) {
+  if (check(ctx) || id < 0 || n_classes < 0 || (n_classes > 0 && !probs)) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return set_semantics(ctx, id, class_id, probs, n_classes);
+}
+
+int mf_fuse_semantics(mf_context* ctx, int id, int class_id, const float* probs, int n_classes,
+                      int recog_times) {
+  if (check(ctx) || id < 0 || n_classes < 0 || (n_classes > 0 && !probs) || recog_times < 0)
+    return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return fuse_semantics(ctx, id, class_id, probs, n_classes, recog_times);
+}
+
+int mf_instance_semantics(mf_context* ctx, int id, int* class_id, int* fused_time, float* probs,
+                          int cap) {
+  if (check(ctx) || id < 0 || cap < 0) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  const Instance& in = ctx->inst[id];
+  if (class_id) *class_id = in.class_id;
+  if (fused_time) *fused_time = in.fused_time;
+  if (probs)
+    for (int i = 0; i < cap && i < (int)in.sem.size(); ++i) probs[i] = in.sem[i];
+  return MF_OK;
+}
+
 }  // extern "C"

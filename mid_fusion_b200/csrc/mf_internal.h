@@ -46,6 +46,10 @@ struct Instance {
   int label;
   Volume vol;          // device pointers, host copy
   size_t reserved;     // reference allocation-list capacity
+  // semantic class (Object::class_id_, semanticfusion_, fused_time_)
+  int class_id = 0;
+  int fused_time = 0;
+  std::vector<float> sem;
 };
 
 // One GN problem (camera or object) tracked on the device.
@@ -140,6 +144,13 @@ int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t
 int track_results(Context* ctx, int slot, int8_t* d_out, float* d_err, float* pose_eval);
 int motion_planes(Context* ctx, const int8_t** res, const float** err);
 // headless renders (mf_render.cu; the shaded volume render in mf_raycast.cu)
+// object management (mf_objects.cu)
+int ensure_export(Context* ctx, size_t bytes);
+int spawn_object(Context* ctx, const uint8_t* mask, float* T_w_o, float* volume_size,
+                 int* volume_resol);
+int set_semantics(Context* ctx, int id, int class_id, const float* probs, int n);
+int fuse_semantics(Context* ctx, int id, int class_id, const float* probs, int n,
+                   int recog_times);
 int render_target(Context* ctx, void* out, size_t bytes, void** target);
 int render_finish(Context* ctx, void* out, void* target, size_t bytes);
 int render_stage_small(Context* ctx, const void* src, size_t bytes, void** dst);

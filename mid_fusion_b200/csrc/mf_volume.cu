@@ -679,7 +679,7 @@ int alloc_keys(Context* ctx, int id, const uint64_t* keys, int n) {
   return MF_OK;
 }
 
-static int ensure_export(Context* ctx, size_t bytes) {
+int ensure_export(Context* ctx, size_t bytes) {
   if (ctx->export_bytes >= bytes) return MF_OK;
   if (ctx->d_export) cudaFree(ctx->d_export);
   ctx->d_export = nullptr;

@@ -325,6 +325,32 @@ class Render:
         return out
 
 
+def spawn_object(depth, mask, k, T_w_c):
+    """Kfusion::spawnNewObjectKernel: (T_w_o, volume_size, volume_resol, n)."""
+    lib = oracle().lib
+    lib.or_spawn_object.restype = C.c_int
+    d = _f32(depth)
+    m = np.ascontiguousarray(mask, np.uint8)
+    T = np.zeros(16, np.float32)
+    size, resol = C.c_float(), C.c_int()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    n = lib.or_spawn_object(vp(d), vp(m), d.shape[1], d.shape[0], vp(_f32(k)),
+                            vp(_f32(T_w_c).reshape(16)), vp(T), C.byref(size), C.byref(resol))
+    return T.reshape(4, 4), size.value, resol.value, n
+
+
+def fuse_semantics(fused, fused_time, probs, recog_times=1):
+    """Object::fuseSemanticLabel: (new fused vector, new count, class id)."""
+    lib = oracle().lib
+    lib.or_fuse_semantics.restype = C.c_int
+    f = np.array(fused, np.float32, copy=True)
+    ft = C.c_int(fused_time)
+    p = _f32(probs)
+    cid = lib.or_fuse_semantics(f.ctypes.data_as(C.c_void_p), f.size, C.byref(ft),
+                                p.ctypes.data_as(C.c_void_p), int(recog_times))
+    return f, ft.value, cid
+
+
 def oracle():
     if "or" not in _cache:
         _cache["or"] = Impl(ORACLE_SO, "or_")
