@@ -264,6 +264,59 @@ int mf_fuse_semantics(mf_context* ctx, int id, int class_id, const float* probs,
 int mf_instance_semantics(mf_context* ctx, int id, int* class_id, int* fused_time, float* probs,
                           int cap);
 
+/* --- formats ------------------------------------------------------------
+ * Kfusion::preprocessing's input stage (kfusion.cpp:210-217): a sensor frame
+ * of in_width x in_height with uint16 millimetre depth and uchar3 colour (host
+ * or device pointers, each optional), subsampled by the integer ratio
+ * in_width / width (mm2metersKernel, preprocessing.cpp:132-159;
+ * rgb2intensity :73-102) into the frame's metres, float colour and grey.
+ * MF_E_ARG for sizes the reference rejects.  Synchronises. */
+int mf_frame_upload_raw(mf_context* ctx, const uint16_t* depth_mm, const uint8_t* rgb,
+                        int in_width, int in_height);
+/* The SLAMBench .raw reader (RawDepthReader, interface.h:207-335): per frame
+ * uint32 (w, h), uint16 depth[w*h] (mm), uint32 (w, h), uchar3 rgb[w*h].
+ * mf_raw_read: frame -1 = the next one; MF_E_NOT_FOUND past the end; either
+ * destination may be NULL.  Host code only: needs no device. */
+typedef struct mf_raw mf_raw;
+int mf_raw_open(const char* path, mf_raw** out, int* width, int* height, long long* n_frames);
+int mf_raw_read(mf_raw* raw, long long frame, uint16_t* depth_mm, uint8_t* rgb);
+int mf_raw_close(mf_raw* raw);
+/* Kfusion::save_poses (kfusion.cpp:1591-1626): appends one TUM line
+ * "frame tx ty tz qx qy qz qw" (tab-separated, %g) per instance to
+ * <prefix>_camera (label 0) or <prefix>_<label>; the first call per instance
+ * truncates the file.  As the reference does, every line carries the camera's
+ * translation with the instance's own rotation. */
+int mf_save_poses(mf_context* ctx, const char* prefix, int frame);
+/* The quaternion (x, y, z, w) of a pose's rotation (getQuaternion,
+ * preprocessing.cpp:312-320) and one TUM line of mf_save_poses; host code
+ * only.  mf_tum_line returns the line length. */
+int mf_pose_quaternion(const float T[16], float q[4]);
+int mf_tum_line(int frame, const float T_translation[16], const float T_rotation[16], char* buf,
+                int cap);
+
+/* --- mesh export ----------------------------------------------------------
+ * Marching cubes over instance id's octree: algorithms::marching_cube
+ * (lib/algorithms/meshing.hpp:20-208) as Kfusion::dump_mesh calls it
+ * (kfusion.cpp:1560-1588): cells whose eight corners all have weight > 0,
+ * foreground probability > 0.5 and count > 3, inside = tsdf < 0, the
+ * reference's edge intersections, triangles dropped when a vertex leaves
+ * (0, (int)dim] -- the reference truncates the extent to an int, so volumes
+ * under 1 m mesh to nothing; float_bounds = 1 bounds by the float extent
+ * instead.  The triangulation table is generated from the cube's
+ * geometry (gen_mc_tables.py): the same polygons as the reference's table,
+ * possibly split along other diagonals.  Triangles are 9 floats (three
+ * vertices, metres, volume frame), blocks in Morton order and cells x-major
+ * within a block.  tris may be host or device memory; with tris NULL or cap
+ * below the count only n_tris is set.  Synchronises. */
+int mf_mesh(mf_context* ctx, int id, int float_bounds, float* tris, long long cap,
+            long long* n_tris);
+/* writeVtkMesh (commons.h:945-1011): legacy ASCII VTK polydata, three points
+ * per triangle.  Host code only. */
+int mf_write_vtk_mesh(const char* path, const float* tris, long long n);
+/* Kfusion::dump_mesh: <prefix>_<label>.vtk for every instance (the
+ * reference's int bound). */
+int mf_dump_mesh(mf_context* ctx, const char* prefix);
+
 /* --- headless renders ---------------------------------------------------
  * The reference's visualisation kernels (rendering/rendering.cpp) into
  * uchar4 images of W x H (mf_render_normal: uchar3).  `out` may be device

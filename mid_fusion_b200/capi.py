@@ -39,7 +39,9 @@ EXPORTS = [
     "mf_refine_mask_use_motion", "mf_download_mask", "mf_retrack_camera",
     "mf_render_volume", "mf_render_depth", "mf_render_intensity", "mf_render_normal",
     "mf_render_track", "mf_render_mask", "mf_spawn_object", "mf_instance_set_semantics",
-    "mf_fuse_semantics", "mf_instance_semantics",
+    "mf_fuse_semantics", "mf_instance_semantics", "mf_frame_upload_raw", "mf_raw_open",
+    "mf_raw_read", "mf_raw_close", "mf_save_poses", "mf_pose_quaternion", "mf_tum_line",
+    "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh",
 ]
 
 
@@ -304,6 +306,31 @@ class Context:
                                               _ptr(pose, np.float32)))
         return pose.reshape(4, 4)
 
+    def upload_raw(self, depth_mm=None, rgb=None):
+        """A sensor frame (uint16 mm depth, uint8 rgb) of an integer multiple of
+        the frame size (mf_frame_upload_raw)."""
+        d = None if depth_mm is None else np.ascontiguousarray(depth_mm, np.uint16)
+        r = None if rgb is None else np.ascontiguousarray(rgb, np.uint8)
+        h, w = (d if d is not None else r).shape[:2]
+        self._check(self.lib.mf_frame_upload_raw(self.h, _ptr(d, np.uint16), _ptr(r, np.uint8),
+                                                 int(w), int(h)))
+
+    def mesh(self, i, float_bounds=False):
+        """(n, 3, 3) float32 marching-cubes triangles of instance i (mf_mesh)."""
+        n = C.c_longlong()
+        fb = int(float_bounds)
+        self._check(self.lib.mf_mesh(self.h, int(i), fb, None, 0, C.byref(n)))
+        out = np.zeros((max(n.value, 1), 3, 3), np.float32)
+        self._check(self.lib.mf_mesh(self.h, int(i), fb, _ptr(out, np.float32), n.value,
+                                     C.byref(n)))
+        return out[:n.value]
+
+    def dump_mesh(self, prefix):
+        self._check(self.lib.mf_dump_mesh(self.h, str(prefix).encode()))
+
+    def save_poses(self, prefix, frame):
+        self._check(self.lib.mf_save_poses(self.h, str(prefix).encode(), int(frame)))
+
     # ---------------------------------------------------------------- objects
     def spawn_object(self, mask):
         """(T_w_o, volume_size, volume_resol, n_pixels) of mf_spawn_object."""
@@ -443,3 +470,64 @@ class Context:
         self._check(self.lib.mf_interp(self.h, i, _ptr(pos, np.float32), len(pos), field,
                                        _ptr(out, np.float32)))
         return out
+
+
+class RawReader:
+    """The SLAMBench .raw sequence reader of the library (mf_raw_*): host code
+    only, usable without a GPU."""
+
+    def __init__(self, path):
+        self.lib = load()
+        h = C.c_void_p()
+        w, hh, n = C.c_int(), C.c_int(), C.c_longlong()
+        rc = self.lib.mf_raw_open(str(path).encode(), C.byref(h), C.byref(w), C.byref(hh),
+                                  C.byref(n))
+        if rc != MF_OK:
+            raise MfError(f"{ERRORS.get(rc, rc)} cannot open {path}")
+        self.h, self.width, self.height, self.n_frames = h, w.value, hh.value, n.value
+
+    def read(self, frame=-1):
+        """(depth uint16 (H, W), rgb uint8 (H, W, 3)), or None past the end."""
+        d = np.zeros((self.height, self.width), np.uint16)
+        c = np.zeros((self.height, self.width, 3), np.uint8)
+        rc = self.lib.mf_raw_read(self.h, C.c_longlong(frame), _ptr(d, np.uint16),
+                                  _ptr(c, np.uint8))
+        if rc == -4:  # MF_E_NOT_FOUND: past the end
+            return None
+        if rc != MF_OK:
+            raise MfError(f"{ERRORS.get(rc, rc)} reading frame {frame}")
+        return d, c
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mf_raw_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pose_quaternion(T):
+    """(x, y, z, w) of mf_pose_quaternion."""
+    q = np.zeros(4, np.float32)
+    load().mf_pose_quaternion(_ptr(_m4(T), np.float32), _ptr(q, np.float32))
+    return q
+
+
+def tum_line(frame, T_translation, T_rotation):
+    buf = C.create_string_buffer(256)
+    n = load().mf_tum_line(int(frame), _ptr(_m4(T_translation), np.float32),
+                           _ptr(_m4(T_rotation), np.float32), buf, 256)
+    if n < 0:
+        raise MfError("mf_tum_line failed")
+    return buf.value.decode()
+
+
+def write_vtk_mesh(path, tris):
+    t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    rc = load().mf_write_vtk_mesh(str(path).encode(), _ptr(t, np.float32), C.c_longlong(len(t)))
+    if rc != MF_OK:
+        raise MfError(f"{ERRORS.get(rc, rc)} writing {path}")

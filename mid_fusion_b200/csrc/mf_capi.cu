@@ -1,6 +1,8 @@
 // C ABI of the MID-Fusion B200 library (declared in include/midfusion_b200.h).
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 #include "mf_internal.h"
 
@@ -710,6 +712,71 @@ int mf_instance_semantics(mf_context* ctx, int id, int* class_id, int* fused_tim
   if (fused_time) *fused_time = in.fused_time;
   if (probs)
     for (int i = 0; i < cap && i < (int)in.sem.size(); ++i) probs[i] = in.sem[i];
+  return MF_OK;
+}
+
+int mf_frame_upload_raw(mf_context* ctx, const uint16_t* depth_mm, const uint8_t* rgb,
+                        int in_width, int in_height) {
+  if (check(ctx) || in_width <= 0 || in_height <= 0) return MF_E_ARG;
+  return frame_upload_raw(ctx, depth_mm, rgb, in_width, in_height);
+}
+
+int mf_save_poses(mf_context* ctx, const char* prefix, int frame) {
+  if (check(ctx) || !prefix) return MF_E_ARG;
+  const int n = (int)ctx->inst.size();
+  std::vector<float> T(16 * (n + 1));
+  MF_CUDA(cudaMemcpyAsync(T.data(), ctx->d_Twc, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  if (n > 0)
+    MF_CUDA(cudaMemcpyAsync(T.data() + 16, ctx->d_Two, 64 * (size_t)n, cudaMemcpyDeviceToHost,
+                            ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i < n; ++i) {
+    Instance& in = ctx->inst[i];
+    const bool cam = in.label == 0;
+    const std::string path = std::string(prefix) + (cam ? "_camera" : "_" + std::to_string(in.label));
+    FILE* f = std::fopen(path.c_str(), in.pose_saved ? "a" : "w");
+    if (!f) {
+      ctx->last_error = "mf_save_poses: cannot open " + path;
+      return MF_E_NOT_FOUND;
+    }
+    in.pose_saved = true;
+    char line[256];
+    // kfusion.cpp:1615-1617 writes the camera's translation on every line,
+    // with the instance's own rotation
+    const int len = tum_line(frame, T.data(), cam ? T.data() : T.data() + 16 * (i + 1), line,
+                             sizeof(line));
+    std::fwrite(line, 1, len, f);
+    std::fclose(f);
+  }
+  return MF_OK;
+}
+
+int mf_mesh(mf_context* ctx, int id, int float_bounds, float* tris, long long cap,
+            long long* n_tris) {
+  if (check(ctx) || id < 0 || !n_tris || cap < 0) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  return mesh_volume(ctx, id, float_bounds, tris, cap, n_tris);
+}
+
+int mf_write_vtk_mesh(const char* path, const float* tris, long long n) {
+  if (!path || n < 0 || (n > 0 && !tris)) return MF_E_ARG;
+  return write_vtk_mesh(path, tris, n);
+}
+
+int mf_dump_mesh(mf_context* ctx, const char* prefix) {
+  if (check(ctx) || !prefix) return MF_E_ARG;
+  for (int i = 0; i < (int)ctx->inst.size(); ++i) {
+    long long n = 0;
+    if (int rc = mesh_volume(ctx, i, 0, nullptr, 0, &n)) return rc;
+    std::vector<float> tris(9 * (size_t)n + 9);
+    if (int rc = mesh_volume(ctx, i, 0, tris.data(), n, &n)) return rc;
+    const std::string path =
+        std::string(prefix) + "_" + std::to_string(ctx->inst[i].label) + ".vtk";
+    if (int rc = write_vtk_mesh(path.c_str(), tris.data(), n)) {
+      ctx->last_error = "mf_dump_mesh: cannot write " + path;
+      return rc;
+    }
+  }
   return MF_OK;
 }
 

@@ -50,6 +50,7 @@ struct Instance {
   int class_id = 0;
   int fused_time = 0;
   std::vector<float> sem;
+  bool pose_saved = false;   // Object::pose_saved_: later poses append
 };
 
 // One GN problem (camera or object) tracked on the device.
@@ -144,6 +145,15 @@ int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t
 int track_results(Context* ctx, int slot, int8_t* d_out, float* d_err, float* pose_eval);
 int motion_planes(Context* ctx, const int8_t** res, const float** err);
 // headless renders (mf_render.cu; the shaded volume render in mf_raycast.cu)
+// formats (mf_io.cu)
+int frame_upload_raw(Context* ctx, const uint16_t* depth_mm, const uint8_t* rgb, int in_w,
+                     int in_h);
+void pose_quaternion(const float* T, float* q);
+int tum_line(int frame, const float* T_translation, const float* T_rotation, char* buf, int cap);
+// mesh export (mf_mesh.cu)
+int mesh_volume(Context* ctx, int id, int float_bounds, float* tris, long long cap,
+                long long* n_tris);
+int write_vtk_mesh(const char* path, const float* tris, long long n);
 // object management (mf_objects.cu)
 int ensure_export(Context* ctx, size_t bytes);
 int spawn_object(Context* ctx, const uint8_t* mask, float* T_w_o, float* volume_size,

@@ -35,6 +35,15 @@ inline Matrix4 getInverseCameraMatrix(const float4& k) {
 #include "functors/projective_functor.hpp"
 #include "kfusion/rendering_impl.hpp"
 
+// the reference's marching cubes (lib/algorithms/meshing.hpp) names the app's
+// FieldType and Triangle (commons.h:156-162) without declaring them
+#include <mutex>
+#include <sstream>
+#include <vector>
+typedef SDF FieldType;
+struct Triangle { float3 vertexes[3]; };
+#include "algorithms/meshing.hpp"
+
 typedef octlib::key_t refkey_t;
 
 struct RefVol {
@@ -219,6 +228,39 @@ void ref_raycast_objects(void** vols, const float* Two, const int* labels, int n
         label_img[p] = (int)INVALID;
       }
     }
+}
+
+// meshing::compute_index of cell (x, y, z) with the inside test of
+// Kfusion::dump_mesh (tsdf < 0); 0 when the cell's block is not allocated
+int ref_mc_index(void* h, int x, int y, int z) {
+  auto& vol = ((RefVol*)h)->vol;
+  const VoxelBlock<SDF>* b = vol._map_index.fetch(x, y, z);
+  if (!b) return -1;
+  auto inside = [](const Volume<SDF>::compute_type& v) { return v.x < 0.f; };
+  return meshing::compute_index(vol._map_index, b, inside, x, y, z);
+}
+// meshing::interp_vertexes for edge 0..11 (the reference handles 0..2)
+void ref_mc_vertex(void* h, int x, int y, int z, int edge, float* out) {
+  auto& vol = ((RefVol*)h)->vol;
+  auto select = [](const Volume<SDF>::compute_type& v) { return v.x; };
+  const float3 p = meshing::interp_vertexes(vol._map_index, select, x, y, z, edge);
+  out[0] = p.x; out[1] = p.y; out[2] = p.z;
+}
+// algorithms::marching_cube as Kfusion::dump_mesh calls it: the triangle count,
+// and up to cap triangles (9 floats each) into out
+long long ref_marching_cube(void* h, float* out, long long cap) {
+  auto& vol = ((RefVol*)h)->vol;
+  auto inside = [](const Volume<SDF>::compute_type& v) { return v.x < 0.f; };
+  auto select = [](const Volume<SDF>::compute_type& v) { return v.x; };
+  std::vector<Triangle> mesh;
+  algorithms::marching_cube(vol._map_index, select, inside, mesh);
+  for (long long i = 0; i < (long long)mesh.size() && i < cap; ++i)
+    for (int k = 0; k < 3; ++k) {
+      out[9 * i + 3 * k] = mesh[i].vertexes[k].x;
+      out[9 * i + 3 * k + 1] = mesh[i].vertexes[k].y;
+      out[9 * i + 3 * k + 2] = mesh[i].vertexes[k].z;
+    }
+  return (long long)mesh.size();
 }
 
 }  // extern "C"

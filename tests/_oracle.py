@@ -351,6 +351,42 @@ def fuse_semantics(fused, fused_time, probs, recog_times=1):
     return f, ft.value, cid
 
 
+def mesh(impl, vol, float_bounds=False):
+    """Marching-cubes triangles (n, 3, 3) of one volume: the oracle's (or_mesh)
+    or the reference's own algorithms::marching_cube (ref_marching_cube, the
+    int bound only)."""
+    if impl.prefix == "or_":
+        f = impl.lib.or_mesh
+        f.argtypes = [P, C.c_void_p, C.c_longlong, C.c_int]
+        extra = (int(float_bounds),)
+    else:
+        assert not float_bounds
+        f = impl.lib.ref_marching_cube
+        f.argtypes = [P, C.c_void_p, C.c_longlong]
+        extra = ()
+    f.restype = C.c_longlong
+    n = f(vol.h, None, 0, *extra)
+    out = np.zeros((max(n, 1), 3, 3), np.float32)
+    f(vol.h, out.ctypes.data_as(C.c_void_p), n, *extra)
+    return out[:n]
+
+
+def mc_cell(impl, vol, x, y, z):
+    """compute_index of a cell (-1 when its block is unallocated) and the
+    twelve edge intersections (12, 3)."""
+    p = impl.prefix
+    fi = getattr(impl.lib, p + "mc_index")
+    fi.restype = C.c_int
+    fi.argtypes = [P, C.c_int, C.c_int, C.c_int]
+    fv = getattr(impl.lib, p + "mc_vertex")
+    fv.restype = None
+    fv.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int, FP]
+    verts = np.zeros((12, 3), np.float32)
+    for e in range(12):
+        fv(vol.h, x, y, z, e, verts[e])
+    return fi(vol.h, x, y, z), verts
+
+
 def oracle():
     if "or" not in _cache:
         _cache["or"] = Impl(ORACLE_SO, "or_")
