@@ -269,12 +269,13 @@ __device__ __forceinline__ void sdf_update(const SdfArgs& a, const float* mask, 
 }
 
 // projective_functor::update_block, lib/functors/projective_functor.hpp:73-111.
-// One CTA of 256 threads per visited block, two voxels per thread (v and
-// v + 256, i.e. z and z + 4): every field plane is read and written coalesced.
-// The two voxels are processed in phases (project both, fetch both pixels,
-// fetch both voxels' fields, update, store) so their memory accesses overlap.
-// Field planes are only touched for voxels that pass the update test.
-__global__ void __launch_bounds__(256)
+// Persistent CTAs of 512 threads (four per SM, 32 registers), one visited
+// block at a time, one voxel per thread: every field plane is read and written
+// coalesced, and only for voxels that pass the update test.  The next block's
+// slot and corner are loaded during the current one, and the instances'
+// constants come from shared memory, so a block's dependent chain is the pixel
+// fetch and the voxel read-modify-write.
+__global__ void __launch_bounds__(512, 4)
 integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
                         const InstFrame* __restrict__ frames, SdfArgs args, F4 k,
                         const int* __restrict__ visit, const int* __restrict__ visit_count) {
@@ -283,83 +284,80 @@ integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
   const float wlim = args.W - 1.5f, hlim = args.H - 1.5f;
   const int W = args.W;
   const float mu = args.mu, maxweight = args.maxweight;
-  for (int item = blockIdx.x; item < n; item += gridDim.x) {
-    const int slot = visit[item];
-    const int4 m = pool.meta[slot];
-    const Volume& V = vols[m.w];
-    const InstFrame& F = frames[m.w];
-    const float vs = V.dim / V.size;
+  // the instances' constants, staged once per CTA (the tables hold
+  // MAX_INSTANCES entries)
+  __shared__ M4 s_Tcw[MAX_INSTANCES];
+  __shared__ F3 s_delta[MAX_INSTANCES], s_cdelta[MAX_INSTANCES];
+  __shared__ float s_vs[MAX_INSTANCES];
+  for (int i = threadIdx.x; i < MAX_INSTANCES; i += blockDim.x) {
+    s_Tcw[i] = frames[i].Tcw;
+    s_delta[i] = frames[i].delta;
+    s_cdelta[i] = frames[i].cam_delta;
+    s_vs[i] = vols[i].dim / vols[i].size;
+  }
+  __syncthreads();
+  // one voxel per thread; the next block's slot and corner are fetched one
+  // block ahead
+  const int v = threadIdx.x;
+  const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
+  int item = blockIdx.x;
+  int next_slot = item < n ? visit[item] : 0;
+  int4 next_m = item < n ? pool.meta[next_slot] : make_int4(0, 0, 0, 0);
+  for (; item < n; item += gridDim.x) {
+    const int slot = next_slot;
+    const int4 m = next_m;
+    if (item + gridDim.x < n) {
+      next_slot = visit[item + gridDim.x];
+      next_m = pool.meta[next_slot];
+    }
+    const float vs = s_vs[m.w];
     const float* mask = args.masks + (size_t)m.w * args.W * args.H;
-    bool vis[2], upd[2];
-    F3 pos[2];
-    int pix[2];
-    // phase 1: voxel -> pixel
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int v = threadIdx.x + h * 256;
-      const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
-      const F3 start = xform(F.Tcw, mk3(m.x * vs, (m.y + y) * vs, (m.z + z) * vs));
-      const F3 camerastart = xform(K, start);
-      const F3 cv = camerastart + ((float)x * F.cam_delta);
-      pos[h] = start + ((float)x * F.delta);
-      vis[h] = false;
-      pix[h] = 0;
-      if (pos[h].z < 0.0001f) continue;
+    // voxel -> pixel
+    const F3 start = xform(s_Tcw[m.w], mk3(m.x * vs, (m.y + y) * vs, (m.z + z) * vs));
+    const F3 camerastart = xform(K, start);
+    const F3 cv = camerastart + ((float)x * s_cdelta[m.w]);
+    const F3 pos = start + ((float)x * s_delta[m.w]);
+    bool vis = false;
+    int pix = 0;
+    if (pos.z >= 0.0001f) {
       const float inv = 1.f / cv.z;
       const float pxf = cv.x * inv + 0.5f, pyf = cv.y * inv + 0.5f;
-      if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) continue;
-      vis[h] = true;
-      pix[h] = (int)((unsigned)pxf + W * (unsigned)pyf);
-    }
-    // phase 2: depth / mask at the pixel, the update test of sdf_update
-    float depthS[2], mval[2], sdf[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      depthS[h] = vis[h] ? __ldg(args.depth + pix[h]) : 0.f;
-      mval[h] = vis[h] ? __ldg(mask + pix[h]) : -1.f;
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      upd[h] = false;
-      sdf[h] = 0.f;
-      if (!vis[h] || depthS[h] <= 0 || mval[h] < 0) continue;
-      const F3 p = pos[h];
-      const float diff = (depthS[h] - p.z) * sqrtf(1 + sq(p.x / p.z) + sq(p.y / p.z));
-      if (diff > -mu) {
-        upd[h] = true;
-        sdf[h] = fmn(1.f, diff / mu);
+      if (!(pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim)) {
+        vis = true;
+        pix = (int)((unsigned)pxf + W * (unsigned)pyf);
       }
     }
-    // phase 3: read-modify-write of the voxels that update
-    float t[2], wt[2], r[2], g[2], b[2];
-    int c[2], w[2];
-    double fg[2];
-    F3 rgb[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (!upd[h]) continue;
-      const size_t o = (size_t)slot * 512 + threadIdx.x + h * 256;
-      t[h] = pool.tsdf[o]; wt[h] = pool.wt[o]; r[h] = pool.r[o]; g[h] = pool.g[o];
-      b[h] = pool.b[o]; c[h] = pool.c[o]; fg[h] = pool.fg[o]; w[h] = pool.w[o];
-      rgb[h] = args.rgb[pix[h]];
+    // depth / mask at the pixel, the update test of sdf_update
+    const float depthS = vis ? __ldg(args.depth + pix) : 0.f;
+    const float mval = vis ? __ldg(mask + pix) : -1.f;
+    bool upd = false;
+    float sdf = 0.f;
+    if (vis && depthS > 0 && mval >= 0) {
+      const float diff = (depthS - pos.z) * sqrtf(1 + sq(pos.x / pos.z) + sq(pos.y / pos.z));
+      if (diff > -mu) {
+        upd = true;
+        sdf = fmn(1.f, diff / mu);
+      }
     }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (!upd[h]) continue;
+    // read-modify-write of the voxel
+    if (upd) {
+      const size_t o = (size_t)slot * 512 + v;
+      const float t = pool.tsdf[o], wt = pool.wt[o], r = pool.r[o], g = pool.g[o],
+                  b = pool.b[o];
+      const int c = pool.c[o], w = pool.w[o];
+      const double fg = pool.fg[o];
+      const F3 rgb = args.rgb[pix];
       // sdf_update, apps/kfusion/src/cpp/kfusion/mapping_impl.hpp:26-46
-      const float x = clampf((wt[h] * t[h] + sdf[h]) / (wt[h] + 1), -1.f, 1.f);
-      const float y = fmn(wt[h] + 1, maxweight);
-      const int cc = c[h];
-      const float nr = (rgb[h].x + r[h] * cc) / (cc + 1);
-      const float ng = (rgb[h].y + g[h] * cc) / (cc + 1);
-      const float nb = (rgb[h].z + b[h] * cc) / (cc + 1);
-      const int ww = w[h];
-      const double nfg = ((double)mval[h] + fg[h] * ww) / (ww + 1);
-      const size_t o = (size_t)slot * 512 + threadIdx.x + h * 256;
-      pool.tsdf[o] = x; pool.wt[o] = y; pool.r[o] = nr; pool.g[o] = ng; pool.b[o] = nb;
-      pool.c[o] = cc + 1; pool.fg[o] = nfg; pool.w[o] = ww + 1;
+      pool.tsdf[o] = clampf((wt * t + sdf) / (wt + 1), -1.f, 1.f);
+      pool.wt[o] = fmn(wt + 1, maxweight);
+      pool.r[o] = (rgb.x + r * c) / (c + 1);
+      pool.g[o] = (rgb.y + g * c) / (c + 1);
+      pool.b[o] = (rgb.z + b * c) / (c + 1);
+      pool.c[o] = c + 1;
+      pool.fg[o] = ((double)mval + fg * w) / (w + 1);
+      pool.w[o] = w + 1;
     }
-    const int any = __syncthreads_or(vis[0] || vis[1]);
+    const int any = __syncthreads_or(vis);
     if (threadIdx.x == 0) pool.active[slot] = any ? 1 : 0;
   }
 }
@@ -593,7 +591,7 @@ int profile_integrate(Context* ctx, int reps, double* us, double* bytes) {
   cudaEventCreate(&e1);
   cudaEventRecord(e0, ctx->stream);
   for (int r = 0; r < reps; ++r)
-    integrate_blocks_kernel<<<sms * 8, 256, 0, ctx->stream>>>(ctx->pool, ctx->d_vols,
+    integrate_blocks_kernel<<<sms * 4, 512, 0, ctx->stream>>>(ctx->pool, ctx->d_vols,
                                                              ctx->d_frames, a, k, ctx->d_visit,
                                                              ctx->d_visit_count);
   cudaEventRecord(e1, ctx->stream);
@@ -629,7 +627,7 @@ int stage_integrate(Context* ctx, const IdList& ids) {
   const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  integrate_blocks_kernel<<<sms * 8, 256, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
+  integrate_blocks_kernel<<<sms * 4, 512, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
                                                            a, k, ctx->d_visit, ctx->d_visit_count);
   MF_CUDA(cudaGetLastError());
   if (max_nodes > 0) {
