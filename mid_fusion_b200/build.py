@@ -40,7 +40,7 @@ def up_to_date():
     if not os.path.exists(LIB):
         return False
     t = os.path.getmtime(LIB)
-    return all(os.path.getmtime(f) <= t for f in sources() + headers())
+    return all(os.path.getmtime(f) <= t for f in sources() + headers() + [__file__])
 
 
 def build(force=False, verbose=False, extra=()):

@@ -71,7 +71,8 @@ static int frame_body(Context* ctx, bool track, bool labels) {
       if (int rc = stage_integrate(ctx, one)) return rc;
     }
   }
-  if (int rc = stage_prepare(ctx, all)) return rc;
+  // the instance frames prepared for integration hold for the raycast: no
+  // pose changes in between
   if (int rc = stage_raycast(ctx, all, ctx->ray_epsilon)) return rc;
   return track_set_ref(ctx);
 }
