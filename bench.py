@@ -136,6 +136,7 @@ def measured_peaks():
 def run_ours(args, rank, world, local_rank):
     import torch
     from mid_fusion_b200 import build
+    from mid_fusion_b200 import capi
     from mid_fusion_b200.capi import Context
 
     n_frames = 1 + args.warmup + args.steps
@@ -171,15 +172,25 @@ def run_ours(args, rank, world, local_rank):
     # device-resident inputs
     d_depth, d_rgb, d_lab = to_device(frames)
 
-    def run(batched, record_poses=True, scene=None, inputs=None):
+    def run(batched, record_poses=True, scene=None, inputs=None, tune=None):
         """Frames through mf_process_frame_device; device time per frame after
-        1 + warmup untimed frames."""
+        1 + warmup untimed frames.  tune="auto": mf_autotune on the last
+        warm-up frame (outside the timed region; its report lands in
+        tuned[id(ctx)]); a dict {stage: variant}: those launch shapes from the
+        start."""
         ctx = make_ctx(batched, scene)
+        if isinstance(tune, dict):
+            for stage, v in tune.items():
+                ctx.tune_set(stage, v)
         dd, dr, dl = inputs or (d_depth, d_rgb, d_lab)
         stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
         lib = ctx.lib
         times, poses = [], []
         for f in range(len(dd)):
+            # two warm-up frames after the tuner re-capture both frame graphs
+            # (one per reference-pyramid parity) with the chosen shapes
+            if tune == "auto" and f == args.warmup - 1:
+                tuned[id(ctx)] = ctx.autotune(reps=5)
             flush.fill_(f & 0xff)
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -211,19 +222,26 @@ def run_ours(args, rank, world, local_rank):
                              To.ctypes.data_as(ctypes.c_void_p))
         return Tc.reshape(4, 4), To.reshape(-1, 4, 4)
 
-    stats = {}
+    def shapes(ctx):
+        return {capi.TUNE_RAYCAST: ctx.tune_get(capi.TUNE_RAYCAST),
+                capi.TUNE_INTEGRATE: ctx.tune_get(capi.TUNE_INTEGRATE)}
+
+    stats, tuned = {}, {}
+    auto = None if args.no_tune else "auto"
     sampler = ClockSampler(local_rank)
     # ---- batched, device-resident
     with sampler:
-        ctx_b, t_b, poses_b, st_b = run(True)
+        ctx_b, t_b, poses_b, st_b = run(True, tune=auto)
     total_b = sum(t_b)
+    tune_b = shapes(ctx_b)  # the plain and e2e runs use the same launch shapes
     prof = ctx_b.profile(reps=20)  # after the timed frames (re-integrates the last one)
     if args.profile:  # the batched device path only (for profiler launch lists)
         return dict(total_b=total_b, total_p=total_b, total_e=total_b, dpos=0.0, gt_err=0.0,
                     status=(st_b, 0), clocks=sampler.summary(), h2d=0, d2h=0,
-                    ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, n_inst=len(s.instances))
+                    ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, n_inst=len(s.instances),
+                    tune=tuned.get(id(ctx_b)))
     # ---- plain (one instance per launch, host-driven GN)
-    ctx_p, t_p, poses_p, st_p = run(False)
+    ctx_p, t_p, poses_p, st_p = run(False, tune=tune_b)
     total_p = sum(t_p)
     # pose agreement between the two paths over the whole sequence
     dpos = 0.0
@@ -238,8 +256,8 @@ def run_ours(args, rank, world, local_rank):
     if do_uneven:
         su = scene_for(rank, n_uneven, "uneven")
         ins = to_device(rendered["uneven"])
-        cub, tub, pub, stub = run(True, scene=su, inputs=ins)
-        cup, tup, pup, stup = run(False, scene=su, inputs=ins)
+        cub, tub, pub, stub = run(True, scene=su, inputs=ins, tune=auto)
+        cup, tup, pup, stup = run(False, scene=su, inputs=ins, tune=shapes(cub))
         du = 0.0
         for (cb, ob), (cp, op) in zip(pub, pup):
             du = max(du, float(np.abs(cb[:3, 3] - cp[:3, 3]).max()),
@@ -250,7 +268,7 @@ def run_ours(args, rank, world, local_rank):
                   "ms_batched": round(1e3 * ub / len(tub), 4),
                   "ms_plain": round(1e3 * up / len(tup), 4),
                   "batched_over_plain": round(up / ub, 3), "pose_diff_batched_vs_plain_m": du,
-                  "status_flags": [stub, stup]}
+                  "autotune": tuned.get(id(cub)), "status_flags": [stub, stup]}
         for c in (cub, cup):
             c.close()
         del ins
@@ -287,6 +305,8 @@ def run_ours(args, rank, world, local_rank):
     # ---- e2e through the C ABI from pinned host buffers
     import ctypes
     ctx_e = make_ctx(True)
+    for stage, v in tune_b.items():
+        ctx_e.tune_set(stage, v)
     stream_e = torch.cuda.ExternalStream(ctx_e.stream(), device=dev)
     h_depth = [torch.from_numpy(f[0]).pin_memory() for f in frames]
     h_rgb = [torch.from_numpy(np.ascontiguousarray(f[1])).pin_memory() for f in frames]
@@ -327,7 +347,8 @@ def run_ours(args, rank, world, local_rank):
     return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
                 status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
                 ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
-                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint, motion=motion)
+                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint, motion=motion,
+                tune=tuned.get(id(ctx_b)))
 
 
 def run_motion(ctx, frames, poses, n, dev, torch):
@@ -493,6 +514,8 @@ def main():
     ap.add_argument("--workers", type=int, default=min(32, os.cpu_count() or 4))
     ap.add_argument("--pool-blocks", type=int, default=1 << 18)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default launch shapes (no mf_autotune before the timed frames)")
     ap.add_argument("--workload", default="multi", choices=["multi", "uneven"],
                     help="multi: background + 3 objects (the headline); uneven: + 12 objects")
     ap.add_argument("--profile", action="store_true",
@@ -574,6 +597,7 @@ def main():
         "uneven12": r.get("uneven"),
         "adjoint": r.get("adjoint"),
         "motion": r.get("motion"),
+        "autotune": r.get("tune"),
         "pose_diff_batched_vs_plain_m": r["dpos"],
         "camera_err_vs_gt_m": r["gt_err"],
         "e2e": {"value": round(value_e, 2), "unit": "frames/s",

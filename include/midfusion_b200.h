@@ -401,6 +401,39 @@ int mf_profile(mf_context* ctx, int reps, double* out, int n);
 /* Batched mode replays the frame as a CUDA graph once captured (default 1). */
 int mf_set_graphs(mf_context* ctx, int enable);
 
+/* --- launch-shape autotuner (no counterpart in the reference) ----------
+ * Two kernels of the frame run in one of several launch shapes that change
+ * their speed but not their results (each pixel / voxel is computed by one
+ * thread from the same inputs in every shape):
+ *   MF_TUNE_RAYCAST    the composite raycast (raycastObjectList): the pixel
+ *                      tile of a 128-thread CTA and the register bound;
+ *   MF_TUNE_INTEGRATE  the voxel-block integration (projective_functor::
+ *                      update_block): 512-thread CTAs resident per SM.
+ * Variant 0 of each is the default.  A context starts with the defaults. */
+#define MF_TUNE_RAYCAST 0
+#define MF_TUNE_INTEGRATE 1
+#define MF_TUNE_MAX_VARIANTS 16
+/* Number of candidate shapes of `stage` (no context, no device needed). */
+int mf_tune_candidates(int stage, int* n);
+/* One-line description of candidate `variant` of `stage` into buf. */
+int mf_tune_describe(int stage, int variant, char* buf, int cap);
+/* Times every candidate of both stages on the current frame (`reps` launches,
+ * best of 3 trials, CUDA events) and keeps the fastest of each; the current
+ * choice stays unless another is more than 1 % faster.  raycast_us and
+ * integrate_us (MF_TUNE_MAX_VARIANTS floats each, may be NULL) receive the
+ * microseconds per launch of every candidate.  Needs a processed frame (the
+ * instances, the frame inputs and the map of the last mf_process_frame or
+ * mf_integrate).  Leaves the map and the model maps unchanged: the raycasts
+ * write scratch maps and the integrations update a scratch copy of the pool
+ * slots in use (allocated for the call and freed before it returns).  The
+ * next batched frame re-captures its graph with the chosen shapes.
+ * Synchronises. */
+int mf_autotune(mf_context* ctx, int reps, float* raycast_us, float* integrate_us);
+/* The candidate in use for `stage`, or set it (a saved choice of an earlier
+ * mf_autotune); an unknown stage or variant is MF_E_ARG. */
+int mf_tune_get(mf_context* ctx, int stage, int* variant);
+int mf_tune_set(mf_context* ctx, int stage, int variant);
+
 /* --- inspection (parity checks, debugging) -----------------------------
  * Blocks: key (code | level), corner voxel, VoxelBlock::active_, and when
  * `voxels` is not NULL the 512 voxels in the reference's 40-byte AoS layout

@@ -41,8 +41,11 @@ EXPORTS = [
     "mf_render_track", "mf_render_mask", "mf_spawn_object", "mf_instance_set_semantics",
     "mf_fuse_semantics", "mf_instance_semantics", "mf_frame_upload_raw", "mf_raw_open",
     "mf_raw_read", "mf_raw_close", "mf_save_poses", "mf_pose_quaternion", "mf_tum_line",
-    "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh",
+    "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh", "mf_tune_candidates", "mf_tune_describe",
+    "mf_autotune", "mf_tune_get", "mf_tune_set",
 ]
+
+TUNE_RAYCAST, TUNE_INTEGRATE, TUNE_MAX_VARIANTS = 0, 1, 16
 
 
 class MfConfig(C.Structure):
@@ -78,6 +81,23 @@ def _ptr(a, dtype):
         return None
     assert a.dtype == dtype and a.flags.c_contiguous, (a.dtype, dtype)
     return a.ctypes.data_as(C.c_void_p)
+
+
+def tune_candidates(stage):
+    """Number of launch-shape candidates of a tuned stage (TUNE_RAYCAST, TUNE_INTEGRATE)."""
+    n = C.c_int()
+    rc = load().mf_tune_candidates(int(stage), C.byref(n))
+    if rc != MF_OK:
+        raise MfError(f"{ERRORS.get(rc, rc)} stage {stage}")
+    return n.value
+
+
+def tune_describe(stage, variant):
+    buf = C.create_string_buffer(128)
+    rc = load().mf_tune_describe(int(stage), int(variant), buf, len(buf))
+    if rc != MF_OK:
+        raise MfError(f"{ERRORS.get(rc, rc)} stage {stage} variant {variant}")
+    return buf.value.decode()
 
 
 def _m4(T):
@@ -201,6 +221,29 @@ class Context:
         self._check(self.lib.mf_profile(self.h, int(reps), _ptr(out, np.float64), len(out)))
         return {"gn_l0_us": out[0], "gn_l0_bytes": out[1], "integrate_us": out[2],
                 "integrate_bytes": out[3], "raycast_us": out[4]}
+
+    def autotune(self, reps=5):
+        """Time every launch-shape candidate on the current frame and keep the
+        fastest (mf_autotune); returns the per-candidate times and the choice."""
+        ray = np.zeros(TUNE_MAX_VARIANTS, np.float32)
+        integ = np.zeros(TUNE_MAX_VARIANTS, np.float32)
+        self._check(self.lib.mf_autotune(self.h, int(reps), _ptr(ray, np.float32),
+                                         _ptr(integ, np.float32)))
+        out = {}
+        for name, stage, t in (("raycast", TUNE_RAYCAST, ray), ("integrate", TUNE_INTEGRATE, integ)):
+            n = tune_candidates(stage)
+            v = self.tune_get(stage)
+            out[name] = {"us": [round(float(x), 2) for x in t[:n]], "chosen": v,
+                         "shape": tune_describe(stage, v)}
+        return out
+
+    def tune_get(self, stage):
+        v = C.c_int()
+        self._check(self.lib.mf_tune_get(self.h, int(stage), C.byref(v)))
+        return v.value
+
+    def tune_set(self, stage, variant):
+        self._check(self.lib.mf_tune_set(self.h, int(stage), int(variant)))
 
     def status(self):
         f = C.c_int()

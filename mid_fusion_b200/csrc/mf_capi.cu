@@ -510,6 +510,41 @@ int mf_set_graphs(mf_context* ctx, int enable) {
   return MF_OK;
 }
 
+int mf_tune_candidates(int stage, int* n) {
+  if (!n || (stage != MF_TUNE_RAYCAST && stage != MF_TUNE_INTEGRATE)) return MF_E_ARG;
+  *n = tune_variant_count(stage);
+  return MF_OK;
+}
+
+int mf_tune_describe(int stage, int variant, char* buf, int cap) {
+  if (!buf || cap < 1 || variant < 0 || variant >= tune_variant_count(stage)) return MF_E_ARG;
+  if (stage == MF_TUNE_RAYCAST) ray_variant_describe(variant, buf, cap);
+  else int_variant_describe(variant, buf, cap);
+  return MF_OK;
+}
+
+int mf_autotune(mf_context* ctx, int reps, float* raycast_us, float* integrate_us) {
+  if (check(ctx) || reps < 1) return MF_E_ARG;
+  float ray[MAX_TUNE_VARIANTS] = {0}, integ[MAX_TUNE_VARIANTS] = {0};
+  if (int rc = autotune(ctx, reps, ray, integ)) return rc;
+  if (raycast_us) std::memcpy(raycast_us, ray, sizeof(ray));
+  if (integrate_us) std::memcpy(integrate_us, integ, sizeof(integ));
+  return MF_OK;
+}
+
+int mf_tune_get(mf_context* ctx, int stage, int* variant) {
+  if (check(ctx) || !variant) return MF_E_ARG;
+  if (stage == MF_TUNE_RAYCAST) *variant = ctx->tune.ray;
+  else if (stage == MF_TUNE_INTEGRATE) *variant = ctx->tune.integrate;
+  else return MF_E_ARG;
+  return MF_OK;
+}
+
+int mf_tune_set(mf_context* ctx, int stage, int variant) {
+  if (check(ctx)) return MF_E_ARG;
+  return tune_set(ctx, stage, variant);
+}
+
 int mf_preprocess(mf_context* ctx) {
   if (check(ctx)) return MF_E_ARG;
   return track_preprocess(ctx);

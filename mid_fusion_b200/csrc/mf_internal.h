@@ -56,6 +56,16 @@ struct Instance {
 // One GN problem (camera or object) tracked on the device.
 struct TrackState;
 
+// Launch shapes chosen by the autotuner (mf_tune.cu): an index into each
+// tuned kernel's candidate table, 0 = the default shape.  `gen` changes with
+// every choice so that captured frame graphs are rebuilt.
+constexpr int MAX_TUNE_VARIANTS = MF_TUNE_MAX_VARIANTS;
+struct Tune {
+  int ray = 0;        // raycast_objects_kernel (ray_variants, mf_raycast.cu)
+  int integrate = 0;  // integrate_blocks_kernel (int_variants, mf_volume.cu)
+  unsigned gen = 0;
+};
+
 struct Context {
   mf_config cfg;
   int W = 0, H = 0;
@@ -100,6 +110,7 @@ struct Context {
   void* graphs = nullptr;           // captured frame graphs (mf_pipeline.cu)
   bool use_graphs = true;
   TrackState* track = nullptr;
+  Tune tune;                        // autotuned launch shapes
   uint8_t* d_render = nullptr;      // W*H*4 render scratch for host destinations
   void* d_render_small = nullptr;   // colour / pointer tables of a render
   size_t render_small_bytes = 0;
@@ -184,6 +195,19 @@ int profile_integrate(Context* ctx, int reps, double* us, double* bytes);
 int profile_gn(Context* ctx, int reps, double* us, double* bytes);
 int profile_raycast(Context* ctx, int reps, double* us);
 void pipeline_free(Context* ctx);
+// launch-shape candidates (autotuner)
+int ray_variant_count();
+void ray_variant_describe(int v, char* buf, int cap);
+int int_variant_count();
+void int_variant_describe(int v, char* buf, int cap);
+// integrate_blocks_kernel alone, on `pool` (the live pool or a scratch copy),
+// over the visit list of the last stage_integrate / visit_list
+int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant);
+int build_visit_list(Context* ctx, uint32_t inst_mask);
+// the autotuner (mf_tune.cu)
+int tune_variant_count(int stage);
+int autotune(Context* ctx, int reps, float* ray_us, float* int_us);
+int tune_set(Context* ctx, int stage, int variant);
 size_t graph_kernel_nodes(Context* ctx);
 int volume_create(Context* ctx, Instance& in);
 void volume_free(Instance& in);

@@ -19,6 +19,7 @@ struct FrameGraphs {
   size_t kernel_nodes[2] = {0, 0};
   int n_instances = -1;
   bool labels = false;
+  unsigned tune_gen = 0;   // launch shapes the graphs were captured with
 };
 
 static FrameGraphs& graphs(Context* ctx) {
@@ -83,11 +84,13 @@ int process_frame(Context* ctx, bool labels) {
   const bool track = track_has_ref(ctx);
   if (!ctx->cfg.batched || !track || !ctx->use_graphs) return frame_body(ctx, track, labels);
   FrameGraphs& g = graphs(ctx);
-  if (g.n_instances != (int)ctx->inst.size() || g.labels != labels) {
+  if (g.n_instances != (int)ctx->inst.size() || g.labels != labels ||
+      g.tune_gen != ctx->tune.gen) {
     for (auto& e : g.exec)
       if (e) { cudaGraphExecDestroy(e); e = nullptr; }
     g.n_instances = (int)ctx->inst.size();
     g.labels = labels;
+    g.tune_gen = ctx->tune.gen;
   }
   const int parity = track_parity(ctx);
   if (!g.exec[parity]) {

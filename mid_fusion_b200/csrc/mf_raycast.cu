@@ -1,3 +1,4 @@
+#include <cstdio>
 #include <cstring>
 // Multi-instance octree raycasting on the device.
 //
@@ -174,12 +175,16 @@ struct RayArgs {
 };
 
 // One thread per pixel, instances in list order (the reference's object loop).
-__global__ void __launch_bounds__(128)
+// 128 threads cover a TW x (128 / TW) pixel tile; MINB is the residency the
+// register allocation is bounded for (1: unbounded).  Every variant computes
+// each pixel alike, so the autotuner may pick any of them (ray_variants).
+template <int TW, int MINB>
+__global__ void __launch_bounds__(128, MINB)
 raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
                        const InstFrame* __restrict__ frames, IdList ids, RayArgs a,
                        int* __restrict__ status) {
-  const int x = blockIdx.x * 16 + (threadIdx.x & 15);
-  const int y = blockIdx.y * 8 + (threadIdx.x >> 4);
+  const int x = blockIdx.x * TW + (threadIdx.x % TW);
+  const int y = blockIdx.y * (128 / TW) + (threadIdx.x / TW);
   if (x >= a.W || y >= a.H) return;
   const int p = x + y * a.W;
   __shared__ int s_slot[8 * 128];
@@ -254,14 +259,43 @@ int stage_raycast(Context* ctx, const IdList& ids, float epsilon) {
   return stage_raycast_to(ctx, ids, epsilon, ctx->d_vertex, ctx->d_normal, ctx->d_label);
 }
 
+// Launch-shape candidates of raycast_objects_kernel: tile width x register
+// bound.  Entry 0 is the default.
+struct RayVariant {
+  int tw, minb;
+  void (*fn)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, int*);
+};
+static const RayVariant ray_variants[] = {
+    {16, 1, raycast_objects_kernel<16, 1>}, {32, 1, raycast_objects_kernel<32, 1>},
+    {8, 1, raycast_objects_kernel<8, 1>},   {16, 6, raycast_objects_kernel<16, 6>},
+    {32, 6, raycast_objects_kernel<32, 6>}, {8, 6, raycast_objects_kernel<8, 6>},
+    {16, 8, raycast_objects_kernel<16, 8>}, {32, 8, raycast_objects_kernel<32, 8>},
+    {8, 8, raycast_objects_kernel<8, 8>},
+};
+constexpr int N_RAY_VARIANTS = (int)(sizeof(ray_variants) / sizeof(ray_variants[0]));
+static_assert(N_RAY_VARIANTS <= MAX_TUNE_VARIANTS, "raycast candidate table too long");
+
+int ray_variant_count() { return N_RAY_VARIANTS; }
+
+void ray_variant_describe(int v, char* buf, int cap) {
+  const RayVariant& r = ray_variants[v];
+  if (r.minb > 1)
+    snprintf(buf, cap, "raycast tile %dx%d, registers bounded for %d CTAs/SM", r.tw, 128 / r.tw,
+             r.minb);
+  else
+    snprintf(buf, cap, "raycast tile %dx%d, registers unbounded", r.tw, 128 / r.tw);
+}
+
 int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex, F3* normal,
                      int* label) {
   if (ids.n == 0) return MF_OK;
   const mf_config& c = ctx->cfg;
   RayArgs a{vertex, normal, label, ctx->W, ctx->H, c.near_plane, c.far_plane, c.mu, epsilon};
-  dim3 grid((ctx->W + 15) / 16, (ctx->H + 7) / 8);
-  raycast_objects_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
-                                                        ids, a, ctx->d_status);
+  const RayVariant& r = ray_variants[ctx->tune.ray];
+  const int th = 128 / r.tw;
+  dim3 grid((ctx->W + r.tw - 1) / r.tw, (ctx->H + th - 1) / th);
+  r.fn<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a,
+                                      ctx->d_status);
   MF_CUDA(cudaGetLastError());
   return MF_OK;
 }

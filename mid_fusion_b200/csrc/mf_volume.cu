@@ -9,6 +9,7 @@
 // request counts also reproduce the reference's allocation-list quirks (see
 // alloc_commit_kernel).
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include "mf_internal.h"
 #include "mf_sample.cuh"
@@ -275,7 +276,10 @@ __device__ __forceinline__ void sdf_update(const SdfArgs& a, const float* mask, 
 // slot and corner are loaded during the current one, and the instances'
 // constants come from shared memory, so a block's dependent chain is the pixel
 // fetch and the voxel read-modify-write.
-__global__ void __launch_bounds__(512, 4)
+// MINB 512-thread CTAs are resident per SM (the register bound) and the grid
+// is MINB CTAs per SM; every variant updates each voxel alike (int_variants).
+template <int MINB>
+__global__ void __launch_bounds__(512, MINB)
 integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
                         const InstFrame* __restrict__ frames, SdfArgs args, F4 k,
                         const int* __restrict__ visit, const int* __restrict__ visit_count) {
@@ -591,9 +595,7 @@ int profile_integrate(Context* ctx, int reps, double* us, double* bytes) {
   cudaEventCreate(&e1);
   cudaEventRecord(e0, ctx->stream);
   for (int r = 0; r < reps; ++r)
-    integrate_blocks_kernel<<<sms * 4, 512, 0, ctx->stream>>>(ctx->pool, ctx->d_vols,
-                                                             ctx->d_frames, a, k, ctx->d_visit,
-                                                             ctx->d_visit_count);
+    if (int rc = launch_integrate_blocks(ctx, ctx->pool, ctx->tune.integrate)) return rc;
   cudaEventRecord(e1, ctx->stream);
   MF_CUDA(cudaEventSynchronize(e1));
   float ms = 0;
@@ -609,6 +611,47 @@ int profile_integrate(Context* ctx, int reps, double* us, double* bytes) {
   return MF_OK;
 }
 
+// Launch-shape candidates of integrate_blocks_kernel; entry 0 is the default.
+struct IntVariant {
+  int minb;
+  void (*fn)(Pool, const Volume*, const InstFrame*, SdfArgs, F4, const int*, const int*);
+};
+static const IntVariant int_variants[] = {
+    {4, integrate_blocks_kernel<4>}, {3, integrate_blocks_kernel<3>},
+    {2, integrate_blocks_kernel<2>},
+};
+constexpr int N_INT_VARIANTS = (int)(sizeof(int_variants) / sizeof(int_variants[0]));
+static_assert(N_INT_VARIANTS <= MAX_TUNE_VARIANTS, "integration candidate table too long");
+
+int int_variant_count() { return N_INT_VARIANTS; }
+
+void int_variant_describe(int v, char* buf, int cap) {
+  snprintf(buf, cap, "integrate %d x 512-thread CTAs per SM", int_variants[v].minb);
+}
+
+int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant) {
+  const mf_config& c = ctx->cfg;
+  SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
+  const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  const IntVariant& v = int_variants[variant];
+  v.fn<<<sms * v.minb, 512, 0, ctx->stream>>>(pool, ctx->d_vols, ctx->d_frames, a, k,
+                                              ctx->d_visit, ctx->d_visit_count);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+// projective_functor::build_active_list over the instances in `inst_mask`.
+int build_visit_list(Context* ctx, uint32_t inst_mask) {
+  MF_CUDA(cudaMemsetAsync(ctx->d_visit_count, 0, sizeof(int), ctx->stream));
+  visit_list_kernel<<<div_up(ctx->pool.cap, 256), 256, 0, ctx->stream>>>(
+      ctx->pool, ctx->d_vols, ctx->d_frames, inst_mask, ctx->W, ctx->H, ctx->d_visit,
+      ctx->d_visit_count);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
 int stage_integrate(Context* ctx, const IdList& ids) {
   if (ids.n == 0) return MF_OK;
   const mf_config& c = ctx->cfg;
@@ -618,18 +661,10 @@ int stage_integrate(Context* ctx, const IdList& ids) {
     mask |= 1u << ids.v[i];
     max_nodes = std::max(max_nodes, ctx->inst[ids.v[i]].vol.n_nodes);
   }
-  MF_CUDA(cudaMemsetAsync(ctx->d_visit_count, 0, sizeof(int), ctx->stream));
-  visit_list_kernel<<<div_up(ctx->pool.cap, 256), 256, 0, ctx->stream>>>(
-      ctx->pool, ctx->d_vols, ctx->d_frames, mask, ctx->W, ctx->H, ctx->d_visit,
-      ctx->d_visit_count);
-  MF_CUDA(cudaGetLastError());
+  if (int rc = build_visit_list(ctx, mask)) return rc;
+  if (int rc = launch_integrate_blocks(ctx, ctx->pool, ctx->tune.integrate)) return rc;
   SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
   const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-  integrate_blocks_kernel<<<sms * 4, 512, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
-                                                           a, k, ctx->d_visit, ctx->d_visit_count);
-  MF_CUDA(cudaGetLastError());
   if (max_nodes > 0) {
     integrate_nodes_kernel<<<dim3(div_up(max_nodes, 128), ids.n), 128, 0, ctx->stream>>>(
         ctx->d_vols, ctx->d_frames, a, k, ids);

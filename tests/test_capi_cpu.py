@@ -62,3 +62,22 @@ def test_bad_arguments_are_rejected(lib):
     cfg.max_instances = 1000
     h = C.c_void_p()
     assert lib.mf_create(C.byref(cfg), C.byref(h)) == -1
+
+
+def test_tune_candidate_tables(lib):
+    """The autotuner's candidate tables answer without a device; unknown stages
+    and variants are rejected."""
+    n_ray = capi.tune_candidates(capi.TUNE_RAYCAST)
+    n_int = capi.tune_candidates(capi.TUNE_INTEGRATE)
+    assert 1 < n_ray <= capi.TUNE_MAX_VARIANTS and 1 < n_int <= capi.TUNE_MAX_VARIANTS
+    shapes = [capi.tune_describe(capi.TUNE_RAYCAST, v) for v in range(n_ray)]
+    assert len(set(shapes)) == n_ray and shapes[0].startswith("raycast tile 16x8")
+    assert capi.tune_describe(capi.TUNE_INTEGRATE, 0).startswith("integrate 4 x")
+    n = C.c_int()
+    assert lib.mf_tune_candidates(2, C.byref(n)) == -1
+    buf = C.create_string_buffer(64)
+    assert lib.mf_tune_describe(capi.TUNE_RAYCAST, n_ray, buf, 64) == -1
+    assert lib.mf_tune_describe(capi.TUNE_INTEGRATE, -1, buf, 64) == -1
+    assert lib.mf_tune_get(None, 0, C.byref(n)) == -1
+    assert lib.mf_tune_set(None, 0, 0) == -1
+    assert lib.mf_autotune(None, 3, None, None) == -1
