@@ -239,6 +239,8 @@ struct Volume {
   long long n_nodes;           // entries in node_tab
   float* n_tsdf; float* n_wt; float* n_r; float* n_g; float* n_b;
   int* n_c; double* n_fg; int* n_w;  // n_nodes x 8 each
+  int* bbox;                   // corners (voxels) of the allocated blocks other than
+                               // block 0: min x, y, z then max x, y, z (empty: min > max)
   uint32_t* req;               // allocation requests per block-table entry
   unsigned long long* last_emit;  // (emission order << 32) | table index
   unsigned long long* emit_total;

@@ -123,6 +123,41 @@ __device__ __noinline__ float ray_first_block(const Volume& V, F3 origin, F3 dir
   return -1.f;
 }
 
+// True when ray_first_block cannot return a block that the march could use:
+// the ray, with the direction clamped exactly as ray_first_block clamps it,
+// misses both the box of the allocated blocks other than block 0 (`box`,
+// voxel corners) and block 0 itself between nearPlane and farPlane.  Boxes
+// and the t range are widened by two voxels, far beyond the float rounding of
+// either test, so a ray that could reach a block is never skipped.  (A block
+// that ray_first_block finds beyond farPlane makes the march return a miss,
+// which is what skipping the ray gives.)
+__device__ __forceinline__ bool ray_misses_blocks(const Volume& V, const int* box, F3 origin,
+                                                  F3 direction, float nearPlane,
+                                                  float farPlane, float epsilon) {
+  F3 d;
+  d.x = fabsf(direction.x) < epsilon ? copysignf(epsilon, direction.x) : direction.x;
+  d.y = fabsf(direction.y) < epsilon ? copysignf(epsilon, direction.y) : direction.y;
+  d.z = fabsf(direction.z) < epsilon ? copysignf(epsilon, direction.z) : direction.z;
+  // the volume cube is [0, 1]^3 and t runs along d in these units
+  const float vn = 1.f / (float)V.size;
+  const float mg = 2.f * vn;
+  const F3 o = origin / V.dim;
+  const F3 inv = mk3(1.f / d.x, 1.f / d.y, 1.f / d.z);
+  const float t0 = nearPlane / V.dim - mg, t1 = farPlane / V.dim + mg;
+  auto hits = [&](float lx, float ly, float lz, float hx, float hy, float hz) {
+    const float ax = (lx - o.x) * inv.x, bx = (hx - o.x) * inv.x;
+    const float ay = (ly - o.y) * inv.y, by = (hy - o.y) * inv.y;
+    const float az = (lz - o.z) * inv.z, bz = (hz - o.z) * inv.z;
+    const float te = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fmaxf(fminf(az, bz), t0));
+    const float tx = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fminf(fmaxf(az, bz), t1));
+    return te <= tx;
+  };
+  if (hits(-mg, -mg, -mg, 8 * vn + mg, 8 * vn + mg, 8 * vn + mg)) return false;
+  if (box[0] > box[3]) return true;  // no other block
+  return !hits(box[0] * vn - mg, box[1] * vn - mg, box[2] * vn - mg, (box[3] + 8) * vn + mg,
+               (box[4] + 8) * vn + mg, (box[5] + 8) * vn + mg);
+}
+
 // raycast(const Volume<SDF>&, origin, direction, ...),
 // apps/kfusion/src/cpp/kfusion/rendering_impl.hpp:80-140.
 __device__ __noinline__ F4 raycast_volume(const Pool& P, const Volume& V, F3 origin,
@@ -185,9 +220,19 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
                        int* __restrict__ status) {
   const int x = blockIdx.x * TW + (threadIdx.x % TW);
   const int y = blockIdx.y * (128 / TW) + (threadIdx.x / TW);
+  __shared__ int s_slot[8 * 128];
+  // per instance: the box of its allocated blocks and the foreground value a
+  // missed ray reads (the reference interpolates fg at the zero hit point)
+  __shared__ int s_box[MAX_INSTANCES][6];
+  __shared__ float s_fg0[MAX_INSTANCES];
+  for (int o = threadIdx.x; o < ids.n; o += blockDim.x) {
+    const Volume& V = vols[ids.v[o]];
+    for (int j = 0; j < 6; ++j) s_box[o][j] = V.bbox[j];
+    s_fg0[o] = volume_interp(pool, V, mk3(0.f, 0.f, 0.f), 1);
+  }
+  __syncthreads();
   if (x >= a.W || y >= a.H) return;
   const int p = x + y * a.W;
-  __shared__ int s_slot[8 * 128];
   const float INVALID = -2;
   float nearest = 1.0e3f;
   double high_fg = 0.f;
@@ -202,7 +247,10 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
     const float largestep = step * 8;
     const F3 o_dir = normalize(rotate(F.inv_T_w_o, w_dir));
     const float nfar = fmn(nearest, a.farPlane);
-    const float t_min = ray_first_block(V, F.o_origin, o_dir, a.nearPlane, nfar, a.epsilon, status);
+    const float t_min =
+        ray_misses_blocks(V, s_box[o], F.o_origin, o_dir, a.nearPlane, nfar, a.epsilon)
+            ? -1.f
+            : ray_first_block(V, F.o_origin, o_dir, a.nearPlane, nfar, a.epsilon, status);
     const F4 hit = t_min > 0.f
                        ? raycast_volume(pool, V, F.o_origin, o_dir,
                                         t_min * V.dim / (unsigned)V.size, nfar, a.mu, step,
@@ -210,7 +258,8 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
                        : F4{0, 0, 0, 0};
     const float hd = F.label == 0 ? hit.w + 0.05f : hit.w;
     if (hd > nearest) { miss++; continue; }
-    const double fg = volume_interp(pool, V, mk3(hit.x, hit.y, hit.z), 1);
+    const bool at0 = hit.x == 0.f && hit.y == 0.f && hit.z == 0.f;
+    const double fg = at0 ? s_fg0[o] : volume_interp(pool, V, mk3(hit.x, hit.y, hit.z), 1);
     if (fg <= 0.5f) { miss++; continue; }
     if (hd == nearest) {
       if (!(fg > high_fg)) { miss++; continue; }

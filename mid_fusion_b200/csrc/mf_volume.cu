@@ -9,6 +9,7 @@
 // request counts also reproduce the reference's allocation-list quirks (see
 // alloc_commit_kernel).
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstring>
 #include "mf_internal.h"
@@ -124,6 +125,16 @@ alloc_mark_kernel(const float* __restrict__ depth, const float* __restrict__ mas
   }
 }
 
+// Grows the instance's box of allocated blocks (read by the raycast to skip
+// rays that cannot meet a block); block 0 is left out, the raycast tests it on
+// its own.
+__device__ __forceinline__ void note_block(const Volume& V, long long bidx, int cx, int cy,
+                                           int cz) {
+  if (bidx == 0) return;
+  atomicMin(&V.bbox[0], cx); atomicMin(&V.bbox[1], cy); atomicMin(&V.bbox[2], cz);
+  atomicMax(&V.bbox[3], cx); atomicMax(&V.bbox[4], cy); atomicMax(&V.bbox[5], cz);
+}
+
 // Octree::alloc_update + updateLevel, lib/octree.hpp:761-786, :826-863.
 // One thread per (block-table entry, instance).  Reference semantics kept:
 //  - the list's slot 0 is never written (alloc_impl.hpp:175, pre-increment) and
@@ -161,6 +172,7 @@ alloc_commit_kernel(const Volume* __restrict__ vols, const InstFrame* __restrict
       pool.meta[slot] = make_int4(cx, cy, cz, inst);
       pool.active[slot] = 1;
       V.block_tab[bidx] = slot;
+      note_block(V, bidx, cx, cy, cz);
       for (int l = V.block_level - 1; l >= 1; --l)
         V.node_tab[V.node_off[l] + (bidx >> (3 * (V.block_level - l)))] = 1;
     }
@@ -190,10 +202,12 @@ __global__ void alloc_keys_kernel(const Volume* __restrict__ vols, int inst,
         V.block_tab[bidx] = -1;
         return;
       }
-      pool.meta[slot] = make_int4((int)gather3(bidx) << 3, (int)gather3(bidx >> 1) << 3,
-                                  (int)gather3(bidx >> 2) << 3, inst);
+      const int cx = (int)gather3(bidx) << 3, cy = (int)gather3(bidx >> 1) << 3,
+                cz = (int)gather3(bidx >> 2) << 3;
+      pool.meta[slot] = make_int4(cx, cy, cz, inst);
       pool.active[slot] = 1;
       V.block_tab[bidx] = slot;
+      note_block(V, bidx, cx, cy, cz);
     }
   }
 }
@@ -276,9 +290,31 @@ __device__ __forceinline__ void sdf_update(const SdfArgs& a, const float* mask, 
 // slot and corner are loaded during the current one, and the instances'
 // constants come from shared memory, so a block's dependent chain is the pixel
 // fetch and the voxel read-modify-write.
+// Hint: bring the 144 128-byte lines holding the eight voxel fields of pool
+// slot `slot` (7 x 2 KB of 4-byte fields, 4 KB of fg) into L2, one line per
+// thread of the first 144.
+__device__ __forceinline__ void prefetch_block_fields(const Pool& pool, int slot) {
+  const int t = threadIdx.x;
+  if (t >= 144) return;
+  const size_t o = (size_t)slot * 512;
+  const int fi = t >> 4;
+  const void* base = fi == 0   ? (const void*)(pool.tsdf + o)
+                     : fi == 1 ? (const void*)(pool.wt + o)
+                     : fi == 2 ? (const void*)(pool.r + o)
+                     : fi == 3 ? (const void*)(pool.g + o)
+                     : fi == 4 ? (const void*)(pool.b + o)
+                     : fi == 5 ? (const void*)(pool.c + o)
+                     : fi == 6 ? (const void*)(pool.w + o)
+                               : (const void*)(pool.fg + o);
+  const char* p = (const char*)base + (fi < 7 ? (t & 15) : t - 112) * 128;
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // MINB 512-thread CTAs are resident per SM (the register bound) and the grid
-// is MINB CTAs per SM; every variant updates each voxel alike (int_variants).
-template <int MINB>
+// is MINB CTAs per SM; with PF the CTA prefetches the next block's voxel
+// fields into L2 while it works on the current one.  Every variant updates
+// each voxel alike (int_variants).
+template <int MINB, bool PF>
 __global__ void __launch_bounds__(512, MINB)
 integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
                         const InstFrame* __restrict__ frames, SdfArgs args, F4 k,
@@ -300,18 +336,26 @@ integrate_blocks_kernel(Pool pool, const Volume* __restrict__ vols,
     s_vs[i] = vols[i].dim / vols[i].size;
   }
   __syncthreads();
-  // one voxel per thread; the next block's slot and corner are fetched one
-  // block ahead
+  // one voxel per thread; the next block's corner is fetched one block ahead
+  // and (PF) the slot after it two blocks ahead
   const int v = threadIdx.x;
   const int x = v & 7, y = (v >> 3) & 7, z = v >> 6;
   int item = blockIdx.x;
   int next_slot = item < n ? visit[item] : 0;
   int4 next_m = item < n ? pool.meta[next_slot] : make_int4(0, 0, 0, 0);
+  int after_slot = 0;
+  if (PF && item + (int)gridDim.x < n) after_slot = visit[item + gridDim.x];
   for (; item < n; item += gridDim.x) {
     const int slot = next_slot;
     const int4 m = next_m;
     if (item + gridDim.x < n) {
-      next_slot = visit[item + gridDim.x];
+      if (PF) {
+        prefetch_block_fields(pool, after_slot);
+        next_slot = after_slot;
+        if (item + 2 * gridDim.x < n) after_slot = visit[item + 2 * gridDim.x];
+      } else {
+        next_slot = visit[item + gridDim.x];
+      }
       next_m = pool.meta[next_slot];
     }
     const float vs = s_vs[m.w];
@@ -517,6 +561,10 @@ int volume_create(Context* ctx, Instance& in) {
   MF_CUDA(dalloc(&V.n_r, nv)); MF_CUDA(dalloc(&V.n_g, nv)); MF_CUDA(dalloc(&V.n_b, nv));
   MF_CUDA(dalloc(&V.n_c, nv)); MF_CUDA(dalloc(&V.n_fg, nv)); MF_CUDA(dalloc(&V.n_w, nv));
   MF_CUDA(dalloc(&V.last_emit, 1)); MF_CUDA(dalloc(&V.emit_total, 1));
+  MF_CUDA(dalloc(&V.bbox, 6));
+  const int empty_box[6] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN};
+  MF_CUDA(cudaMemcpyAsync(V.bbox, empty_box, sizeof(empty_box), cudaMemcpyHostToDevice,
+                          ctx->stream));
   if (nv) fill_node_values_kernel<<<div_up(nv, 256), 256, 0, ctx->stream>>>(V);
   MF_CUDA(cudaGetLastError());
   return MF_OK;
@@ -525,7 +573,7 @@ int volume_create(Context* ctx, Instance& in) {
 void volume_free(Instance& in) {
   Volume& V = in.vol;
   void* ps[] = {V.block_tab, V.req, V.node_tab, V.n_tsdf, V.n_wt, V.n_r, V.n_g, V.n_b,
-                V.n_c, V.n_fg, V.n_w, V.last_emit, V.emit_total};
+                V.n_c, V.n_fg, V.n_w, V.last_emit, V.emit_total, V.bbox};
   for (void* p : ps) if (p) cudaFree(p);
   std::memset(&V, 0, sizeof(V));
 }
@@ -614,11 +662,13 @@ int profile_integrate(Context* ctx, int reps, double* us, double* bytes) {
 // Launch-shape candidates of integrate_blocks_kernel; entry 0 is the default.
 struct IntVariant {
   int minb;
+  bool prefetch;
   void (*fn)(Pool, const Volume*, const InstFrame*, SdfArgs, F4, const int*, const int*);
 };
 static const IntVariant int_variants[] = {
-    {4, integrate_blocks_kernel<4>}, {3, integrate_blocks_kernel<3>},
-    {2, integrate_blocks_kernel<2>},
+    {4, false, integrate_blocks_kernel<4, false>}, {3, false, integrate_blocks_kernel<3, false>},
+    {2, false, integrate_blocks_kernel<2, false>}, {4, true, integrate_blocks_kernel<4, true>},
+    {3, true, integrate_blocks_kernel<3, true>},   {2, true, integrate_blocks_kernel<2, true>},
 };
 constexpr int N_INT_VARIANTS = (int)(sizeof(int_variants) / sizeof(int_variants[0]));
 static_assert(N_INT_VARIANTS <= MAX_TUNE_VARIANTS, "integration candidate table too long");
@@ -626,7 +676,8 @@ static_assert(N_INT_VARIANTS <= MAX_TUNE_VARIANTS, "integration candidate table 
 int int_variant_count() { return N_INT_VARIANTS; }
 
 void int_variant_describe(int v, char* buf, int cap) {
-  snprintf(buf, cap, "integrate %d x 512-thread CTAs per SM", int_variants[v].minb);
+  snprintf(buf, cap, "integrate %d x 512-thread CTAs per SM%s", int_variants[v].minb,
+           int_variants[v].prefetch ? ", next block's fields prefetched to L2" : "");
 }
 
 int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant) {
