@@ -228,6 +228,9 @@ def run_ours(args, rank, world, local_rank):
 
     stats, tuned = {}, {}
     auto = None if args.no_tune else "auto"
+    if args.shapes:
+        r_v, i_v = (int(v) for v in args.shapes.split(","))
+        auto = {capi.TUNE_RAYCAST: r_v, capi.TUNE_INTEGRATE: i_v}
     sampler = ClockSampler(local_rank)
     # ---- batched, device-resident
     with sampler:
@@ -516,6 +519,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-tune", action="store_true",
                     help="keep the default launch shapes (no mf_autotune before the timed frames)")
+    ap.add_argument("--shapes", default=None,
+                    help="RAYCAST,INTEGRATE: use these launch-shape candidates (a saved "
+                         "mf_autotune choice) instead of tuning")
     ap.add_argument("--workload", default="multi", choices=["multi", "uneven"],
                     help="multi: background + 3 objects (the headline); uneven: + 12 objects")
     ap.add_argument("--profile", action="store_true",

@@ -158,7 +158,7 @@ int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, doubl
  * tracking loop with a fixed memory budget, or a host that has handed the rest
  * of the device memory to other work.  Its scratch (FP64 per-CTA partials, the
  * 32 sums and a CTA ticket) is one static device array of 1 MiB + 512 B, so a
- * level may have at most 4096 x 512 pixels at level 0 and 4096 x 256 above
+ * level may have at most 4096 x 768 pixels at level 0 and 4096 x 256 above
  * (larger levels return MF_E_ARG).  The pose is passed to the kernel by value
  * and the context's poses and sums are not modified.  Same results as
  * mf_track_eval, bit for bit.

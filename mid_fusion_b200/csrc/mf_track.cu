@@ -29,7 +29,16 @@ namespace mf {
 
 constexpr float INVALIDF = -2.f;
 constexpr int GN_THREADS = 256;
-constexpr int GN_PIX_MAX = 2;  // pixels per thread per iteration at level 0 (1 above)
+#ifndef MF_GN_PIX0
+#define MF_GN_PIX0 3
+#endif
+#ifndef MF_GN_MINB
+#define MF_GN_MINB 3
+#endif
+// pixels per thread per iteration at level 0 (1 above): 3 makes the 640x480
+// level one wave of 400 CTAs on 148 SMs x 3 resident (2: 600 CTAs in two
+// waves, 30.9 us per launch against 24.8 us)
+constexpr int GN_PIX_MAX = MF_GN_PIX0;
 __host__ __device__ constexpr int gn_pix(int L) { return L == 0 ? GN_PIX_MAX : 1; }
 
 struct GNState {
@@ -722,7 +731,7 @@ __device__ __forceinline__ double warp_sum_fp64(const float* acc, const int* cnt
 // KIND 0: the camera problem; KIND 1: object problems (one instantiation each
 // keeps the kernel's code small).
 template <int KIND>
-__global__ void __launch_bounds__(GN_THREADS, 3)
+__global__ void __launch_bounds__(GN_THREADS, MF_GN_MINB)
 gn_iter_kernel(GNArgs a, IdList slots, int L) {
   const int s = slots.v[blockIdx.y];
   GNState& S = a.st[s];
@@ -1273,8 +1282,8 @@ int track_download_level(Context* ctx, int L, int which, float* out) {
 //   [0, EVAL_PARTIALS_BYTES)        double partials[EVAL_MAX_TILES][32]
 //   [EVAL_SUMS_OFF, +256)           double sums[32]
 //   [EVAL_TICKET_OFF, +4)           unsigned ticket (zeroed before each launch)
-// EVAL_MAX_TILES bounds the level's pixel count: 4096 CTAs x 512 pixels at
-// level 0 (2 097 152 px, e.g. 1920x1080) and 4096 x 256 above it.
+// EVAL_MAX_TILES bounds the level's pixel count: 4096 CTAs x 768 pixels at
+// level 0 (3 145 728 px, e.g. 2048x1536) and 4096 x 256 above it.
 constexpr int EVAL_MAX_TILES = 4096;
 constexpr size_t EVAL_PARTIALS_BYTES = (size_t)EVAL_MAX_TILES * 32 * sizeof(double);
 constexpr size_t EVAL_SUMS_OFF = EVAL_PARTIALS_BYTES;

@@ -73,8 +73,8 @@ def test_static_scratch_matches_allocating_entry_point():
 
 
 def test_static_scratch_rejects_levels_beyond_its_size():
-    # level 0 of 2048 x 1536 needs 6144 CTA partials; the scratch holds 4096
-    ctx = Context(2048, 1536, pool_blocks=1 << 10)
+    # level 0 of 2560 x 1920 needs 6400 CTA partials; the scratch holds 4096
+    ctx = Context(2560, 1920, pool_blocks=1 << 10)
     sums = np.zeros(32, np.float64)
     rc = ctx.lib.mf_track_eval_static(ctx.h, 0, 0, None, sums.ctypes.data_as(C.c_void_p))
     assert rc == -1  # MF_E_ARG
