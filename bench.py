@@ -44,6 +44,10 @@ UNEVEN = ("640x480 RGB-D, background 512^3@1cm + 12 objects with octrees of 32^3
 UNEVEN_STEPS = 8
 
 
+ROOM = ("320x240 RGB-D, one static room (4 spheres, 3 boxes), one octree 256^3 @ 1 cm, "
+        "30 frames")
+ROOM_FRAMES = 30
+
 ADJ_PAIRS, ADJ_PAIRS_HD, HD = 64, 16, (1280, 720)
 MOTION_FRAMES = 16
 
@@ -55,6 +59,9 @@ def scene_for(rank, n_frames, workload="multi"):
                           bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512)
     if workload == "uneven":
         return make_scene("uneven", W, H, n_frames=n_frames, seed=23 + rank, n_objects=12)
+    if workload == "room":  # the plain single-octree method at 320x240 (fx = fy = 262.5)
+        return make_scene("room", 320, 240, n_frames=n_frames, seed=2 + rank, bg_size=256,
+                          bg_dim=2.56)
     return make_scene("multi", W, H, n_frames=n_frames, seed=11 + rank, n_objects=3,
                       bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512)
 
@@ -147,6 +154,7 @@ def run_ours(args, rank, world, local_rank):
     if do_uneven:
         jobs["uneven"] = n_uneven
         jobs["hd"] = 3
+        jobs["room"] = ROOM_FRAMES
     rendered = render_frames(rank, jobs, args.workers)  # before the first CUDA call
     frames = rendered[main]
     torch.cuda.set_device(local_rank)
@@ -157,8 +165,8 @@ def run_ours(args, rank, world, local_rank):
 
     def make_ctx(batched, scene=None):
         sc = scene or s
-        ctx = Context(W, H, k=sc.k, pool_blocks=args.pool_blocks, batched=batched,
-                      robust="huber")
+        ctx = Context(sc.width, sc.height, k=sc.k, pool_blocks=args.pool_blocks,
+                      batched=batched, robust="huber")
         for inst, T in zip(sc.instances, sc.volume_poses(0)):
             ctx.add_instance(inst.size, inst.dim, T, inst.label)
         ctx.set_camera_pose(sc.cam_poses[0])
@@ -276,6 +284,21 @@ def run_ours(args, rank, world, local_rank):
             c.close()
         del ins
 
+    # ---- the plain single-octree room at 320x240 (batched path, one instance)
+    room = None
+    if do_uneven:
+        sr = scene_for(rank, ROOM_FRAMES, "room")
+        ins = to_device(rendered["room"])
+        crb, trb, prb, strb = run(True, scene=sr, inputs=ins, tune=auto)
+        rerr = float(np.linalg.norm(prb[-1][0][:3, 3] - sr.cam_poses[ROOM_FRAMES - 1][:3, 3]))
+        room = {"workload": ROOM, "instances": 1, "steps": len(trb),
+                "value": round(len(trb) / sum(trb), 2), "unit": "frames/s",
+                "ms_per_step": round(1e3 * sum(trb) / len(trb), 4),
+                "camera_err_vs_gt_m": rerr, "autotune": tuned.get(id(crb)),
+                "status_flags": strb}
+        crb.close()
+        del ins
+
     # ---- adjoint of the camera cost: perturbed (pose, frame) pairs
     adjoint = None
     if do_uneven:
@@ -350,7 +373,7 @@ def run_ours(args, rank, world, local_rank):
     return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
                 status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
                 ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
-                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint, motion=motion,
+                n_inst=len(s.instances), uneven=uneven, adjoint=adjoint, motion=motion, room=room,
                 tune=tuned.get(id(ctx_b)))
 
 
@@ -601,6 +624,7 @@ def main():
                   "ms_per_step": round(1e3 * total_p / args.steps, 4)},
         "batched_over_plain": round(total_p / total_b, 3),
         "uneven12": r.get("uneven"),
+        "room320": r.get("room"),
         "adjoint": r.get("adjoint"),
         "motion": r.get("motion"),
         "autotune": r.get("tune"),

@@ -668,6 +668,11 @@ __global__ void tile_depth_range_kernel(PyrPtrs pyr, int cur, float2* __restrict
 //    of its 8 projected corners (2 px of slack for rounding);
 //  - or, with no such tap, the blended model vertex is 0, the world origin:
 //    rows then need a live point within 0.1 m of it (in object coordinates).
+// Called by a whole warp: lane l projects frustum corner l & 7 and the warp
+// combines the corners with shuffles (every lane gets the answer).  A corner
+// behind camera 1 or a NaN projection makes the answer true, as the first such
+// corner did in a sequential loop; otherwise no NaN reaches the minima and
+// maxima, so their order does not matter.
 __device__ bool object_tile_live(const GNArgs& a, const GNState& S, int L, int tile, int w,
                                  int n) {
   const int ppt = gn_pix(L);
@@ -683,21 +688,34 @@ __device__ bool object_tile_live(const GNArgs& a, const GNState& S, int L, int t
   const float2 zr = a.zr[L * a.max_tiles + tile];
   if (!(zr.x <= zr.y)) return false;  // no pixel of the tile reaches the projection
   const M4 iK = inverse_camera_matrix(a.kL), K0 = camera_matrix(a.k0);
-  float qx0 = INFINITY, qx1 = -INFINITY, qy0 = INFINITY, qy1 = -INFINITY;
-  F3 lo = mk3(INFINITY), hi = mk3(-INFINITY);
-  for (int c = 0; c < 8; ++c) {
-    const float x = (float)((c & 1) ? xb : xa), y = (float)((c & 2) ? yb : ya);
-    const float z = (c & 4) ? zr.y : zr.x;
-    const F3 o2v = xform(S.invTf, z * rotate(iK, mk3(x, y, 1.f)));
-    lo = mk3(fminf(lo.x, o2v.x), fminf(lo.y, o2v.y), fminf(lo.z, o2v.z));
-    hi = mk3(fmaxf(hi.x, o2v.x), fmaxf(hi.y, o2v.y), fmaxf(hi.z, o2v.z));
-    const F3 c1v = xform(S.T_c1_o1, o2v);
-    if (!(c1v.z > 0.f)) return true;  // the frustum reaches behind camera 1: no bound
+  const int c = threadIdx.x & 7;
+  const float x = (float)((c & 1) ? xb : xa), y = (float)((c & 2) ? yb : ya);
+  const float z = (c & 4) ? zr.y : zr.x;
+  const F3 o2v = xform(S.invTf, z * rotate(iK, mk3(x, y, 1.f)));
+  F3 lo = o2v, hi = o2v;
+  const F3 c1v = xform(S.T_c1_o1, o2v);
+  bool unbounded = !(c1v.z > 0.f);  // the frustum reaches behind camera 1: no bound
+  float qx0 = 0.f, qy0 = 0.f;
+  if (!unbounded) {
     const F3 pr = rotate(K0, c1v);
-    const float qx = pr.x / pr.z, qy = pr.y / pr.z;
-    if (isnan(qx) || isnan(qy)) return true;
-    qx0 = fminf(qx0, qx); qx1 = fmaxf(qx1, qx);
-    qy0 = fminf(qy0, qy); qy1 = fmaxf(qy1, qy);
+    qx0 = pr.x / pr.z;
+    qy0 = pr.y / pr.z;
+    unbounded = isnan(qx0) || isnan(qy0);
+  }
+  if (__any_sync(0xffffffffu, unbounded)) return true;
+  float qx1 = qx0, qy1 = qy0;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    qx0 = fminf(qx0, __shfl_xor_sync(0xffffffffu, qx0, o));
+    qx1 = fmaxf(qx1, __shfl_xor_sync(0xffffffffu, qx1, o));
+    qy0 = fminf(qy0, __shfl_xor_sync(0xffffffffu, qy0, o));
+    qy1 = fmaxf(qy1, __shfl_xor_sync(0xffffffffu, qy1, o));
+    lo.x = fminf(lo.x, __shfl_xor_sync(0xffffffffu, lo.x, o));
+    lo.y = fminf(lo.y, __shfl_xor_sync(0xffffffffu, lo.y, o));
+    lo.z = fminf(lo.z, __shfl_xor_sync(0xffffffffu, lo.z, o));
+    hi.x = fmaxf(hi.x, __shfl_xor_sync(0xffffffffu, hi.x, o));
+    hi.y = fmaxf(hi.y, __shfl_xor_sync(0xffffffffu, hi.y, o));
+    hi.z = fmaxf(hi.z, __shfl_xor_sync(0xffffffffu, hi.z, o));
   }
   if (has_box && floorf(qx1) + 3.f >= (float)S.box[0] && floorf(qx0) - 2.f <= (float)S.box[2] &&
       floorf(qy1) + 3.f >= (float)S.box[1] && floorf(qy0) - 2.f <= (float)S.box[3])
@@ -742,7 +760,10 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   bool live = true;
   if (KIND == 1) {
     __shared__ int s_live;
-    if (threadIdx.x == 0) s_live = object_tile_live(a, S, L, blockIdx.x, w, n) ? 1 : 0;
+    if (threadIdx.x < 32) {
+      const bool lv = object_tile_live(a, S, L, blockIdx.x, w, n);
+      if (threadIdx.x == 0) s_live = lv ? 1 : 0;
+    }
     __syncthreads();
     live = s_live != 0;
   }
@@ -1319,7 +1340,10 @@ gn_eval_static_kernel(GNArgs a, int s, int L, int set_pose, M4 Tf, M4 invTf,
   bool live = true;
   if (KIND == 1) {
     __shared__ int s_live;
-    if (threadIdx.x == 0) s_live = object_tile_live(a, S, L, blockIdx.x, w, n) ? 1 : 0;
+    if (threadIdx.x < 32) {
+      const bool lv = object_tile_live(a, S, L, blockIdx.x, w, n);
+      if (threadIdx.x == 0) s_live = lv ? 1 : 0;
+    }
     __syncthreads();
     live = s_live != 0;
   }

@@ -54,7 +54,7 @@ __global__ void prepare_kernel(const float* __restrict__ Twc_p, const float* __r
 
 // ------------------------------------------------------------------ allocation
 // buildVolumeAllocationList, apps/kfusion/src/cpp/kfusion/alloc_impl.hpp:121-191.
-// One thread per (pixel, instance).  A sample in an allocated block marks it
+// One thread per ray-casting (pixel, instance).  A sample in an allocated block marks it
 // active; a sample in an unallocated block adds to that block's request count
 // (runs of equal blocks along a ray are added at once).  The emission order of
 // the single-threaded reference (row, column, step) of the thread's last
@@ -63,14 +63,42 @@ __global__ void __launch_bounds__(256)
 alloc_mark_kernel(const float* __restrict__ depth, const float* __restrict__ masks, int W,
                   int H, const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
                   IdList ids, Pool pool) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int inst = ids.v[blockIdx.y];
   const Volume& V = vols[inst];
   const InstFrame& F = frames[inst];
   unsigned count = 0, last_order = 0, last_idx = 0;
+  // The CTA's pixels that cast a ray (depth != 0, mask >= 0) are packed, in
+  // pixel order, onto its first threads: an object's pixels are sparse, and a
+  // ray of 100 samples on one lane of a warp idled the other 31.  Every result
+  // below is a sum, a maximum or an idempotent flag, so which thread handles
+  // which pixel does not change it.
+  __shared__ int s_pix[256];
+  __shared__ float s_d[256];
+  __shared__ int s_wn[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dq = q < W * H ? depth[q] : 0.f;
+    const bool ray = dq != 0 && !(masks[(size_t)inst * W * H + (q < W * H ? q : 0)] < 0);
+    const unsigned b = __ballot_sync(0xffffffffu, ray);
+    if (lane == 0) s_wn[warp] = __popc(b);
+    __syncthreads();
+    int base = 0;
+    for (int w = 0; w < warp; ++w) base += s_wn[w];
+    if (ray) {
+      const int slot = base + __popc(b & ((1u << lane) - 1u));
+      s_pix[slot] = q;
+      s_d[slot] = dq;
+    }
+    __syncthreads();
+  }
+  int n_rays = 0;
+  for (int w = 0; w < 8; ++w) n_rays += s_wn[w];
+  const bool has_ray = (int)threadIdx.x < n_rays;
+  const int p = has_ray ? s_pix[threadIdx.x] : 0;
+  const float d = has_ray ? s_d[threadIdx.x] : 0.f;
   // no early return: every lane reaches the warp reduction below
-  const float d = p < W * H ? depth[p] : 0.f;
-  if (d != 0 && !(masks[(size_t)inst * W * H + p] < 0)) {
+  if (has_ray) {
     const unsigned x = p % W, y = p / W;
     const float size_f = (float)(unsigned)V.size;
     const F3 w_vertex = xform(F.kPose, mk3((x + 0.5f) * d, (y + 0.5f) * d, d));
@@ -83,9 +111,13 @@ alloc_mark_kernel(const float* __restrict__ depth, const float* __restrict__ mas
     int cur_key = -1, cur_slot = -1;
     uint32_t cur_bidx = 0;
     for (int i = 0; i < F.num_steps; i++) {
-      const F3 s = floor3(pos * F.inv_voxel);
-      if (s.x < size_f && s.y < size_f && s.z < size_f && s.x >= 0 && s.y >= 0 && s.z >= 0) {
-        const I3 v = to_i3(s);
+      // the reference floors pos / voxel and tests 0 <= floor < size; with an
+      // integer size that holds exactly when 0 <= pos / voxel < size, and there
+      // the truncating conversion is the floor (one conversion per axis
+      // instead of a floor and a conversion; NaN fails the test either way)
+      const float fx = pos.x * F.inv_voxel, fy = pos.y * F.inv_voxel, fz = pos.z * F.inv_voxel;
+      if (fx < size_f && fy < size_f && fz < size_f && fx >= 0 && fy >= 0 && fz >= 0) {
+        const I3 v{(int)fx, (int)fy, (int)fz};
         const int key = (v.x >> 3) | ((v.y >> 3) << 10) | ((v.z >> 3) << 20);
         if (key != cur_key) {  // a new block along the ray: look it up once
           cur_key = key;
