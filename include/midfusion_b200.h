@@ -384,6 +384,32 @@ int mf_process_frame(mf_context* ctx, const float* depth, const uint8_t* rgb,
 /* Same with device pointers. */
 int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
                             const uint16_t* d_labels);
+/* Kfusion::tracking with motion segmentation (apps/kfusion/src/cpp/
+ * kfusion.cpp:265-466) and the integration that follows (:606-630), for one
+ * frame from host buffers (labels required).  Host-driven (it synchronises
+ * between stages), not a replayed graph:
+ *  1. the camera is tracked against the whole model;
+ *  2. mf_motion_residuals at the tracked pose gives every object's inlier
+ *     ratio and the moving labels (residual_threshold: the reference's 1.5,
+ *     kernels.h:95; moved_threshold: 0.9, --obj-moved);
+ *  3. with moving objects the camera is tracked again with their pixels
+ *     excluded, only the moving objects are tracked, and the motion residuals
+ *     are computed again;
+ *  4. from this entry point's third frame on, every instance's generalized
+ *     mask is refined (mf_refine_mask_use_motion): the background and static
+ *     objects with the camera's rows (those motion residuals when objects
+ *     move, else the camera's last GN rows), a moving object with the rows of
+ *     its own last GN iteration (the reference recomputes them at the object's
+ *     final pose, kfusion.cpp:446-466; not done here);
+ *  5. every instance is integrated, the composite raycast replaces the model
+ *     maps, and the frame becomes the photometric reference.
+ * The first frame (no reference yet) is integrated and raycast untracked.
+ * moving_labels receives the moving-label bits of step 2 (0 on the first
+ * frame).  The reference's exclusion of never-moving classes
+ * (Object::static_object) is not applied. */
+int mf_process_frame_motion(mf_context* ctx, const float* depth, const uint8_t* rgb,
+                            const uint16_t* labels, float residual_threshold,
+                            float moved_threshold, uint32_t* moving_labels);
 /* Camera pose (16 floats) and every instance's volume pose (16 floats each,
  * instance order); either pointer may be NULL.  Synchronises. */
 int mf_get_poses(mf_context* ctx, float* T_w_c, float* T_w_o);

@@ -42,7 +42,7 @@ EXPORTS = [
     "mf_fuse_semantics", "mf_instance_semantics", "mf_frame_upload_raw", "mf_raw_open",
     "mf_raw_read", "mf_raw_close", "mf_save_poses", "mf_pose_quaternion", "mf_tum_line",
     "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh", "mf_tune_candidates", "mf_tune_describe",
-    "mf_autotune", "mf_tune_get", "mf_tune_set",
+    "mf_autotune", "mf_tune_get", "mf_tune_set", "mf_process_frame_motion",
 ]
 
 TUNE_RAYCAST, TUNE_INTEGRATE, TUNE_MAX_VARIANTS = 0, 1, 16
@@ -221,6 +221,18 @@ class Context:
         self._check(self.lib.mf_profile(self.h, int(reps), _ptr(out, np.float64), len(out)))
         return {"gn_l0_us": out[0], "gn_l0_bytes": out[1], "integrate_us": out[2],
                 "integrate_bytes": out[3], "raycast_us": out[4]}
+
+    def process_frame_motion(self, depth, rgb, labels, residual_threshold=1.5,
+                             moved_threshold=0.9):
+        """One frame through mf_process_frame_motion; returns the moving-label bits."""
+        d = np.ascontiguousarray(depth, np.float32)
+        r = np.ascontiguousarray(rgb, np.uint8)
+        lab = np.ascontiguousarray(labels, np.uint16)
+        bits = C.c_uint32()
+        self._check(self.lib.mf_process_frame_motion(
+            self.h, _ptr(d, np.float32), _ptr(r, np.uint8), _ptr(lab, np.uint16),
+            C.c_float(residual_threshold), C.c_float(moved_threshold), C.byref(bits)))
+        return bits.value
 
     def autotune(self, reps=5):
         """Time every launch-shape candidate on the current frame and keep the

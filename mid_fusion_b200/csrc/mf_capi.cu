@@ -453,6 +453,21 @@ int mf_process_frame(mf_context* ctx, const float* depth, const uint8_t* rgb,
   return process_frame(ctx, labels != nullptr);
 }
 
+int mf_process_frame_motion(mf_context* ctx, const float* depth, const uint8_t* rgb,
+                            const uint16_t* labels, float residual_threshold,
+                            float moved_threshold, uint32_t* moving_labels) {
+  if (check(ctx) || !depth || !rgb || !labels || !moving_labels || !(residual_threshold > 0))
+    return MF_E_ARG;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  MF_CUDA(cudaMemcpyAsync(ctx->d_depth, depth, 4 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_rgb8, rgb, 3 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  rgb_convert_kernel<<<(unsigned)((WH + 255) / 256), 256, 0, ctx->stream>>>(
+      ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, (int)WH);
+  MF_CUDA(cudaGetLastError());
+  MF_CUDA(cudaMemcpyAsync(ctx->d_labels, labels, 2 * WH, cudaMemcpyHostToDevice, ctx->stream));
+  return process_frame_motion(ctx, residual_threshold, moved_threshold, moving_labels);
+}
+
 int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
                             const uint16_t* d_labels) {
   if (check(ctx) || !d_depth || !d_rgb) return MF_E_ARG;

@@ -111,6 +111,10 @@ struct Context {
   bool use_graphs = true;
   TrackState* track = nullptr;
   Tune tune;                        // autotuned launch shapes
+  // mf_process_frame_motion: frames it has processed, and two planes of
+  // result rows (2 x W*H int8 each) for the mask refinement
+  int motion_frames = 0;
+  int8_t* d_motion_rows = nullptr;
   uint8_t* d_render = nullptr;      // W*H*4 render scratch for host destinations
   void* d_render_small = nullptr;   // colour / pointer tables of a render
   size_t render_small_bytes = 0;
@@ -191,6 +195,8 @@ int track_parity(Context* ctx);
 void track_set_parity(Context* ctx, int parity);
 int launch_generalize(Context* ctx);
 int process_frame(Context* ctx, bool labels);
+int process_frame_motion(Context* ctx, float residual_threshold, float moved_threshold,
+                         uint32_t* moving_labels);
 int profile_integrate(Context* ctx, int reps, double* us, double* bytes);
 int profile_gn(Context* ctx, int reps, double* us, double* bytes);
 int profile_raycast(Context* ctx, int reps, double* us);

@@ -28,6 +28,8 @@ static FrameGraphs& graphs(Context* ctx) {
 }
 
 void pipeline_free(Context* ctx) {
+  if (ctx->d_motion_rows) cudaFree(ctx->d_motion_rows);
+  ctx->d_motion_rows = nullptr;
   if (!ctx->graphs) return;
   FrameGraphs& g = *(FrameGraphs*)ctx->graphs;
   for (auto& e : g.exec)
@@ -121,6 +123,99 @@ int process_frame(Context* ctx, bool labels) {
   }
   MF_CUDA(cudaGraphLaunch(g.exec[parity], ctx->stream));
   track_set_parity(ctx, 1 - parity);
+  return MF_OK;
+}
+
+// Kfusion::tracking with motion segmentation (kfusion.cpp:265-466), then the
+// integration of kfusion.cpp:606-630 with motion-refined masks, the raycast
+// and the new reference frame.  Host-driven: which objects move is decided on
+// the host between the stages, as the reference decides it.
+//  1. the camera is tracked against the whole model (no mask, :274-281);
+//  2. motion residuals at the tracked pose (the model raycast with the
+//     objects at their last poses), per-object inlier ratios and the moving
+//     labels (:291-347);
+//  3. with moving objects: the camera is tracked again with their pixels
+//     excluded (:358-393), only the moving objects are tracked (:396-411),
+//     and the motion residuals are computed again at the new pose (:418-441);
+//  4. from the third frame on (frame > 1, :620), every instance's generalized
+//     mask is refined with result rows (Object::refine_mask_use_motion): the
+//     background and the static objects with the camera's rows (the motion
+//     residuals of step 3 when objects move, else the rows of the camera's
+//     last GN iteration, :282, :396-400), a moving object with the rows of
+//     its own last GN iteration (:404-405; the reference recomputes them at
+//     the object's final pose, :446-466, which this library does not);
+//  5. every instance is integrated with its mask, the composite raycast
+//     replaces the model maps and the frame becomes the reference.
+// The first frame (no reference yet) is integrated and raycast untracked.
+int process_frame_motion(Context* ctx, float thr, float moved, uint32_t* moving_out) {
+  if (ctx->inst.empty()) return MF_E_STATE;
+  if (int rc = track_init(ctx)) return rc;
+  const int frame = ctx->motion_frames++;
+  *moving_out = 0;
+  if (!track_has_ref(ctx)) return frame_body(ctx, false, true);
+  const int n = (int)ctx->inst.size();
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  if (!ctx->d_motion_rows) MF_CUDA(cudaMalloc(&ctx->d_motion_rows, 4 * WH));
+  int8_t* cam_rows = ctx->d_motion_rows;
+  int8_t* obj_rows = ctx->d_motion_rows + 2 * WH;
+  if (int rc = launch_generalize(ctx)) return rc;
+  if (int rc = track_preprocess(ctx)) return rc;
+  if (int rc = track_camera(ctx, 0)) return rc;
+  uint32_t moving = 0, again = 0;
+  float ratio[MAX_INSTANCES];
+  if (n > 1)
+    if (int rc = motion_residuals(ctx, thr, moved, ratio, &moving)) return rc;
+  IdList mov;
+  mov.n = 0;
+  bool is_moving[MAX_INSTANCES] = {};
+  for (int i = 1; i < n; ++i) {
+    const int l = ctx->inst[i].label;
+    if (l >= 0 && l < 32 && ((moving >> l) & 1u)) {
+      mov.v[mov.n++] = i;
+      is_moving[i] = true;
+    }
+  }
+  if (mov.n) {
+    if (int rc = track_camera(ctx, moving, 1)) return rc;
+    if (int rc = track_objects(ctx, mov)) return rc;
+    if (int rc = motion_residuals(ctx, thr, moved, ratio, &again)) return rc;
+  }
+  if (frame > 1) {
+    const int8_t* rows0 = nullptr;  // the last motion residuals
+    if (!mov.n) {
+      if (int rc = track_results(ctx, 0, cam_rows, nullptr, nullptr)) return rc;
+      rows0 = cam_rows;
+    }
+    for (int i = 0; i < n; ++i) {
+      const int8_t* rows = rows0;
+      if (is_moving[i]) {
+        if (int rc = track_results(ctx, i, obj_rows, nullptr, nullptr)) return rc;
+        rows = obj_rows;
+      }
+      if (int rc = refine_mask_use_motion(ctx, i, rows, ctx->cfg.use_icp, ctx->cfg.use_rgb))
+        return rc;
+    }
+  }
+  IdList all;
+  all.n = n;
+  for (int i = 0; i < n; ++i) all.v[i] = i;
+  if (ctx->cfg.batched) {
+    if (int rc = stage_prepare(ctx, all)) return rc;
+    if (int rc = stage_alloc(ctx, all)) return rc;
+    if (int rc = stage_integrate(ctx, all)) return rc;
+  } else {
+    for (int i = 0; i < n; ++i) {
+      IdList one;
+      one.n = 1;
+      one.v[0] = i;
+      if (int rc = stage_prepare(ctx, one)) return rc;
+      if (int rc = stage_alloc(ctx, one)) return rc;
+      if (int rc = stage_integrate(ctx, one)) return rc;
+    }
+  }
+  if (int rc = stage_raycast(ctx, all, ctx->ray_epsilon)) return rc;
+  if (int rc = track_set_ref(ctx)) return rc;
+  *moving_out = moving;
   return MF_OK;
 }
 
