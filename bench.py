@@ -327,6 +327,14 @@ def run_ours(args, rank, world, local_rank):
     motion = None
     if do_uneven:
         motion = run_motion(ctx_b, frames, [p[0] for p in poses_b], MOTION_FRAMES, dev, torch)
+        try:  # the whole per-frame flow with motion segmentation in one call
+            ctx_m = make_ctx(True)
+            for stage, v in tune_b.items():
+                ctx_m.tune_set(stage, v)
+            motion["process_frame_motion"] = run_motion_frames(ctx_m, frames, args, dev, torch)
+            ctx_m.close()
+        except Exception as e:  # an optional measurement never breaks the line
+            motion["process_frame_motion"] = {"error": str(e)[:200]}
 
     # ---- e2e through the C ABI from pinned host buffers
     import ctypes
@@ -417,6 +425,31 @@ def run_motion(ctx, frames, poses, n, dev, torch):
             "what": "mf_motion_residuals (live raycast, residual codes, inlier ratios, moving "
                     "bits to the host) + mf_track_results of every object + "
                     "mf_refine_mask_use_motion of every instance",
+            "status_flags": ctx.status()}
+
+
+def run_motion_frames(ctx, frames, args, dev, torch):
+    """Frames through mf_process_frame_motion from host buffers (camera track,
+    motion residuals, masked re-track, moving objects only, mask refinement,
+    integration, raycast); device time per frame with CUDA events after
+    1 + warmup untimed frames, the call's own synchronisations included."""
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    times, moving = [], []
+    for f in range(len(frames)):
+        d, rgb, lab = frames[f]
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        bits = ctx.process_frame_motion(d, rgb, lab, 1.5, 0.9)
+        e1.record(stream)
+        e1.synchronize()
+        if f >= 1 + args.warmup:
+            times.append(e0.elapsed_time(e1))
+            moving.append(bin(bits).count("1"))
+    ms = float(np.mean(times))
+    return {"frames": len(times), "ms_per_frame": round(ms, 4),
+            "frames_per_s": round(1e3 / ms, 2),
+            "moving_objects_mean": round(float(np.mean(moving)), 2),
             "status_flags": ctx.status()}
 
 
