@@ -486,12 +486,16 @@ integrate_count_kernel(Pool pool, const Volume* __restrict__ vols,
 // over every internal node of the selected instances.  The reference takes the
 // node's voxel from unpack_morton(code) with the level bits still in the code,
 // and offsets child i by dir * rotate(Tcw, (h, h, h)) element-wise; both kept.
+// One thread per (node, child): the eight children update disjoint values, so
+// the reference's loop over them runs as eight threads.
 __global__ void __launch_bounds__(128)
 integrate_nodes_kernel(const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
                        SdfArgs args, F4 k, IdList ids) {
   const int inst = ids.v[blockIdx.y];
   const Volume& V = vols[inst];
-  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long e = t >> 3;
+  const int i = (int)(t & 7);
   if (e >= V.n_nodes || !V.node_tab[e]) return;
   int l = 1;
   while (l + 1 < V.block_level && e >= V.node_off[l + 1]) ++l;
@@ -509,18 +513,16 @@ integrate_nodes_kernel(const Volume* __restrict__ vols, const InstFrame* __restr
   const F3 basepix = xform(K, base_cam);
   const float* mask = args.masks + (size_t)inst * args.W * args.H;
   const float wlim = args.W - 1.5f, hlim = args.H - 1.5f;
-  for (int i = 0; i < 8; ++i) {
-    const F3 dir = mk3((float)((i & 1) > 0), (float)((i & 2) > 0), (float)((i & 4) > 0));
-    const F3 vox_cam = base_cam + dir * delta;
-    const F3 pix_hom = basepix + dir * delta_c;
-    if (vox_cam.z < 0.0001f) continue;
-    const float inv = 1.f / pix_hom.z;
-    const float pxf = pix_hom.x * inv + 0.5f, pyf = pix_hom.y * inv + 0.5f;
-    if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) continue;
-    const size_t o = (size_t)e * 8 + i;
-    sdf_update(args, mask, vox_cam, pxf, pyf, V.n_tsdf[o], V.n_wt[o], &V.n_r[o], &V.n_g[o],
-               &V.n_b[o], V.n_c[o], V.n_fg[o], V.n_w[o]);
-  }
+  const F3 dir = mk3((float)((i & 1) > 0), (float)((i & 2) > 0), (float)((i & 4) > 0));
+  const F3 vox_cam = base_cam + dir * delta;
+  const F3 pix_hom = basepix + dir * delta_c;
+  if (vox_cam.z < 0.0001f) return;
+  const float inv = 1.f / pix_hom.z;
+  const float pxf = pix_hom.x * inv + 0.5f, pyf = pix_hom.y * inv + 0.5f;
+  if (pxf < 0.5f || pxf > wlim || pyf < 0.5f || pyf > hlim) return;
+  const size_t o = (size_t)e * 8 + i;
+  sdf_update(args, mask, vox_cam, pxf, pyf, V.n_tsdf[o], V.n_wt[o], &V.n_r[o], &V.n_g[o],
+             &V.n_b[o], V.n_c[o], V.n_fg[o], V.n_w[o]);
 }
 
 __global__ void interp_points_kernel(Pool pool, const Volume* __restrict__ vols, int inst,
@@ -749,7 +751,7 @@ int stage_integrate(Context* ctx, const IdList& ids) {
   SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
   const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
   if (max_nodes > 0) {
-    integrate_nodes_kernel<<<dim3(div_up(max_nodes, 128), ids.n), 128, 0, ctx->stream>>>(
+    integrate_nodes_kernel<<<dim3(div_up(max_nodes * 8, 128), ids.n), 128, 0, ctx->stream>>>(
         ctx->d_vols, ctx->d_frames, a, k, ids);
     MF_CUDA(cudaGetLastError());
   }
