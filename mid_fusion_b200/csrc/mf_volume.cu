@@ -54,11 +54,11 @@ __global__ void prepare_kernel(const float* __restrict__ Twc_p, const float* __r
 
 // ------------------------------------------------------------------ allocation
 // buildVolumeAllocationList, apps/kfusion/src/cpp/kfusion/alloc_impl.hpp:121-191.
-// One thread per ray-casting (pixel, instance).  A sample in an allocated block marks it
-// active; a sample in an unallocated block adds to that block's request count
-// (runs of equal blocks along a ray are added at once).  The emission order of
-// the single-threaded reference (row, column, step) of the thread's last
-// emitted sample is folded into last_emit with atomicMax.
+// One thread per ray-casting (pixel, instance).  A sample in an allocated
+// block marks it active; a sample in an unallocated block adds to that block's
+// request count (runs of equal blocks along a ray are added at once).  The
+// emission order of the single-threaded reference (row, column, step) of the
+// thread's last emitted sample is folded into last_emit with atomicMax.
 __global__ void __launch_bounds__(256)
 alloc_mark_kernel(const float* __restrict__ depth, const float* __restrict__ masks, int W,
                   int H, const Volume* __restrict__ vols, const InstFrame* __restrict__ frames,
@@ -315,13 +315,6 @@ __device__ __forceinline__ void sdf_update(const SdfArgs& a, const float* mask, 
   }
 }
 
-// projective_functor::update_block, lib/functors/projective_functor.hpp:73-111.
-// Persistent CTAs of 512 threads (four per SM, 32 registers), one visited
-// block at a time, one voxel per thread: every field plane is read and written
-// coalesced, and only for voxels that pass the update test.  The next block's
-// slot and corner are loaded during the current one, and the instances'
-// constants come from shared memory, so a block's dependent chain is the pixel
-// fetch and the voxel read-modify-write.
 // Hint: bring the 144 128-byte lines holding the eight voxel fields of pool
 // slot `slot` (7 x 2 KB of 4-byte fields, 4 KB of fg) into L2, one line per
 // thread of the first 144.
@@ -342,6 +335,13 @@ __device__ __forceinline__ void prefetch_block_fields(const Pool& pool, int slot
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
+// projective_functor::update_block, lib/functors/projective_functor.hpp:73-111.
+// Persistent CTAs of 512 threads, one visited block at a time, one voxel per
+// thread: every field plane is read and written coalesced, and only for voxels
+// that pass the update test.  The next block's slot and corner are loaded
+// during the current one, and the instances' constants come from shared
+// memory, so a block's dependent chain is the pixel fetch and the voxel
+// read-modify-write.
 // MINB 512-thread CTAs are resident per SM (the register bound) and the grid
 // is MINB CTAs per SM; with PF the CTA prefetches the next block's voxel
 // fields into L2 while it works on the current one.  Every variant updates
