@@ -162,24 +162,46 @@ __global__ void half_sample_kernel(const float* __restrict__ in0, float* __restr
 }
 
 // depth2vertexKernel, preprocessing.cpp:52-71.
-__global__ void depth2vertex_kernel(const float* __restrict__ depth, F3* __restrict__ vertex,
-                                    int w, int h, M4 invK) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= w * h) return;
+__device__ __forceinline__ void depth2vertex_px(const float* __restrict__ depth,
+                                                F3* __restrict__ vertex, int w, int p,
+                                                const M4& invK) {
   const int x = p % w, y = p / w;
   const float d = depth[p];
   vertex[p] = d > 0 ? d * rotate(invK, mk3((float)x, (float)y, 1.f)) : mk3(0.f);
 }
 
+// The planes of every level of the live pyramid; the level kernels below take
+// the level from blockIdx.y, so one launch covers all levels.
+struct LevelMaps {
+  const float* D[MAX_PYR];
+  F3* V[MAX_PYR];
+  const float* I[MAX_PYR];
+  F3* N[MAX_PYR];
+  float* GX[MAX_PYR];
+  float* GY[MAX_PYR];
+  F3* COV[MAX_PYR];
+  uint8_t* MASK[MAX_PYR];
+  int w[MAX_PYR], h[MAX_PYR];
+  M4 invK[MAX_PYR];
+  float focal[MAX_PYR];
+};
+
+__global__ void depth2vertex_levels_kernel(LevelMaps m) {
+  const int l = blockIdx.y;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= m.w[l] * m.h[l]) return;
+  depth2vertex_px(m.D[l], m.V[l], m.w[l], p, m.invK[l]);
+}
+
 // vertex2normalKernel<SDF, false> (preprocessing.h:39-81), gradientsKernel
 // (preprocessing.cpp:235-246, borders untouched) and calc_icp_cov
 // (tracking.cpp:845-871, sigma_xy = sigma_disp = 1, baseline 0.075).
-__global__ void normal_grad_cov_kernel(const F3* __restrict__ V, const float* __restrict__ I,
-                                       const float* __restrict__ D, F3* __restrict__ N,
-                                       float* __restrict__ GX, float* __restrict__ GY,
-                                       F3* __restrict__ COV, int w, int h, float focal) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= w * h) return;
+__device__ __forceinline__ void normal_grad_cov_px(const F3* __restrict__ V,
+                                                   const float* __restrict__ I,
+                                                   const float* __restrict__ D,
+                                                   F3* __restrict__ N, float* __restrict__ GX,
+                                                   float* __restrict__ GY, F3* __restrict__ COV,
+                                                   int w, int h, float focal, int p) {
   const int x = p % w, y = p / w;
   const F3 left = V[imx(x - 1, 0) + w * y], right = V[imn(x + 1, w - 1) + w * y];
   const F3 down = V[x + w * imx(y - 1, 0)], up = V[x + w * imn(y + 1, h - 1)];
@@ -199,6 +221,17 @@ __global__ void normal_grad_cov_kernel(const F3* __restrict__ V, const float* __
   c.z = (d * d * 1.0f) / (focal * 0.075f);
   c.x = c.x * c.x; c.y = c.y * c.y; c.z = c.z * c.z;
   COV[p] = c;
+}
+
+// normal_grad_cov_px on every level; it also clears the level's ICP outlier
+// mask (no pixel is masked until the camera track sets one).
+__global__ void normal_grad_cov_levels_kernel(LevelMaps m) {
+  const int l = blockIdx.y;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= m.w[l] * m.h[l]) return;
+  normal_grad_cov_px(m.V[l], m.I[l], m.D[l], m.N[l], m.GX[l], m.GY[l], m.COV[l], m.w[l],
+                     m.h[l], m.focal[l], p);
+  m.MASK[l][p] = 0;
 }
 
 struct SlotPtrs {
@@ -258,12 +291,20 @@ __global__ void half_sample_slots_kernel(SlotPtrs sp, int iw, int ih, float e_d)
   out[p] = t / sum;
 }
 
-__global__ void depth2vertex_slots_kernel(SlotPtrs sp, int w, int h, M4 invK) {
+// The rendered reference depth and vertex planes of every slot at every level.
+struct SlotLevels {
+  const float* D[MAX_PYR][MAX_INSTANCES];
+  F3* V[MAX_PYR][MAX_INSTANCES];
+  int w[MAX_PYR], h[MAX_PYR];
+  M4 invK[MAX_PYR];
+};
+
+// depth2vertex of every slot (blockIdx.y) at every level (blockIdx.z).
+__global__ void depth2vertex_slots_kernel(SlotLevels sl) {
+  const int l = blockIdx.z;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= w * h) return;
-  const int x = p % w, y = p / w;
-  const float d = sp.D[blockIdx.y][p];
-  sp.V[blockIdx.y][p] = d > 0 ? d * rotate(invK, mk3((float)x, (float)y, 1.f)) : mk3(0.f);
+  if (p >= sl.w[l] * sl.h[l]) return;
+  depth2vertex_px(sl.D[l][blockIdx.y], sl.V[l][blockIdx.y], sl.w[l], p, sl.invK[l]);
 }
 
 // ------------------------------------------------------------------ GN setup
@@ -316,15 +357,6 @@ __global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __r
   S.Tf = T0;
   S.invTf = inverse(T0);
   S.evalTf = T0;
-}
-
-__global__ void level_start_kernel(GNState* st, IdList slots) {
-  const int t = threadIdx.x;
-  if (t >= slots.n) return;
-  GNState& S = st[slots.v[t]];
-  S.prev_err = INFINITY;
-  S.done = 0;
-  S.ticket = 0;
 }
 
 __global__ void finalize_camera_kernel(const GNState* st, float* __restrict__ Twc) {
@@ -411,6 +443,10 @@ struct GNArgs {
   int robust;
   int use_icp, use_rgb;
   int device_step;      // 1: the last block runs gn_step; 0: only the sums
+  int first_iter;       // 1: the first iteration of a level in the batched loop:
+                        // a stopped problem runs again and the step starts
+                        // from prev_err = infinity (trackLiveFrame's per-level
+                        // reset, tracking.cpp:247-249, 624-627)
 };
 
 struct Row { int result; float e; float J[6]; };
@@ -753,7 +789,7 @@ __global__ void __launch_bounds__(GN_THREADS, MF_GN_MINB)
 gn_iter_kernel(GNArgs a, IdList slots, int L) {
   const int s = slots.v[blockIdx.y];
   GNState& S = a.st[s];
-  if (S.done) return;
+  if (S.done && !a.first_iter) return;
   const int w = a.pyr.w[L], h = a.pyr.h[L];
   const int n = w * h;
   // object problems: a tile that cannot hold a valid row skips its pixels
@@ -847,7 +883,10 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   __syncthreads();
   if (threadIdx.x == 0) {
     S.ticket = 0;
-    if (a.device_step) gn_step_dev(S, tot, L);
+    if (a.device_step) {
+      if (a.first_iter) S.prev_err = INFINITY;
+      gn_step_dev(S, tot, L);
+    }
   }
 }
 
@@ -939,17 +978,28 @@ int track_preprocess(Context* ctx) {
         P.D[l - 1], P.D[l], P.I[T.cur][l - 1], P.I[T.cur][l], P.w[l - 1], P.h[l - 1], e_d);
     MF_CUDA(cudaGetLastError());
   }
+  // vertex maps of every level, then normals, gradients, covariances and the
+  // cleared outlier masks of every level: two launches
+  LevelMaps m{};
   for (int l = 0; l < T.levels; ++l) {
     const F4 kl = kdiv(ctx->cfg, l);
-    const int n = P.w[l] * P.h[l];
-    depth2vertex_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(P.D[l], P.V[T.cur][l], P.w[l],
-                                                                  P.h[l], inverse_camera_matrix(kl));
-    normal_grad_cov_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(
-        P.V[T.cur][l], P.I[T.cur][l], P.D[l], P.N[l], P.GX[l], P.GY[l], P.COV[l], P.w[l], P.h[l],
-        kl.x);
-    MF_CUDA(cudaGetLastError());
-    MF_CUDA(cudaMemsetAsync(P.MASK[l], 0, n, ctx->stream));
+    m.D[l] = P.D[l];
+    m.V[l] = P.V[T.cur][l];
+    m.I[l] = P.I[T.cur][l];
+    m.N[l] = P.N[l];
+    m.GX[l] = P.GX[l];
+    m.GY[l] = P.GY[l];
+    m.COV[l] = P.COV[l];
+    m.MASK[l] = P.MASK[l];
+    m.w[l] = P.w[l];
+    m.h[l] = P.h[l];
+    m.invK[l] = inverse_camera_matrix(kl);
+    m.focal[l] = kl.x;
   }
+  const dim3 grid(div_up((long long)P.w[0] * P.h[0], 256), T.levels);
+  depth2vertex_levels_kernel<<<grid, 256, 0, ctx->stream>>>(m);
+  normal_grad_cov_levels_kernel<<<grid, 256, 0, ctx->stream>>>(m);
+  MF_CUDA(cudaGetLastError());
   return MF_OK;
 }
 
@@ -966,8 +1016,16 @@ int track_set_ref(Context* ctx) {
 // The camera's ICP outlier mask, trackLiveFrame(..., mask): cv::resize to each
 // level: 2x (INTER_AREA) keeps any nonzero of a 2x2 cell, 4x (INTER_LINEAR)
 // samples taps 4x+1 and 4x+2 per axis.
-__global__ void mask_pyramid_kernel(const uint8_t* __restrict__ m0, uint8_t* __restrict__ out,
-                                    int W, int w, int h, int l) {
+struct MaskLevels {
+  uint8_t* out[MAX_PYR];
+  int w[MAX_PYR], h[MAX_PYR];
+};
+
+// One launch for every level (level = blockIdx.y); each level reads m0 only.
+__global__ void mask_pyramid_kernel(const uint8_t* __restrict__ m0, MaskLevels ml, int W) {
+  const int l = blockIdx.y;
+  const int w = ml.w[l], h = ml.h[l];
+  uint8_t* __restrict__ out = ml.out[l];
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= w * h) return;
   const int x = p % w, y = p / w;
@@ -996,12 +1054,15 @@ __global__ void label_mask_kernel(const int* __restrict__ label, uint32_t moving
 int track_set_mask(Context* ctx, const uint8_t* d_mask0) {
   TrackState& T = *ctx->track;
   PyrPtrs& P = T.pyr;
+  MaskLevels ml{};
   for (int l = 0; l < T.levels; ++l) {
-    const int n = P.w[l] * P.h[l];
-    mask_pyramid_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(d_mask0, P.MASK[l], ctx->W,
-                                                                  P.w[l], P.h[l], l);
-    MF_CUDA(cudaGetLastError());
+    ml.out[l] = P.MASK[l];
+    ml.w[l] = P.w[l];
+    ml.h[l] = P.h[l];
   }
+  mask_pyramid_kernel<<<dim3(div_up((long long)P.w[0] * P.h[0], 256), T.levels), 256, 0,
+                        ctx->stream>>>(d_mask0, ml, ctx->W);
+  MF_CUDA(cudaGetLastError());
   return MF_OK;
 }
 
@@ -1014,23 +1075,31 @@ static int render_reference(Context* ctx, const IdList& slots) {
   render_depth_kernel<<<dim3(div_up(WH, 256), slots.n), 256, 0, ctx->stream>>>(
       ctx->d_vertex, ctx->d_label, T.d_state, slots, sp, ctx->W, WH);
   MF_CUDA(cudaGetLastError());
+  // the depth pyramid level by level, then the vertex maps of every level in
+  // one launch
+  SlotLevels sl{};
   for (int l = 0; l < T.levels; ++l) {
     SlotPtrs q{};
     for (int i = 0; i < slots.n; ++i) {
       q.D[i] = T.rD[slots.v[i]][l];
       q.V[i] = T.rV[slots.v[i]][l];
       q.Din[i] = l > 0 ? T.rD[slots.v[i]][l - 1] : nullptr;
+      sl.D[l][i] = q.D[i];
+      sl.V[l][i] = q.V[i];
     }
+    sl.w[l] = P.w[l];
+    sl.h[l] = P.h[l];
+    sl.invK[l] = inverse_camera_matrix(kdiv(ctx->cfg, l));
     const int n = P.w[l] * P.h[l];
     if (l > 0) {
       half_sample_slots_kernel<<<dim3(div_up(n, 256), slots.n), 256, 0, ctx->stream>>>(
           q, P.w[l - 1], P.h[l - 1], 0.1f * 3);
       MF_CUDA(cudaGetLastError());
     }
-    depth2vertex_slots_kernel<<<dim3(div_up(n, 256), slots.n), 256, 0, ctx->stream>>>(
-        q, P.w[l], P.h[l], inverse_camera_matrix(kdiv(ctx->cfg, l)));
-    MF_CUDA(cudaGetLastError());
   }
+  depth2vertex_slots_kernel<<<dim3(div_up(WH, 256), slots.n, T.levels), 256, 0,
+                              ctx->stream>>>(sl);
+  MF_CUDA(cudaGetLastError());
   return MF_OK;
 }
 
@@ -1081,10 +1150,10 @@ static int tile_depth_range(Context* ctx) {
 static int gn_device(Context* ctx, const IdList& slots, int kind) {
   TrackState& T = *ctx->track;
   for (int L = T.levels - 1; L >= 0; --L) {
-    level_start_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, slots);
-    const GNArgs a = make_args(ctx, L, 1);
+    GNArgs a = make_args(ctx, L, 1);
     const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_THREADS * gn_pix(L));
     for (int it = 0; it < ctx->cfg.gn_iterations[L]; ++it) {
+      a.first_iter = it == 0;  // the level's reset happens in its first iteration
       if (kind == 0) gn_iter_kernel<0><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
       else gn_iter_kernel<1><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
     }
