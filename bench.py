@@ -198,7 +198,10 @@ def run_ours(args, rank, world, local_rank):
             # two warm-up frames after the tuner re-capture both frame graphs
             # (one per reference-pyramid parity) with the chosen shapes
             if tune == "auto" and f == args.warmup - 1:
-                tuned[id(ctx)] = ctx.autotune(reps=5)
+                try:
+                    tuned[id(ctx)] = ctx.autotune(reps=5)
+                except Exception as e:  # keep the default shapes; the line still prints
+                    tuned[id(ctx)] = {"error": str(e)[:200]}
             flush.fill_(f & 0xff)
             torch.cuda.synchronize(dev)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
