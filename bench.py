@@ -50,6 +50,8 @@ ROOM_FRAMES = 30
 
 ADJ_PAIRS, ADJ_PAIRS_HD, HD = 64, 16, (1280, 720)
 MOTION_FRAMES = 16
+CPU_SAMPLE_FRAMES = 8     # timed CPU-baseline frames (about 10 s of host work)
+POSE_CHECK_FRAMES = 3     # frames re-tracked on the CPU from the device's previous state
 
 
 def scene_for(rank, n_frames, workload="multi"):
@@ -370,20 +372,40 @@ def run_ours(args, rank, world, local_rank):
     total_e = sum(t_e)
     h2d = W * H * (4 + 3 + 2)
     d2h = 64 * (1 + len(s.instances))
-    # ---- CPU baseline: rank 0 at N=1, a bounded sample of the same sequence
-    cpu = None
+    # ---- CPU baseline: rank 0 at N=1, a bounded sample of the same sequence,
+    # and the per-frame pose check against the reference and the FP64 oracle
+    cpu, pose_check = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import cpu_baseline as CB
-        n_cpu = min(3, n_frames - 1)
-        sec, kind = CB.time_frames(s, frames, 1, n_cpu, use_reference=True)
+        first = 1 + args.warmup                 # the GPU arm's first timed frame
+        n_cpu = min(CPU_SAMPLE_FRAMES, n_frames - first)
+        sec, kind = CB.time_frames(s, frames, first, n_cpu, use_reference=True)
         cpu = {"value": round(1.0 / sec, 4), "unit": "frames/s", "cores": CB.threads(),
                "kind": kind,
-               "sample": f"frames 1..{n_cpu} of the same sequence (frame 0 untimed), full "
-                         f"640x480 frames, OpenMP on every host thread"}
+               "sample": f"frames {first}..{first + n_cpu - 1} of the same sequence (the GPU "
+                         f"arm's first timed frames) after {first} untimed frames, full "
+                         f"640x480 frames, OpenMP on every host thread, the reference's "
+                         f"Release flags (-g -O1)"}
+        # device poses and model maps frame by frame (untimed), then each frame
+        # re-tracked on the CPU from the device's previous pose and maps
+        ctx_c = make_ctx(True)
+        cams, objs, maps = [], [], []
+        for f in range(POSE_CHECK_FRAMES + 1):
+            rc = ctx_c.lib.mf_process_frame_device(ctx_c.h, ctx_ptr(d_depth[f]),
+                                                   ctx_ptr(d_rgb[f]), ctx_ptr(d_lab[f]))
+            if rc != 0:
+                raise RuntimeError(f"mf_process_frame_device failed: {rc}")
+            c, o = ctx_poses(ctx_c)
+            cams.append(c)
+            objs.append(o)
+            maps.append(ctx_c.download_raycast())
+        ctx_c.close()
+        pose_check = CB.pose_check(s, frames, cams, objs, maps, POSE_CHECK_FRAMES)
     return dict(total_b=total_b, total_p=total_p, total_e=total_e, dpos=dpos, gt_err=gt_err,
                 status=(st_b, st_p), clocks=sampler.summary(), h2d=h2d, d2h=d2h,
                 ms_b=1e3 * total_b / max(len(t_b), 1), stats=stats, prof=prof, cpu=cpu,
+                pose_check=pose_check,
                 n_inst=len(s.instances), uneven=uneven, adjoint=adjoint, motion=motion, room=room,
                 tune=tuned.get(id(ctx_b)))
 
@@ -498,34 +520,47 @@ def run_adjoint(ctx, scene, frames, poses, pairs, dev, torch):
 
 def run_reference(args):
     """The reference's CPU implementation of the path on the host cores: one step
-    = one frame of the same workload (oracle/cpu_baseline.py: the reference's own
-    allocation / integration / raycast code built with OpenMP, the tracking
-    restated where the reference needs TooN)."""
+    = one frame of the same workload, every stage the reference's own code
+    (oracle/cpu_baseline.py: tracking.cpp, preprocessing.cpp, object.cpp,
+    rendering.cpp and lib/ compiled unmodified with OpenMP), built with the
+    reference's Release flags (-g -O1); the same frames with an -O3 build are
+    reported beside it."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cpu_baseline as CB
     n_frames = 1 + args.warmup + args.steps
     frames = render_frames(0, {"multi": n_frames}, args.workers)["multi"]
     s = scene_for(0, n_frames)
-    p = CB.CpuPipeline(s, use_reference=True)
-    t = []
-    for f in range(n_frames):
-        d, rgb, lab = frames[f]
-        t0 = time.perf_counter()
-        p.step(d, rgb, lab)
-        if f >= 1 + args.warmup:
-            t.append(time.perf_counter() - t0)
-    total = sum(t)
-    value = len(t) / total
+
+    def timed(build):
+        p = CB.CpuPipeline(s, use_reference=True, build=build)
+        t = []
+        for f in range(n_frames):
+            d, rgb, lab = frames[f]
+            t0 = time.perf_counter()
+            p.step(d, rgb, lab)
+            if f >= 1 + args.warmup:
+                t.append(time.perf_counter() - t0)
+        return sum(t), len(t), p.kind
+
+    total, n, kind = timed("stock")
+    value = n / total
+    o3 = None
+    if CB.reference_available("o3"):
+        t3, n3, _ = timed("o3")
+        o3 = {"value": round(n3 / t3, 4), "unit": "frames/s", "ms_per_step": round(1e3 * t3 / n3, 3),
+              "flags": "-O3 -march=x86-64-v3 -fopenmp"}
     return {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "frames/s",
         "n_gpus": args.gpus, "device": "host cores only", "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(1e3 * total / len(t), 3), "higher_is_better": True,
+        "ms_per_step": round(1e3 * total / n, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4},
         "cpu_baseline": {"value": round(value, 4), "unit": "frames/s", "cores": CB.threads(),
-                         "kind": p.kind,
-                         "sample": f"{len(t)} frames after {1 + args.warmup} untimed, full "
-                                   "640x480 frames, OpenMP on every host thread"},
+                         "kind": kind,
+                         "sample": f"{n} frames after {1 + args.warmup} untimed, full "
+                                   "640x480 frames, OpenMP on every host thread, the "
+                                   "reference's Release flags (-g -O1 -march=x86-64-v3)"},
+        "o3": o3,
         "e2e": {"value": round(value, 4), "unit": "frames/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -671,6 +706,7 @@ def main():
         "roofline": roofline,
         "rooflines_other": others,
         "cpu_baseline": r.get("cpu"),
+        "pose_check": r.get("pose_check"),
         "gpu_launches": launches,
         "clocks": r["clocks"],
         "status_flags": r["status"],

@@ -151,7 +151,9 @@ int mf_track_objects(mf_context* ctx, const int* ids, int n);
 int mf_track_info(mf_context* ctx, int slot, int* iterations, double* sums, double* pose);
 /* One evaluation of the normal equations (the 32 reduceKernel sums,
  * tracking.cpp:1191-1352) of a problem at `level` and at `pose` (NULL: its
- * current pose), without a GN step. */
+ * current pose), without a GN step.  MF_E_STATE when the slot holds no
+ * tracking problem yet (mf_track_camera sets up slot 0, mf_track_objects the
+ * object slots). */
 int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, double* sums);
 /* No counterpart in the reference.  mf_track_eval without any device memory
  * allocation, for callers that must not allocate while they run: a real-time
@@ -163,7 +165,11 @@ int mf_track_eval(mf_context* ctx, int slot, int level, const float* pose, doubl
  * and the context's poses and sums are not modified.  Same results as
  * mf_track_eval, bit for bit.
  *  - The first call on a device looks up the scratch's device address; make
- *    it (for example once at start-up) before any stream capture.
+ *    it (for example once at start-up) before any stream capture.  The
+ *    address is kept for the life of the process, which assumes the device's
+ *    primary context is not reset (cudaDeviceReset) in between.
+ *  - The slot must hold a tracking problem (set up by mf_track_camera /
+ *    mf_track_objects); otherwise MF_E_STATE, as for mf_track_eval.
  *  - The context's device must be the current device.
  *  - The scratch is shared by every context on the device: calls that overlap
  *    in time (other threads, other contexts) race on it and give wrong sums.
@@ -413,7 +419,8 @@ int mf_process_frame_motion(mf_context* ctx, const float* depth, const uint8_t* 
 /* Camera pose (16 floats) and every instance's volume pose (16 floats each,
  * instance order); either pointer may be NULL.  Synchronises. */
 int mf_get_poses(mf_context* ctx, float* T_w_c, float* T_w_o);
-/* Work counters of the last frame: out[0] voxel blocks in the pool, out[1]
+/* Work counters of the last frame: out[0] voxel blocks in the pool (at most
+ * its capacity; a full pool is the MF_STATUS_POOL_FULL flag), out[1]
  * blocks visited by the last integration, out[2 + i] ray samples instance i
  * emitted into its allocation list, out[2 + n_instances] kernel launches in one
  * replay of the batched frame graph (0 before capture).  Synchronises. */

@@ -1,4 +1,5 @@
 // C ABI of the MID-Fusion B200 library (declared in include/midfusion_b200.h).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -504,7 +505,9 @@ int mf_frame_stats(mf_context* ctx, long long* out, int n) {
     MF_CUDA(cudaMemcpyAsync(&em[i], ctx->inst[i].vol.emit_total, sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
-  out[0] = pc;
+  // the device counter keeps counting requests once the pool is full
+  // (MF_STATUS_POOL_FULL reports that): the blocks held are at most cap
+  out[0] = std::min(pc, ctx->pool.cap);
   out[1] = vc;
   for (size_t i = 0; i < ctx->inst.size() && (int)i + 2 < n; ++i) out[2 + i] = (long long)em[i];
   if ((int)ctx->inst.size() + 2 < n) out[2 + ctx->inst.size()] = (long long)graph_kernel_nodes(ctx);

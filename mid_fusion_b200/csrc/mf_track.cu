@@ -83,6 +83,7 @@ struct TrackState {
   float* rD[MAX_INSTANCES][MAX_PYR] = {};
   F3* rV[MAX_INSTANCES][MAX_PYR] = {};
   GNState* d_state = nullptr;       // MAX_INSTANCES (slot 0: camera, slot i: object i)
+  int slot_kind[MAX_INSTANCES];     // per slot: -1 never set up, else the GNState kind
   double* d_partials = nullptr;     // MAX_INSTANCES x max_tiles x 32
   int max_tiles = 0;
   float2* d_zr = nullptr;           // MAX_PYR x max_tiles live depth range per CTA tile
@@ -908,6 +909,7 @@ int track_init(Context* ctx) {
   if (ctx->track) return MF_OK;
   TrackState* ts = new TrackState;
   ctx->track = ts;
+  for (int i = 0; i < MAX_INSTANCES; ++i) ts->slot_kind[i] = -1;
   ts->levels = std::max(1, std::min(ctx->cfg.pyramid_levels, MAX_PYR));
   PyrPtrs& P = ts->pyr;
   for (int l = 0; l < ts->levels; ++l) {
@@ -1208,6 +1210,7 @@ int track_camera(Context* ctx, uint32_t moving, int retrack) {
     return MF_E_STATE;
   }
   T.tracked = true;
+  T.slot_kind[0] = 0;
   setup_camera_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc, T.d_Twc_prev,
                                                 F4{c.k[0], c.k[1], c.k[2], c.k[3]}, retrack);
   MF_CUDA(cudaGetLastError());
@@ -1237,6 +1240,7 @@ int track_objects(Context* ctx, const IdList& ids) {
   if (int rc = track_init(ctx)) return rc;
   if (ids.n == 0) return MF_OK;
   TrackState& T = *ctx->track;
+  for (int i = 0; i < ids.n; ++i) T.slot_kind[ids.v[i]] = 1;
   setup_objects_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, ids, ctx->d_Twc, T.d_Twc_prev,
                                                   ctx->d_Two, ctx->d_inst_label);
   MF_CUDA(cudaGetLastError());
@@ -1280,6 +1284,10 @@ int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64) {
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums) {
   if (!ctx->track) return MF_E_STATE;
   TrackState& T = *ctx->track;
+  if (T.slot_kind[slot] < 0) {
+    ctx->last_error = "mf_track_eval: slot " + std::to_string(slot) + " has no tracking problem";
+    return MF_E_STATE;
+  }
   GNState S;
   MF_CUDA(cudaMemcpyAsync(&S, T.d_state + slot, sizeof(GNState), cudaMemcpyDeviceToHost,
                           ctx->stream));
@@ -1530,6 +1538,12 @@ int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double
     return MF_E_ARG;
   }
   if (!ctx->track) return MF_E_STATE;
+  const int kind = ctx->track->slot_kind[slot];
+  if (kind < 0) {
+    ctx->last_error = "mf_track_eval_static: slot " + std::to_string(slot) +
+                      " has no tracking problem";
+    return MF_E_STATE;
+  }
   unsigned char* scratch = nullptr;
   if (int rc = eval_scratch_setup(ctx, &scratch)) return rc;
   M4 Tf{}, invTf{};
@@ -1539,11 +1553,11 @@ int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double
     invTf = inverse(Tf);
   }
   const GNArgs a = make_args(ctx, L, 0);
-  if (slot != 0)
+  if (kind == 1)
     if (int rc = tile_depth_range(ctx)) return rc;
   // the ticket must be zero when the launch starts (the last CTA also resets it)
   MF_CUDA(cudaMemsetAsync(scratch + EVAL_TICKET_OFF, 0, sizeof(unsigned), ctx->stream));
-  if (slot == 0)
+  if (kind == 0)
     gn_eval_static_kernel<0><<<tiles, GN_THREADS, 0, ctx->stream>>>(a, slot, L, set_pose, Tf,
                                                                      invTf, scratch);
   else
@@ -1748,6 +1762,7 @@ int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8
   M4 Tl;
   std::memcpy(&Tl, T_live16, 64);
   const mf_config& c = ctx->cfg;
+  T.slot_kind[0] = 0;
   cost_setup_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc,
                                               F4{c.k[0], c.k[1], c.k[2], c.k[3]}, Tl,
                                               inverse(Tl));

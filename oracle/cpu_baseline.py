@@ -1,21 +1,23 @@
 """TEST / BASELINE INFRASTRUCTURE ONLY: the CPU frame pipeline used as the
-reported CPU baseline (bench.py's cpu_baseline leg and --impl reference arm).
+reported CPU baseline (bench.py's cpu_baseline leg and --impl reference arm),
+and the per-frame pose check of the bench's cpu_baseline leg.
 
-One frame = the reference's per-frame order (apps/kfusion/src/benchmark.cpp:113-159):
-camera tracking (Tracking::trackLiveFrame) and object tracking
-(Tracking::trackEachObject) against the last raycast, then
-Object::integrate_volume_kernel for every instance and raycastObjectList.
+One frame = the reference's per-frame order (apps/kfusion/src/benchmark.cpp:113-159,
+Kfusion::tracking / integration / raycasting): preprocessing, camera tracking
+(Tracking::trackLiveFrame, masked by the object pixels of the last raycast as in
+kfusion.cpp:370-400) and object tracking (Tracking::trackEachObject) against the
+last raycast, then Object::integrate_volume_kernel for every instance and
+raycastObjectList.
 
-kind "reference": allocation, integration and raycast run the reference's own
-code (lib/ + the header-only SDF kernels, compiled with OpenMP into
-oracle/_ref/libmf_ref_omp.so); tracking runs this project's restatement,
-because the reference's tracking needs TooN / OpenCV, which are not available.
-kind "port": everything runs the restatement (oracle/liboracle.so).
+kind "reference": every stage runs the reference's own code, compiled
+unmodified with OpenMP from apps/kfusion/src/cpp/{tracking,preprocessing,object,
+rendering} and lib/ into oracle/_ref/libmf_ref_track_omp.so (the reference's
+Release flags, -g -O1) or libmf_ref_track_omp_o3.so (-O3).
+kind "port": everything runs the project's restatement (oracle/liboracle.so).
 Both use every host thread through OpenMP, as the reference does.
 """
 from __future__ import annotations
 
-import ctypes as C
 import os
 import sys
 import time
@@ -23,7 +25,8 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_OMP = os.path.join(HERE, "_ref", "libmf_ref_omp.so")
+REF_BUILDS = {"stock": os.path.join(HERE, "_ref", "libmf_ref_track_omp.so"),
+              "o3": os.path.join(HERE, "_ref", "libmf_ref_track_omp_o3.so")}
 
 
 def _tests_path():
@@ -32,54 +35,76 @@ def _tests_path():
         sys.path.insert(0, p)
 
 
+def reference_available(build="stock"):
+    return os.path.exists(REF_BUILDS[build])
+
+
 class CpuPipeline:
-    def __init__(self, scene, use_reference=True, fp64=False):
+    def __init__(self, scene, use_reference=True, fp64=False, build="stock"):
         _tests_path()
         import _oracle as O
         self.O = O
-        self.s = scene
-        self.kind = "port"
-        impl = O.oracle()
-        if use_reference and os.path.exists(REF_OMP):
-            impl = O.Impl(REF_OMP, "ref_")
-            impl.lib.ref_pin_epsilon(scene.instances[0].size)
-            self.kind = "reference"
-        self.impl = impl
-        s = scene
-        self.vols = [impl.volume(i.size, i.dim) for i in s.instances]
-        self.labels = [i.label for i in s.instances]
-        self.trk = O.Tracker(s.width, s.height, s.k, robust=1, fp64=fp64)
-        # labels of the object instances: their model pixels are ICP outliers
-        # of the camera (trackLiveFrame's mask variant, tracking.cpp:1750-1879)
-        self.moving = [i.label for i in s.instances[1:]]
+        self.s = s = scene
         H, W = s.height, s.width
+        self.labels = [i.label for i in s.instances]
+        # object pixels of the last raycast are ICP outliers of the camera
+        self.moving = [i.label for i in s.instances[1:]]
         self.vertex = np.zeros((H, W, 3), np.float32)
         self.normal = np.zeros((H, W, 3), np.float32)
         self.label_img = np.zeros((H, W), np.int32)
         self.T = s.cam_poses[0].astype(np.float32)
         self.poses = [P.astype(np.float32) for P in s.volume_poses(0)]
         self.frame = 0
+        if use_reference and reference_available(build):
+            self.kind = "reference"
+            lib = O.reference_tracking(REF_BUILDS[build])
+            # the direction epsilon of the reference's ray iterator comes from
+            # the first octree it traverses: the background's
+            lib.rt_pin_epsilon(s.instances[0].size)
+            self.trk = O.RefTracker(W, H, s.k, robust=1, lib=lib)
+            self.objs = [O.RefObject(self.trk, P, size=i.size, dim=i.dim, label=i.label)
+                         for i, P in zip(s.instances, self.poses)]
+            self.render = O.RefRender(W, H, lib=lib)
+        else:
+            self.kind = "port"
+            self.impl = O.oracle()
+            self.vols = [self.impl.volume(i.size, i.dim) for i in s.instances]
+            self.trk = O.Tracker(W, H, s.k, robust=1, fp64=fp64)
 
     def step(self, depth, rgb, labels):
         from mid_fusion_b200.scene import generalize_masks
         s = self.s
-        self.trk.set_frame(rgb, depth)
-        if self.frame > 0:
-            T_prev = self.T
-            self.trk.set_mask((np.isin(self.label_img, self.moving) * 255).astype(np.uint8))
-            self.T = self.trk.track_camera(T_prev, T_prev, self.vertex,
-                                           self.normal).astype(np.float32)
-            for i in range(1, len(self.vols)):
-                self.poses[i] = self.trk.track_object(self.poses[i], self.T, T_prev, self.vertex,
-                                                      self.normal, self.label_img,
-                                                      self.labels[i]).astype(np.float32)
+        mask = (np.isin(self.label_img, self.moving) * 255).astype(np.uint8)
         masks = generalize_masks(labels, self.labels)
         rgb3 = rgb.astype(np.float32) / np.float32(255.0)
-        for i, v in enumerate(self.vols):
-            v.integrate(depth, rgb3, masks[i], self.T, self.poses[i], s.k, 0.1)
-        self.impl.raycast_objects(self.vols, self.poses, self.labels, self.T, s.k, s.width,
-                                  s.height, eps_size=s.instances[0].size, vertex=self.vertex,
-                                  normal=self.normal, label_img=self.label_img)
+        if self.kind == "reference":
+            self.trk.set_frame(rgb, depth)
+            if self.frame > 0:
+                T_prev = self.T
+                self.T = self.trk.track_camera(T_prev, T_prev, self.vertex, self.normal,
+                                               mask=mask)
+                for o in self.objs[1:]:
+                    self.trk.track_object(o, self.T, T_prev)
+            for i, o in enumerate(self.objs):
+                o.integrate(depth, rgb3, masks[i], self.T, s.k, 0.1, self.frame)
+            self.vertex, self.normal, self.label_img = self.render.raycast(self.objs, self.T, s.k)
+            self.poses = [o.pose()[0] for o in self.objs]
+        else:
+            self.trk.set_frame(rgb, depth)
+            if self.frame > 0:
+                T_prev = self.T
+                self.trk.set_mask(mask)
+                self.T = self.trk.track_camera(T_prev, T_prev, self.vertex,
+                                               self.normal).astype(np.float32)
+                for i in range(1, len(self.vols)):
+                    self.poses[i] = self.trk.track_object(
+                        self.poses[i], self.T, T_prev, self.vertex, self.normal, self.label_img,
+                        self.labels[i]).astype(np.float32)
+            for i, v in enumerate(self.vols):
+                v.integrate(depth, rgb3, masks[i], self.T, self.poses[i], s.k, 0.1)
+            self.impl.raycast_objects(self.vols, self.poses, self.labels, self.T, s.k, s.width,
+                                      s.height, eps_size=s.instances[0].size, vertex=self.vertex,
+                                      normal=self.normal, label_img=self.label_img)
         self.trk.set_ref()
         self.frame += 1
 
@@ -89,10 +114,10 @@ def threads():
     return int(n) if n else (os.cpu_count() or 1)
 
 
-def time_frames(scene, frames, n_first, n_timed, use_reference=True):
+def time_frames(scene, frames, n_first, n_timed, use_reference=True, build="stock"):
     """Runs frames [0, n_first + n_timed); times the last n_timed.  Returns
     (seconds per frame, kind)."""
-    p = CpuPipeline(scene, use_reference)
+    p = CpuPipeline(scene, use_reference, build=build)
     t = []
     for f in range(n_first + n_timed):
         d, rgb, lab = frames[f]
@@ -101,3 +126,79 @@ def time_frames(scene, frames, n_first, n_timed, use_reference=True):
         if f >= n_first:
             t.append(time.perf_counter() - t0)
     return float(np.mean(t)), p.kind
+
+
+def _pose_err(A, B):
+    """(translation distance in m, rotation angle in rad) between two poses."""
+    A = np.asarray(A, np.float64)
+    B = np.asarray(B, np.float64)
+    dt = float(np.linalg.norm(A[:3, 3] - B[:3, 3]))
+    R = A[:3, :3].T @ B[:3, :3]
+    # the angle from both the skew part (accurate for small angles) and the trace
+    w = 0.5 * np.array([R[2, 1] - R[1, 2], R[0, 2] - R[2, 0], R[1, 0] - R[0, 1]])
+    return dt, float(np.arctan2(np.linalg.norm(w), 0.5 * (np.trace(R) - 1.0)))
+
+
+def pose_check(scene, frames, gpu_cam, gpu_obj, gpu_maps, n):
+    """Per-frame pose agreement from the same start: for frames 1..n, the
+    reference's tracker (serial parity build of tracking.cpp) and the all-FP64
+    oracle each track frame f from the device's frame f-1 pose, model maps and
+    object poses; the result is compared with the device's frame f poses.
+    gpu_cam[f] (4x4), gpu_obj[f] (K x 4 x 4), gpu_maps[f] = (vertex, normal,
+    label) after frame f.  Returns the max errors over the frames (m / rad),
+    camera and objects separately, of device vs reference, device vs FP64 and
+    reference vs FP64."""
+    _tests_path()
+    import _oracle as O
+    s = scene
+    W, H = s.width, s.height
+    labels = [i.label for i in s.instances]
+    out = {k: {"camera_m": 0.0, "camera_rad": 0.0, "objects_m": 0.0, "objects_rad": 0.0}
+           for k in ("device_vs_reference", "device_vs_fp64_oracle",
+                     "reference_vs_fp64_oracle")}
+
+    def upd(key, part, e):
+        out[key][part + "_m"] = max(out[key][part + "_m"], e[0])
+        out[key][part + "_rad"] = max(out[key][part + "_rad"], e[1])
+
+    have_ref = O.reference_tracking() is not None
+    for f in range(1, n + 1):
+        d0, rgb0, _ = frames[f - 1]
+        d1, rgb1, _ = frames[f]
+        vm, nm, lm = gpu_maps[f - 1]
+        T_prev = np.asarray(gpu_cam[f - 1], np.float32)
+        mask = (np.isin(lm, labels[1:]) * 255).astype(np.uint8)
+        D = O.Tracker(W, H, s.k, robust=1, fp64=True)
+        D.set_frame(rgb0, d0)
+        D.set_ref()
+        D.set_frame(rgb1, d1)
+        D.set_mask(mask)
+        Td = D.track_camera(T_prev, T_prev, vm, nm)
+        upd("device_vs_fp64_oracle", "camera", _pose_err(gpu_cam[f], Td))
+        if have_ref:
+            R = O.RefTracker(W, H, s.k)
+            R.set_frame(rgb0, d0)
+            R.set_ref()
+            R.set_frame(rgb1, d1)
+            Tr = R.track_camera(T_prev, T_prev, vm, nm, mask=mask)
+            upd("device_vs_reference", "camera", _pose_err(gpu_cam[f], Tr))
+            upd("reference_vs_fp64_oracle", "camera", _pose_err(Tr, Td))
+        Tc = np.asarray(gpu_cam[f], np.float32)
+        for i, label in enumerate(labels[1:], 1):
+            if not np.any(lm == label):
+                continue
+            P_prev = np.asarray(gpu_obj[f - 1][i], np.float32)
+            Pd = D.track_object(P_prev, Tc, T_prev, vm, nm, lm, label)
+            upd("device_vs_fp64_oracle", "objects", _pose_err(gpu_obj[f][i], Pd))
+            if have_ref:
+                sel = (lm == label)[..., None]
+                mv = np.where(sel, vm, np.float32(0)).astype(np.float32)
+                mn = np.where(sel, nm, np.array([-2.0, 0, 0], np.float32)).astype(np.float32)
+                ob = R.object(P_prev, mv, mn)
+                Pr, _ = R.track_object(ob, Tc, T_prev)
+                upd("device_vs_reference", "objects", _pose_err(gpu_obj[f][i], Pr))
+                upd("reference_vs_fp64_oracle", "objects", _pose_err(Pr, Pd))
+    if not have_ref:
+        del out["device_vs_reference"], out["reference_vs_fp64_oracle"]
+    out["frames"] = n
+    return out

@@ -82,7 +82,7 @@ unsigned ref_integrate(void* h, const float* depth, const float* rgb3, const flo
     r.list = (refkey_t*)calloc(sizeof(refkey_t) * total, 1);
     r.reserved = total;
   }
-  cv::Mat m(H, W, 4, (void*)mask);
+  cv::Mat m(H, W, CV_32FC1, (void*)mask);
   const unsigned allocated = buildVolumeAllocationList(
       r.list, r.reserved, r.vol._map_index, T_w_c, T_w_o, getCameraMatrix(k), depth, m,
       make_uint2(W, H), r.vol._resol, voxelsize, 2 * mu);

@@ -13,6 +13,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libmf_ref.so")
+REF_TRACK_SO = os.path.join(ROOT, "oracle", "_ref", "libmf_ref_track.so")
 
 P = C.c_void_p
 FP = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
@@ -400,6 +401,261 @@ def reference():
     if "ref" not in _cache:
         _cache["ref"] = Impl(REF_SO, "ref_")
     return _cache["ref"]
+
+
+def reference_tracking(path=REF_TRACK_SO):
+    """The reference's own tracking / preprocessing / object / rendering code
+    (oracle/_ref/libmf_ref_track.so, or another build of it at `path`), or
+    None when it was not built."""
+    if not os.path.exists(path):
+        return None
+    key = "reftrk:" + path
+    if key not in _cache:
+        lib = C.CDLL(path)
+        I32 = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        V = C.c_void_p
+
+        def fn(name, res, *args):
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = list(args)
+        fn("rt_create", P, C.c_int, C.c_int, C.c_int, I32, C.c_int, C.c_int, C.c_int)
+        fn("rt_destroy", None, P)
+        fn("rt_rgb2intensity", None, U8P, C.c_int, C.c_int, FP, FP)
+        fn("rt_set_frame", None, P, FP, FP, FP, V)
+        fn("rt_set_ref_from_current", None, P)
+        fn("rt_track_live", C.c_int, P, FP, FP, FP, FP, FP, V)
+        fn("rt_reduction", None, P, C.c_int, FP)
+        fn("rt_get_level", C.c_int, P, C.c_int, C.c_int, FP)
+        fn("rt_track_data", None, P, C.c_int, I32, FP, FP)
+        fn("rt_compute_residuals", None, P, FP, FP, FP, FP, FP, C.c_int, C.c_int, C.c_float)
+        fn("rt_object_create", P, C.c_int, C.c_int, FP, C.c_int, C.c_float, C.c_int)
+        fn("rt_object_destroy", None, P)
+        fn("rt_object_set_maps", None, P, C.c_int, C.c_int, V, V, V)
+        fn("rt_object_set_pose", None, P, V, V)
+        fn("rt_object_pose", None, P, FP, FP)
+        fn("rt_track_object", None, P, P, FP, FP, FP, FP, FP)
+        fn("rt_object_take_results", None, P, P)
+        fn("rt_refine_mask_use_motion", None, P, FP, C.c_int, C.c_int, C.c_int, C.c_int)
+        fn("rt_object_set_static_state", C.c_int, P, C.c_int)
+        fn("rt_object_fuse_semantics", C.c_int, P, FP, C.c_int, FP)
+        fn("rt_pin_epsilon", None, C.c_int)
+        fn("rt_object_set_label", None, P, C.c_int)
+        fn("rt_object_integrate", None, P, FP, FP, FP, C.c_int, C.c_int, FP, FP, C.c_float,
+           C.c_int)
+        fn("rt_raycast_objects", None, V, C.c_int, FP, FP, C.c_int, C.c_int, C.c_float,
+           C.c_float, C.c_float, FP, FP, I32)
+        fn("rt_render_volume", None, V, C.c_int, U8P, C.c_int, C.c_int, FP, FP, C.c_float,
+           C.c_float, C.c_float, C.c_float, FP, C.c_int, C.c_int, FP, FP, I32, U8P, C.c_int)
+        fn("rt_render_depth", None, U8P, FP, C.c_int, C.c_int, C.c_float, C.c_float)
+        fn("rt_render_intensity", None, U8P, FP, C.c_int, C.c_int)
+        fn("rt_render_normal", None, U8P, FP, C.c_int, C.c_int)
+        fn("rt_render_track", None, U8P, I32, FP, C.c_int, C.c_int, C.c_int)
+        fn("rt_check_static_state", None, U8P, U8P, I32, C.c_int, C.c_int, C.c_int, C.c_int)
+        _cache[key] = lib
+    return _cache[key]
+
+
+def _vp(a):
+    return None if a is None else a.ctypes.data
+
+
+class RefTracker:
+    """The reference's Tracking class (tracking.cpp) compiled from its own
+    sources: ICP + photometric rows, robust kernel Huber by default."""
+
+    def __init__(self, W, H, k, iters=(10, 5, 4), robust=1, use_icp=True, use_rgb=True,
+                 lib=None):
+        self.lib = lib or reference_tracking()
+        assert self.lib is not None, "oracle/_ref/libmf_ref_track.so not built"
+        self.W, self.H, self.k = W, H, _f32(k)
+        self.levels = len(iters)
+        self.h = self.lib.rt_create(W, H, len(iters), np.asarray(iters, np.int32), robust,
+                                    int(use_icp), int(use_rgb))
+
+    def __del__(self):
+        try:
+            self.lib.rt_destroy(self.h)
+        except Exception:
+            pass
+
+    def grey(self, rgb):
+        g = np.zeros((self.H, self.W), np.float32)
+        c = np.zeros((self.H, self.W, 3), np.float32)
+        self.lib.rt_rgb2intensity(np.ascontiguousarray(rgb, np.uint8), self.W, self.H, g, c)
+        return g
+
+    def set_frame(self, rgb, depth, human_mask=None):
+        self._grey = self.grey(rgb)
+        self._depth = _f32(depth)
+        m = None if human_mask is None else np.ascontiguousarray(human_mask, np.uint8)
+        self.lib.rt_set_frame(self.h, self.k, self._grey, self._depth, _vp(m))
+
+    def set_ref(self):
+        self.lib.rt_set_ref_from_current(self.h)
+
+    def track_camera(self, T_in, T_w_r, vertex, normal, mask=None):
+        T = _f32(T_in).reshape(16).copy()
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        self.lib.rt_track_live(self.h, T, _f32(T_w_r).reshape(16), self.k, _f32(vertex),
+                               _f32(normal), _vp(m))
+        return T.reshape(4, 4)
+
+    def object(self, T_w_o, vertex=None, normal=None, vertex_bef=None, class_id=1):
+        o = RefObject(self, T_w_o, class_id)
+        o.set_maps(vertex, normal, vertex_bef)
+        return o
+
+    def track_object(self, obj, T_w_c2, T_w_c1):
+        self.lib.rt_track_object(self.h, obj.h, self.k, _f32(T_w_c2).reshape(16),
+                                 _f32(T_w_c1).reshape(16), self._grey, self._depth)
+        return obj.pose()
+
+    def reduction(self, level):
+        out = np.zeros(32, np.float32)
+        self.lib.rt_reduction(self.h, level, out)
+        return out
+
+    def level(self, l, which):
+        w, h = self.W >> l, self.H >> l
+        out = np.zeros(w * h * 3, np.float32)
+        self.lib.rt_get_level(self.h, l, which, out)
+        if which in (2, 3, 6, 7, 9):
+            return out.reshape(h, w, 3)
+        return out[:w * h].reshape(h, w)
+
+    def track_data(self, level=0):
+        n = 2 * self.W * self.H
+        res = np.zeros(n, np.int32)
+        err = np.zeros(n, np.float32)
+        J = np.zeros(6 * n, np.float32)
+        self.lib.rt_track_data(self.h, level, res, err, J)
+        return (res.reshape(2, self.H, self.W), err.reshape(2, self.H, self.W),
+                J.reshape(2, self.H, self.W, 6))
+
+    def compute_residuals(self, T_w_l, T_w_r, vertex, normal, vertex_l, use_icp=True,
+                          use_rgb=True, threshold=1.5):
+        self.lib.rt_compute_residuals(self.h, _f32(T_w_l).reshape(16), _f32(T_w_r).reshape(16),
+                                      _f32(vertex), _f32(normal), _f32(vertex_l), int(use_icp),
+                                      int(use_rgb), float(threshold))
+        return self.track_data(0)
+
+
+class RefObject:
+    """The reference's Object (object.cpp): pose, volume, model maps, result
+    rows and semantic state (a small 64^3 volume unless size / dim are given)."""
+
+    def __init__(self, trk, T_w_o, class_id=1, size=64, dim=1.0, label=None):
+        self.lib, self.W, self.H = trk.lib, trk.W, trk.H
+        self.h = self.lib.rt_object_create(trk.W, trk.H, _f32(T_w_o).reshape(16), int(size),
+                                           float(dim), class_id)
+        if label is not None:
+            self.lib.rt_object_set_label(self.h, int(label))
+
+    def integrate(self, depth, rgb3, mask, T_w_c, k, mu=0.1, frame=0):
+        self.lib.rt_object_integrate(self.h, _f32(depth), _f32(rgb3), _f32(mask), self.W, self.H,
+                                     _f32(T_w_c).reshape(16), _f32(k), float(mu), int(frame))
+
+    def __del__(self):
+        try:
+            self.lib.rt_object_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_maps(self, vertex=None, normal=None, vertex_bef=None):
+        keep = [None if a is None else _f32(a) for a in (vertex, normal, vertex_bef)]
+        self.lib.rt_object_set_maps(self.h, self.W, self.H, *[_vp(a) for a in keep])
+
+    def set_pose(self, T_w_o=None, T_virtual=None):
+        keep = [None if a is None else _f32(a).reshape(16) for a in (T_w_o, T_virtual)]
+        self.lib.rt_object_set_pose(self.h, *[_vp(a) for a in keep])
+
+    def pose(self):
+        a = np.zeros(16, np.float32)
+        b = np.zeros(16, np.float32)
+        self.lib.rt_object_pose(self.h, a, b)
+        return a.reshape(4, 4), b.reshape(4, 4)
+
+    def take_results(self, trk):
+        self.lib.rt_object_take_results(self.h, trk.h)
+
+    def refine_mask(self, mask, use_icp=True, use_rgb=True):
+        m = _f32(mask).copy()
+        self.lib.rt_refine_mask_use_motion(self.h, m, self.W, self.H, int(use_icp), int(use_rgb))
+        return m
+
+    def set_static_state(self, state):
+        return bool(self.lib.rt_object_set_static_state(self.h, int(state)))
+
+    def fuse_semantics(self, prob, recog_time=1):
+        out = np.zeros(80, np.float32)
+        cid = self.lib.rt_object_fuse_semantics(self.h, _f32(prob), int(recog_time), out)
+        return cid, out
+
+
+class RefRender:
+    """The reference's raycastObjectList and render kernels (rendering.cpp),
+    compiled from its own sources, over RefObject lists."""
+
+    def __init__(self, W, H, lib=None):
+        self.lib = lib or reference_tracking()
+        assert self.lib is not None, "oracle/_ref/libmf_ref_track.so not built"
+        self.W, self.H = W, H
+
+    @staticmethod
+    def _objs(objs):
+        return (C.c_void_p * len(objs))(*[o.h for o in objs])
+
+    def raycast(self, objs, T_w_c, k, near=0.1, far=4.0, mu=0.1):
+        v = np.zeros((self.H, self.W, 3), np.float32)
+        n = np.zeros((self.H, self.W, 3), np.float32)
+        lab = np.zeros((self.H, self.W), np.int32)
+        self.lib.rt_raycast_objects(self._objs(objs), len(objs), _f32(T_w_c).reshape(16), _f32(k),
+                                    self.W, self.H, near, far, mu, v, n, lab)
+        return v, n, lab
+
+    def volume(self, objs, T_w_c, k, near, far, mu, largestep, render_color, colors, maps=None,
+               ambient=(0.1, 0.1, 0.1)):
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        if maps is None:
+            v = nr = np.zeros((self.H, self.W, 3), np.float32)
+            lab = np.zeros((self.H, self.W), np.int32)
+        else:
+            v, nr, lab = _f32(maps[0]), _f32(maps[1]), np.ascontiguousarray(maps[2], np.int32)
+        col = np.ascontiguousarray(colors, np.uint8).reshape(-1, 4)
+        self.lib.rt_render_volume(self._objs(objs), len(objs), out, self.W, self.H,
+                                  _f32(T_w_c).reshape(16), _f32(k), near, far, mu, largestep,
+                                  _f32(ambient), int(maps is None), int(render_color), v, nr, lab,
+                                  col, len(col))
+        return out
+
+    def depth(self, depth, near, far):
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        self.lib.rt_render_depth(out, _f32(depth), self.W, self.H, near, far)
+        return out
+
+    def intensity(self, grey):
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        self.lib.rt_render_intensity(out, _f32(grey), self.W, self.H)
+        return out
+
+    def normal(self, normal):
+        out = np.zeros((self.H, self.W, 3), np.uint8)
+        self.lib.rt_render_normal(out, _f32(normal), self.W, self.H)
+        return out
+
+    def track(self, res, err, mode):
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        self.lib.rt_render_track(out, np.ascontiguousarray(res, np.int32), _f32(err), self.W,
+                                 self.H, int(mode))
+        return out
+
+    def static_inliers(self, object_mask, res, use_icp=True, use_rgb=True):
+        out = np.zeros((self.H, self.W), np.uint8)
+        self.lib.rt_check_static_state(out, np.ascontiguousarray(object_mask, np.uint8),
+                                       np.ascontiguousarray(res, np.int32), self.W, self.H,
+                                       int(use_icp), int(use_rgb))
+        return out
 
 
 class Tracker:

@@ -3,6 +3,12 @@
 * tests/golden/volume_golden.npz: allocation, integration and multi-instance
   raycast outputs of the reference's own code (oracle/_ref, generated by
   tests/golden/make_golden.py), compared bit for bit.
+* tests/golden/track_golden.npz: the reference's own tracking
+  (tracking.cpp / preprocessing.cpp / object.cpp, generated by
+  tests/golden/make_track_golden.py): pyramid digests, camera poses and
+  per-level sums (plain and masked trackLiveFrame), object poses and sums
+  (trackEachObject) and motion residual rows, which the single-precision
+  tracking oracle reproduces bit for bit.
 * Fixed cases of the reference's unit tests: unique_multiscale counts
   (lib/test/algorithms/unique_unittest.cpp:113-143), bilinear interpolation on
   a checkerboard (apps/kfusion/test/preprocessing/interp_unittest.cpp:24-51),
@@ -19,6 +25,7 @@ import pytest
 import _oracle as O
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "volume_golden.npz")
+TRACK_GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "track_golden.npz")
 
 
 def digest(a):
@@ -72,6 +79,46 @@ def test_volume_golden_vectors():
         assert np.array_equal(nrm, g[f"f{f}_normal"])
         f += 1
     assert f >= 2
+
+
+def test_track_golden_vectors():
+    g = np.load(TRACK_GOLDEN)
+    H, W = g["depth0"].shape
+    k, labels = g["k"], [int(x) for x in g["labels"]]
+    T0, P0, vm, nm, lm = g["T0"], g["P0"], g["vertex"], g["normal"], g["label"]
+
+    def tracker():
+        t = O.Tracker(W, H, k, robust=1, fp64=False)
+        t.set_frame(g["rgb0"], g["depth0"])
+        t.set_ref()
+        t.set_frame(g["rgb1"], g["depth1"])
+        return t
+
+    def sums(t, level):
+        out = np.zeros(32, np.float64)
+        t.lib.ot_last_sums(t.h, level, out)
+        return out.astype(np.float32)
+
+    F = tracker()
+    for level in range(3):
+        for which in range(7):
+            assert digest(F.level(level, which)) == str(g[f"pyr_l{level}_w{which}"]), (level, which)
+    Tc = F.track_camera(T0, T0, vm, nm).astype(np.float32)
+    assert np.array_equal(Tc, g["camera_pose"])
+    for level in range(3):
+        assert np.array_equal(sums(F, level), g["camera_sums"][level]), level
+    for i, label in enumerate(labels[1:], 1):
+        To = F.track_object(P0[i], Tc, T0, vm, nm, lm, label).astype(np.float32)
+        assert np.array_equal(To, g[f"object{label}_pose"]), label
+        for level in range(3):
+            assert np.array_equal(sums(F, level), g[f"object{label}_sums"][level]), (label, level)
+    Fm = tracker()
+    Fm.set_mask((np.isin(lm, labels[1:]) * 255).astype(np.uint8))
+    assert np.array_equal(Fm.track_camera(T0, T0, vm, nm).astype(np.float32),
+                          g["camera_pose_masked"])
+    res, err = F.motion_residuals(Tc, T0, vm, nm, g["live_vertex"])
+    assert np.array_equal(res, g["residual_codes"])
+    assert np.array_equal(err[res == 1], g["residual_errors_valid"])
 
 
 def test_unique_multiscale_counts(lib):
