@@ -659,6 +659,7 @@ def main():
                 "algorithmic_bytes_per_launch": int(prof["gn_l0_bytes"]),
                 "traffic": traffic_from_profiles("gn_iter_kernel_l0_640x480.md")}
     ai = gbs(prof["integrate_bytes"], prof["integrate_us"])
+    ar = gbs(prof["raycast_bytes"], prof["raycast_us"])
     others = {
         "integrate_blocks_kernel": {"achieved": round(ai, 1), "unit": "GB/s",
                                     "frac": round(ai / hbm, 4),
@@ -666,8 +667,10 @@ def main():
                                     "algorithmic_bytes_per_launch": int(prof["integrate_bytes"]),
                                     "traffic": traffic_from_profiles(
                                         "integrate_blocks_kernel_640x480.md")},
-        "raycast_objects_kernel": {"us_per_launch": round(prof["raycast_us"], 2),
-                                   "bound": "instruction fetch (ncu: no_instruction stalls)",
+        "raycast_objects_kernel": {"achieved": round(ar, 1), "unit": "GB/s",
+                                   "frac": round(ar / hbm, 4),
+                                   "us_per_launch": round(prof["raycast_us"], 2),
+                                   "algorithmic_bytes_per_launch": int(prof["raycast_bytes"]),
                                    "traffic": traffic_from_profiles(
                                        "raycast_objects_kernel_640x480.md")},
     }

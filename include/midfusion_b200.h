@@ -39,6 +39,7 @@ extern "C" {
 #define MF_STATUS_RAY_GUARD 4
 #define MF_STATUS_GN_FALLBACK 8     /* a 6x6 system used the truncated eigen solve */
 #define MF_STATUS_ADJOINT 16        /* mf_camera_cost skipped the TSDF adjoint of a ray */
+#define MF_STATUS_GN_TIMEOUT 32     /* a grid barrier of the persistent GN launch gave up */
 
 /* Robust kernels of Tracking::calc_robust_weight,
  * apps/kfusion/src/cpp/tracking/tracking.cpp:1504-1532 (enum RobustW,
@@ -208,7 +209,9 @@ int mf_camera_cost(mf_context* ctx, const float T_live[16], double* out, float* 
  * > -3; -1 for the background and for objects out of view.
  * moving_labels (optional): bit `label` set for each object with
  * 0.05 < ratio < moved_threshold (the reference's defaults: residual
- * threshold 1.5, kernels.h:95; moved threshold 0.9, config --obj-moved).
+ * threshold 1.5, kernels.h:95; moved threshold 0.9, config --obj-moved)
+ * whose class (mf_instance_set_semantics) is not one of the never-moving
+ * classes 63, 69, 70 (Object::static_object, object.cpp:326).
  * The bits can be passed to mf_track_camera.  Synchronises. */
 int mf_motion_residuals(mf_context* ctx, float residual_threshold, float moved_threshold,
                         float* inlier_ratio, uint32_t* moving_labels);
@@ -229,6 +232,18 @@ int mf_motion_download(mf_context* ctx, int8_t* results, float* errors, float* l
  * float[2][H][W]): TrackData::error of the rows with result 1, else 0. */
 int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* d_errors,
                      float* pose_eval);
+/* Replaces the object part of Kfusion::tracking's residual pass,
+ * kfusion.cpp:446-466: after a moving object id >= 1 was tracked
+ * (mf_track_objects) and the live raycast redone at its new pose
+ * (mf_motion_residuals), its result rows recomputed by
+ * Tracking::compute_residuals (tracking.cpp:1535-1747) at its virtual camera
+ * pose T_w_o1 inverse(T_c2_o2) (tracking.cpp:696) against its own pixels of
+ * the model maps and of the live raycast -- what the reference copies into
+ * the object's trackresult_ for Object::refine_mask_use_motion.  Rows to
+ * d_results (device int8[2][H][W]); the virtual pose (host float[16],
+ * optional; given, the call synchronises). */
+int mf_object_residuals(mf_context* ctx, int id, float threshold, int8_t* d_results,
+                        float* T_virtual);
 /* Object::refine_mask_use_motion (object/object.cpp:255-315, outliers not
  * absorbed into the background) on instance id's generalized mask of the
  * current frame: where the mask is >= 0, an ICP row of -4 or -6 or a
@@ -310,12 +325,21 @@ int mf_tum_line(int frame, const float T_translation[16], const float T_rotation
  * under 1 m mesh to nothing; float_bounds = 1 bounds by the float extent
  * instead.  The triangulation table is generated from the cube's
  * geometry (gen_mc_tables.py): the same polygons as the reference's table,
- * possibly split along other diagonals.  Triangles are 9 floats (three
+ * possibly split along other diagonals; with the reference's own table
+ * (mf_mesh_set_triangle_table) the triangles are the reference's, one for
+ * one.  Triangles are 9 floats (three
  * vertices, metres, volume frame), blocks in Morton order and cells x-major
  * within a block.  tris may be host or device memory; with tris NULL or cap
  * below the count only n_tris is set.  Synchronises. */
 int mf_mesh(mf_context* ctx, int id, int float_bounds, float* tris, long long cap,
             long long* n_tris);
+/* The marching-cubes triangulation table mf_mesh uses for this context: 256
+ * rows of 16 ints, each at most 5 edge triples (edges 0..11 as
+ * lib/algorithms/meshing.hpp numbers them) ended by -1 -- the layout of the
+ * reference's triTable (lib/algorithms/edge_tables.h), which a caller that has
+ * it passes as &triTable[0][0] to get the reference's triangles.  NULL
+ * restores the built-in table.  MF_E_ARG for a malformed row. */
+int mf_mesh_set_triangle_table(mf_context* ctx, const int* table);
 /* writeVtkMesh (commons.h:945-1011): legacy ASCII VTK polydata, three points
  * per triangle.  Host code only. */
 int mf_write_vtk_mesh(const char* path, const float* tris, long long n);
@@ -404,15 +428,15 @@ int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t
  *  4. from this entry point's third frame on, every instance's generalized
  *     mask is refined (mf_refine_mask_use_motion): the background and static
  *     objects with the camera's rows (those motion residuals when objects
- *     move, else the camera's last GN rows), a moving object with the rows of
- *     its own last GN iteration (the reference recomputes them at the object's
- *     final pose, kfusion.cpp:446-466; not done here);
+ *     move, else the camera's last GN rows), a moving object with its rows
+ *     recomputed at its virtual camera pose (mf_object_residuals,
+ *     kfusion.cpp:446-466);
  *  5. every instance is integrated, the composite raycast replaces the model
  *     maps, and the frame becomes the photometric reference.
  * The first frame (no reference yet) is integrated and raycast untracked.
  * moving_labels receives the moving-label bits of step 2 (0 on the first
- * frame).  The reference's exclusion of never-moving classes
- * (Object::static_object) is not applied. */
+ * frame).  Objects of the never-moving classes (Object::static_object)
+ * never move. */
 int mf_process_frame_motion(mf_context* ctx, const float* depth, const uint8_t* rgb,
                             const uint16_t* labels, float residual_threshold,
                             float moved_threshold, uint32_t* moving_labels);
@@ -428,11 +452,21 @@ int mf_frame_stats(mf_context* ctx, long long* out, int n);
 /* Kernel timing on the current frame (CUDA events on the context's stream,
  * `reps` launches each): out[0] us per camera GN evaluation at level 0 and
  * out[1] its algorithmic bytes; out[2] us per integration launch and out[3] its
- * algorithmic bytes (counted); out[4] us per raycast launch.  Re-integrates
- * the current frame, so call it only after the frames that matter. */
+ * algorithmic bytes (counted); out[4] us per raycast launch and out[5] its
+ * algorithmic bytes (counted by a replay of the march: 8 B per voxel read,
+ * 32 B per trilinear interpolation, 64 + 192 B per candidate hit's
+ * foreground interpolation and gradient, 28 B of output per pixel).
+ * Re-integrates the current frame, so call it only after the frames that
+ * matter. */
 int mf_profile(mf_context* ctx, int reps, double* out, int n);
 /* Batched mode replays the frame as a CUDA graph once captured (default 1). */
 int mf_set_graphs(mf_context* ctx, int enable);
+/* No counterpart in the reference.  Batched GN runs every iteration of a
+ * pyramid level in one cooperative launch per level and stage, with a grid
+ * barrier between iterations and an early end once every problem has stopped
+ * (1, the default), or one launch per iteration (0).  Both give the same
+ * poses bit for bit.  Applies to frames captured after the call. */
+int mf_set_gn_persistent(mf_context* ctx, int enable);
 
 /* --- launch-shape autotuner (no counterpart in the reference) ----------
  * Two kernels of the frame run in one of several launch shapes that change

@@ -74,8 +74,34 @@ def left_jacobian(twist, h=1e-7):
     return J
 
 
-class CameraCost(torch.autograd.Function):
-    """E = CameraCost.apply(twist, tsdf, context, T0).
+_EXT = None
+
+
+def _extension():
+    """The libtorch autograd Function (csrc_torch/mf_autograd.cpp), loaded
+    from its in-tree build; there is no Python fallback."""
+    global _EXT
+    if _EXT is None:
+        import importlib.machinery
+        import importlib.util
+        import os
+        from . import build as B
+        path = B.torch_ext_path()
+        if not os.path.exists(path):
+            raise RuntimeError(f"libtorch extension not built: {path} "
+                               "(run python -m mid_fusion_b200.build)")
+        loader = importlib.machinery.ExtensionFileLoader(B.TORCH_EXT_NAME, path)
+        spec = importlib.util.spec_from_file_location(B.TORCH_EXT_NAME, path, loader=loader)
+        mod = importlib.util.module_from_spec(spec)
+        loader.exec_module(mod)
+        _EXT = mod
+    return _EXT
+
+
+class CameraCost:
+    """E = CameraCost.apply(twist, tsdf, context, T0): the camera-tracking
+    cost as a libtorch torch::autograd::Function (CameraCostFunction in
+    csrc_torch/mf_autograd.cpp), whose backward runs the hand-written adjoint.
 
     twist: (6,) float64 tensor (v, w); tsdf: the tensor from pool_tsdf_tensor
     (or any float32 CUDA tensor of the same length, which is copied into the
@@ -83,23 +109,8 @@ class CameraCost(torch.autograd.Function):
     reference frame; T0: 4x4 base pose (numpy)."""
 
     @staticmethod
-    def forward(fctx, twist, tsdf, context, T0):
-        pool = pool_tsdf_tensor(context)
-        if tsdf.data_ptr() != pool.data_ptr():
-            pool.copy_(tsdf)
-        tw = twist.detach().cpu().numpy().astype(np.float64)
-        T = (se3_exp(tw) @ np.asarray(T0, np.float64)).astype(np.float32)
-        E, _, _ = context.camera_cost(T)
-        fctx.context, fctx.T = context, T
-        fctx.save_for_backward(twist, tsdf)
-        return torch.tensor(E, dtype=torch.float64)
-
-    @staticmethod
-    def backward(fctx, gE):
-        twist, tsdf = fctx.saved_tensors
-        grad = torch.zeros(tsdf.numel(), dtype=torch.float32, device=tsdf.device)
-        _, g_eps, _ = fctx.context.camera_cost(fctx.T, grad.data_ptr())
-        J = left_jacobian(twist.detach().cpu().numpy())
-        g_twist = torch.from_numpy(J.T @ g_eps).to(twist.dtype)
-        s = float(gE)
-        return g_twist * s, (grad * s).view_as(tsdf), None, None
+    def apply(twist, tsdf, context, T0):
+        import ctypes
+        T0t = torch.as_tensor(np.asarray(T0, np.float64))
+        ptr = ctypes.cast(context.h, ctypes.c_void_p).value
+        return _extension().camera_cost(twist, tsdf, int(ptr), T0t)

@@ -63,7 +63,35 @@ def build(force=False, verbose=False, extra=()):
     return LIB
 
 
+TORCH_EXT_NAME = "mf_autograd_ext"
+TORCH_EXT_DIR = os.path.join(LIB_DIR, "torch_ext")
+TORCH_EXT_SRC = os.path.join(HERE, "csrc_torch", "mf_autograd.cpp")
+
+
+def torch_ext_path():
+    return os.path.join(TORCH_EXT_DIR, TORCH_EXT_NAME + ".so")
+
+
+def build_torch_ext(verbose=False):
+    """The libtorch autograd Function over mf_camera_cost
+    (csrc_torch/mf_autograd.cpp), built in-tree against the CUDA library."""
+    out = torch_ext_path()
+    if (os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(TORCH_EXT_SRC) and
+            os.path.getmtime(out) >= os.path.getmtime(LIB)):
+        return out
+    from torch.utils import cpp_extension
+    os.makedirs(TORCH_EXT_DIR, exist_ok=True)
+    cpp_extension.load(
+        name=TORCH_EXT_NAME, sources=[TORCH_EXT_SRC], build_directory=TORCH_EXT_DIR,
+        extra_cflags=["-O2", "-std=c++17"],
+        extra_ldflags=[f"-L{LIB_DIR}", "-lmidfusion_b200", f"-Wl,-rpath,{LIB_DIR}",
+                       "-Wl,-rpath,$ORIGIN/.."],
+        verbose=verbose, is_python_module=True)
+    return out
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True,
           extra=["-Xptxas", "-v"] if "--ptxas-v" in sys.argv else [])
     print(LIB)
+    print(build_torch_ext(verbose=True))

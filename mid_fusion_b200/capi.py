@@ -43,6 +43,7 @@ EXPORTS = [
     "mf_raw_read", "mf_raw_close", "mf_save_poses", "mf_pose_quaternion", "mf_tum_line",
     "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh", "mf_tune_candidates", "mf_tune_describe",
     "mf_autotune", "mf_tune_get", "mf_tune_set", "mf_process_frame_motion",
+    "mf_set_gn_persistent", "mf_object_residuals", "mf_mesh_set_triangle_table",
 ]
 
 TUNE_RAYCAST, TUNE_INTEGRATE, TUNE_MAX_VARIANTS = 0, 1, 16
@@ -220,7 +221,7 @@ class Context:
         out = np.zeros(6, np.float64)
         self._check(self.lib.mf_profile(self.h, int(reps), _ptr(out, np.float64), len(out)))
         return {"gn_l0_us": out[0], "gn_l0_bytes": out[1], "integrate_us": out[2],
-                "integrate_bytes": out[3], "raycast_us": out[4]}
+                "integrate_bytes": out[3], "raycast_us": out[4], "raycast_bytes": out[5]}
 
     def process_frame_motion(self, depth, rgb, labels, residual_threshold=1.5,
                              moved_threshold=0.9):
@@ -256,6 +257,9 @@ class Context:
 
     def tune_set(self, stage, variant):
         self._check(self.lib.mf_tune_set(self.h, int(stage), int(variant)))
+
+    def set_gn_persistent(self, enable):
+        self._check(self.lib.mf_set_gn_persistent(self.h, int(enable)))
 
     def status(self):
         f = C.c_int()
@@ -361,6 +365,15 @@ class Context:
                                               _ptr(pose, np.float32)))
         return pose.reshape(4, 4)
 
+    def object_residuals(self, i, d_ptr, threshold=1.5):
+        """Object i's result rows recomputed at its virtual camera pose
+        (kfusion.cpp:446-466) into device memory at d_ptr (2 * H * W int8);
+        returns the virtual pose."""
+        pose = np.zeros(16, np.float32)
+        self._check(self.lib.mf_object_residuals(self.h, int(i), C.c_float(threshold),
+                                                 C.c_void_p(d_ptr), _ptr(pose, np.float32)))
+        return pose.reshape(4, 4)
+
     def upload_raw(self, depth_mm=None, rgb=None):
         """A sensor frame (uint16 mm depth, uint8 rgb) of an integer multiple of
         the frame size (mf_frame_upload_raw)."""
@@ -379,6 +392,15 @@ class Context:
         self._check(self.lib.mf_mesh(self.h, int(i), fb, _ptr(out, np.float32), n.value,
                                      C.byref(n)))
         return out[:n.value]
+
+    def set_triangle_table(self, table=None):
+        """The marching-cubes triangle table for mf_mesh (256 x 16 ints, -1
+        ended), or None for the built-in one."""
+        if table is None:
+            self._check(self.lib.mf_mesh_set_triangle_table(self.h, None))
+            return
+        t = np.ascontiguousarray(table, np.int32).reshape(256, 16)
+        self._check(self.lib.mf_mesh_set_triangle_table(self.h, _ptr(t, np.int32)))
 
     def dump_mesh(self, prefix):
         self._check(self.lib.mf_dump_mesh(self.h, str(prefix).encode()))

@@ -153,7 +153,9 @@ int mf_create(const mf_config* cfg, mf_context** out) {
        cudaMalloc(&ctx->d_labels, 2 * WH) == cudaSuccess &&
        cudaMalloc(&ctx->d_vertex, sizeof(F3) * WH) == cudaSuccess &&
        cudaMalloc(&ctx->d_normal, sizeof(F3) * WH) == cudaSuccess &&
-       cudaMalloc(&ctx->d_label, sizeof(int) * WH) == cudaSuccess;
+       cudaMalloc(&ctx->d_label, sizeof(int) * WH) == cudaSuccess &&
+       cudaMalloc(&ctx->d_rayhit, sizeof(F4) * WH * cfg->max_instances) == cudaSuccess &&
+       cudaMalloc(&ctx->d_raytf, sizeof(float2) * WH * cfg->max_instances) == cudaSuccess;
   if (!ok) {
     ctx->last_error = "device allocation failed";
     return fail(MF_E_CUDA);
@@ -199,7 +201,8 @@ int mf_destroy(mf_context* ctx) {
                 ctx->d_reserved, ctx->d_inst_label, ctx->d_visit, ctx->d_visit_count,
                 ctx->d_depth, ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, ctx->d_masks,
                 ctx->d_labels, ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->d_export,
-                ctx->d_render, ctx->d_render_small};
+                ctx->d_render, ctx->d_render_small, ctx->d_rayhit, ctx->d_raytf,
+                ctx->d_mc_tris};
   for (void* p : ps) if (p) cudaFree(p);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -518,13 +521,21 @@ int mf_profile(mf_context* ctx, int reps, double* out, int n) {
   if (check(ctx) || !out || n < 6 || reps < 1) return MF_E_ARG;
   if (int rc = profile_gn(ctx, reps, &out[0], &out[1])) return rc;
   if (int rc = profile_integrate(ctx, reps, &out[2], &out[3])) return rc;
-  out[5] = 0;
-  return profile_raycast(ctx, reps, &out[4]);
+  return profile_raycast(ctx, reps, &out[4], &out[5]);
 }
 
 int mf_set_graphs(mf_context* ctx, int enable) {
   if (check(ctx)) return MF_E_ARG;
   ctx->use_graphs = enable != 0;
+  return MF_OK;
+}
+
+int mf_set_gn_persistent(mf_context* ctx, int enable) {
+  if (check(ctx)) return MF_E_ARG;
+  if (ctx->gn_persistent != (enable != 0)) {
+    ctx->gn_persistent = enable != 0;
+    ++ctx->tune.gen;  // captured frame graphs are rebuilt
+  }
   return MF_OK;
 }
 
@@ -671,6 +682,15 @@ int mf_track_results(mf_context* ctx, int id, int8_t* d_results, float* d_errors
   return track_results(ctx, id, d_results, d_errors, pose_eval);
 }
 
+int mf_object_residuals(mf_context* ctx, int id, float threshold, int8_t* d_results,
+                        float* T_virtual) {
+  if (check(ctx) || !d_results || id < 1 || !(threshold > 0)) return MF_E_ARG;
+  if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+  const int rc = object_residuals(ctx, id, threshold, d_results, T_virtual);
+  if (rc == MF_OK && T_virtual) MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return rc;
+}
+
 int mf_refine_mask_use_motion(mf_context* ctx, int id, const int8_t* d_results) {
   if (check(ctx) || id < 0) return MF_E_ARG;
   if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
@@ -809,6 +829,11 @@ int mf_mesh(mf_context* ctx, int id, int float_bounds, float* tris, long long ca
   if (check(ctx) || id < 0 || !n_tris || cap < 0) return MF_E_ARG;
   if (id >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
   return mesh_volume(ctx, id, float_bounds, tris, cap, n_tris);
+}
+
+int mf_mesh_set_triangle_table(mf_context* ctx, const int* table) {
+  if (check(ctx)) return MF_E_ARG;
+  return mesh_set_table(ctx, table);
 }
 
 int mf_write_vtk_mesh(const char* path, const float* tris, long long n) {

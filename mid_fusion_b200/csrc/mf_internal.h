@@ -101,6 +101,11 @@ struct Context {
   F3* d_vertex = nullptr;
   F3* d_normal = nullptr;
   int* d_label = nullptr;
+  // phased raycast: per instance and pixel, the unbounded hit (x, y, z, t) and
+  // (crossing sample t, foreground at the hit); max_instances x W*H each
+  F4* d_rayhit = nullptr;
+  float2* d_raytf = nullptr;
+  int8_t* d_mc_tris = nullptr;      // marching-cubes triangulation table (mf_mesh)
 
   // staging
   float* h_pinned = nullptr;        // small pinned host staging area
@@ -109,6 +114,7 @@ struct Context {
   float ray_epsilon = 0.f;          // ray iterator direction epsilon (first volume)
   void* graphs = nullptr;           // captured frame graphs (mf_pipeline.cu)
   bool use_graphs = true;
+  bool gn_persistent = true;        // batched GN: one cooperative launch per level
   TrackState* track = nullptr;
   Tune tune;                        // autotuned launch shapes
   // mf_process_frame_motion: frames it has processed, and two planes of
@@ -158,6 +164,8 @@ int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
                      uint32_t* moving);
 int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t* llabel);
 int track_results(Context* ctx, int slot, int8_t* d_out, float* d_err, float* pose_eval);
+int object_residuals(Context* ctx, int i, float threshold, int8_t* d_rows, float* T_virtual);
+int mesh_set_table(Context* ctx, const int* table);
 int motion_planes(Context* ctx, const int8_t** res, const float** err);
 // headless renders (mf_render.cu; the shaded volume render in mf_raycast.cu)
 // formats (mf_io.cu)
@@ -199,7 +207,7 @@ int process_frame_motion(Context* ctx, float residual_threshold, float moved_thr
                          uint32_t* moving_labels);
 int profile_integrate(Context* ctx, int reps, double* us, double* bytes);
 int profile_gn(Context* ctx, int reps, double* us, double* bytes);
-int profile_raycast(Context* ctx, int reps, double* us);
+int profile_raycast(Context* ctx, int reps, double* us, double* bytes);
 void pipeline_free(Context* ctx);
 // launch-shape candidates (autotuner)
 int ray_variant_count();

@@ -7,9 +7,12 @@
 // counts each block's kept triangles, the second writes them at the block's
 // offset in cell order (x-major, then y, then z, as the reference loops).
 // Blocks are taken in Morton order.  The triangulation table is this
-// project's (gen_mc_tables.py); the cell test, the edge intersections and the
-// vertex bounds are the reference's.
+// project's (gen_mc_tables.py) unless the caller supplies one
+// (mf_mesh_set_triangle_table: the reference's triTable gives its triangles
+// one for one); the cell test, the edge intersections and the vertex bounds
+// are the reference's.
 #include <cstdio>
+#include <cstring>
 #include <string>
 #include <vector>
 #include "mf_internal.h"
@@ -17,7 +20,6 @@
 
 namespace mf {
 
-__constant__ int8_t c_mc_tris[256][3 * MF_MC_MAX_TRIS];
 // corner offsets and edges (meshing.hpp:31-74); each edge is interpolated from
 // its first corner to its second
 __constant__ int8_t c_corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 0, 1}, {0, 0, 1},
@@ -28,6 +30,7 @@ __constant__ int8_t c_edge[12][2] = {{0, 1}, {1, 2}, {2, 3}, {0, 3}, {4, 5}, {5,
 struct MeshArgs {
   Pool pool;
   Volume V;
+  const int8_t* tris;      // triangulation table, 256 x 3 * MF_MC_MAX_TRIS edge indices
   const int* slots;        // the instance's blocks, Morton order
   int n_blocks;
   const long long* offset; // first triangle of each block (pass 2)
@@ -101,7 +104,7 @@ __global__ void __launch_bounds__(512) mesh_kernel(MeshArgs a) {
         if (c[i].x < 0.f) index |= 1 << i;
   }
   // kept triangles of this cell, in table order
-  const int8_t* tr = c_mc_tris[index];
+  const int8_t* tr = a.tris + index * (3 * MF_MC_MAX_TRIS);
   F3 v[3 * MF_MC_MAX_TRIS];
   int kept = 0;
   for (int e = 0; e < 3 * MF_MC_MAX_TRIS && tr[e] != -1; e += 3) {
@@ -147,14 +150,43 @@ __global__ void __launch_bounds__(512) mesh_kernel(MeshArgs a) {
   }
 }
 
-static bool g_mc_table_ready = false;
+// The context's triangulation table on the device: `table` (256 rows of 16
+// ints, edge triples ended by -1, the layout of the reference's triTable,
+// lib/algorithms/edge_tables.h), or the built-in one when table is NULL.
+int mesh_set_table(Context* ctx, const int* table) {
+  int8_t t[256][3 * MF_MC_MAX_TRIS];
+  if (!table) {
+    std::memcpy(t, MF_MC_TRIS, sizeof(t));
+  } else {
+    for (int r = 0; r < 256; ++r) {
+      const int* row = table + 16 * r;
+      int n = 0;
+      while (n < 16 && row[n] != -1) ++n;
+      if (n == 16 || n % 3 != 0 || n > 3 * MF_MC_MAX_TRIS) {
+        ctx->last_error = "mf_mesh_set_triangle_table: row " + std::to_string(r) +
+                          " is not at most 5 edge triples ended by -1";
+        return MF_E_ARG;
+      }
+      for (int e = 0; e < 3 * MF_MC_MAX_TRIS; ++e) {
+        if (e < n && (row[e] < 0 || row[e] > 11)) {
+          ctx->last_error = "mf_mesh_set_triangle_table: edge index outside 0..11 in row " +
+                            std::to_string(r);
+          return MF_E_ARG;
+        }
+        t[r][e] = e < n ? (int8_t)row[e] : (int8_t)-1;
+      }
+    }
+  }
+  if (!ctx->d_mc_tris) MF_CUDA(cudaMalloc(&ctx->d_mc_tris, sizeof(t)));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_mc_tris, t, sizeof(t), cudaMemcpyHostToDevice, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
 
 int mesh_volume(Context* ctx, int id, int float_bounds, float* tris, long long cap,
                 long long* n_tris) {
-  if (!g_mc_table_ready) {
-    MF_CUDA(cudaMemcpyToSymbol(c_mc_tris, MF_MC_TRIS, sizeof(MF_MC_TRIS)));
-    g_mc_table_ready = true;
-  }
+  if (!ctx->d_mc_tris)
+    if (int rc = mesh_set_table(ctx, nullptr)) return rc;
   const Volume& V = ctx->inst[id].vol;
   // the instance's blocks in Morton order (the block table's own order)
   const long long n_tab = 1LL << (3 * V.block_level);
@@ -177,6 +209,7 @@ int mesh_volume(Context* ctx, int id, int float_bounds, float* tris, long long c
   MF_CUDA(cudaMemcpyAsync(d_slots, slots.data(), sizeof(int) * nb, cudaMemcpyHostToDevice,
                           ctx->stream));
   MeshArgs a;
+  a.tris = ctx->d_mc_tris;
   a.pool = ctx->pool;
   a.V = V;
   a.slots = d_slots;

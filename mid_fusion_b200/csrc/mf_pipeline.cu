@@ -141,9 +141,8 @@ int process_frame(Context* ctx, bool labels) {
 //     mask is refined with result rows (Object::refine_mask_use_motion): the
 //     background and the static objects with the camera's rows (the motion
 //     residuals of step 3 when objects move, else the rows of the camera's
-//     last GN iteration, :282, :396-400), a moving object with the rows of
-//     its own last GN iteration (:404-405; the reference recomputes them at
-//     the object's final pose, :446-466, which this library does not);
+//     last GN iteration, :282, :396-400), a moving object with its rows
+//     recomputed at its virtual camera pose against its own maps (:446-466);
 //  5. every instance is integrated with its mask, the composite raycast
 //     replaces the model maps and the frame becomes the reference.
 // The first frame (no reference yet) is integrated and raycast untracked.
@@ -189,7 +188,7 @@ int process_frame_motion(Context* ctx, float thr, float moved, uint32_t* moving_
     for (int i = 0; i < n; ++i) {
       const int8_t* rows = rows0;
       if (is_moving[i]) {
-        if (int rc = track_results(ctx, i, obj_rows, nullptr, nullptr)) return rc;
+        if (int rc = object_residuals(ctx, i, thr, obj_rows, nullptr)) return rc;
         rows = obj_rows;
       }
       if (int rc = refine_mask_use_motion(ctx, i, rows, ctx->cfg.use_icp, ctx->cfg.use_rgb))

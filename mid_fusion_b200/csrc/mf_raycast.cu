@@ -159,11 +159,15 @@ __device__ __forceinline__ bool ray_misses_blocks(const Volume& V, const int* bo
 }
 
 // raycast(const Volume<SDF>&, origin, direction, ...),
-// apps/kfusion/src/cpp/kfusion/rendering_impl.hpp:80-140.
+// apps/kfusion/src/cpp/kfusion/rendering_impl.hpp:80-140.  With TC, *tc gets
+// the march parameter t of the sample at which the crossing was found
+// (+infinity when the march finds none).
+template <bool TC = false>
 __device__ __noinline__ F4 raycast_volume(const Pool& P, const Volume& V, F3 origin,
                                           F3 direction,
                              float nearPlane, float farPlane, float mu, float step,
-                             float largestep) {
+                             float largestep, float* tc = nullptr) {
+  if (TC) *tc = INFINITY;
   const F3 invR = mk3(1.0f / direction.x, 1.0f / direction.y, 1.0f / direction.z);
   const F3 tbot = (-1.f * invR) * origin;
   const F3 ttop = invR * (V.dim - origin);
@@ -194,6 +198,7 @@ __device__ __noinline__ F4 raycast_volume(const Pool& P, const Volume& V, F3 ori
         f_t = f_tt;
       }
       if (f_tt < 0) {
+        if (TC) *tc = t;
         t = t + stepsize * f_tt / (f_t - f_tt);
         const F3 p = origin + direction * t;
         return F4{p.x, p.y, p.z, t};
@@ -283,7 +288,274 @@ raycast_objects_kernel(Pool pool, const Volume* __restrict__ vols,
   }
 }
 
-int profile_raycast(Context* ctx, int reps, double* us) {
+// ------------------------------------------------------------------------
+// Phased composite raycast: the same maps as raycast_objects_kernel, in two
+// launches.
+//  1. raycast_hits_kernel (grid.z = instance): every instance's ray of every
+//     pixel, traversed and marched up to the far plane, not to the running
+//     nearest hit: the hit (x, y, z, t), the march parameter tc of the sample
+//     at which the crossing was found (+inf: none) and the foreground value at
+//     the hit.  The warps of a CTA all work on one instance.
+//  2. raycast_fold_kernel: per pixel, the reference's composite over the
+//     instances in list order.  The reference bounds instance o's traversal
+//     and march by nfar = min(nearest, far) (rendering.cpp:47-62): with the
+//     same start and the same steps, the bounded march finds the unbounded
+//     march's crossing exactly when that crossing's sample lies before nfar
+//     (tc < nfar), and otherwise returns the zero hit, whose foreground is
+//     read at the volume origin.  The fold applies that rule, then the
+//     nearest-hit / foreground / tie tests, and computes the gradient of the
+//     final winner only.
+// The bounded traversal reaches the same first block as the unbounded one
+// whenever the march's crossing lies before nfar (the block's entry and all
+// its ancestors' lie before the crossing); the maps equal the one-kernel
+// path's bit for bit (autotuner identity test).
+struct RayRec {
+  F4* hit;      // [o * W * H + p]
+  float2* tf;   // (tc, foreground at the hit)
+};
+
+template <int TW>
+__global__ void __launch_bounds__(128)
+raycast_hits_kernel(Pool pool, const Volume* __restrict__ vols,
+                    const InstFrame* __restrict__ frames, IdList ids, RayArgs a, RayRec rec,
+                    int* __restrict__ status) {
+  const int x = blockIdx.x * TW + (threadIdx.x % TW);
+  const int y = blockIdx.y * (128 / TW) + (threadIdx.x / TW);
+  if (x >= a.W || y >= a.H) return;
+  const int o = blockIdx.z;
+  const int i = ids.v[o];
+  const Volume& V = vols[i];
+  const InstFrame& F = frames[i];
+  const int p = x + y * a.W;
+  const M4 view = frames[ids.v[0]].view;
+  const F3 w_dir = rotate(view, mk3((float)x, (float)y, 1.f));
+  const float step = V.dim / V.size;
+  const F3 o_dir = normalize(rotate(F.inv_T_w_o, w_dir));
+  const float t_min =
+      ray_misses_blocks(V, V.bbox, F.o_origin, o_dir, a.nearPlane, a.farPlane, a.epsilon)
+          ? -1.f
+          : ray_first_block(V, F.o_origin, o_dir, a.nearPlane, a.farPlane, a.epsilon, status);
+  F4 hit = F4{0, 0, 0, 0};
+  float tc = INFINITY, fg = 0.f;
+  if (t_min > 0.f) {
+    hit = raycast_volume<true>(pool, V, F.o_origin, o_dir, t_min * V.dim / (unsigned)V.size,
+                               a.farPlane, a.mu, step, step * 8, &tc);
+    if (tc < INFINITY) fg = volume_interp(pool, V, mk3(hit.x, hit.y, hit.z), 1);
+  }
+  const size_t q = (size_t)o * a.W * a.H + p;
+  rec.hit[q] = hit;
+  rec.tf[q] = make_float2(tc, fg);
+}
+
+template <int TW>
+__global__ void __launch_bounds__(128)
+raycast_fold_kernel(Pool pool, const Volume* __restrict__ vols,
+                    const InstFrame* __restrict__ frames, IdList ids, RayArgs a, RayRec rec) {
+  const int x = blockIdx.x * TW + (threadIdx.x % TW);
+  const int y = blockIdx.y * (128 / TW) + (threadIdx.x / TW);
+  __shared__ int s_slot[8 * 128];
+  __shared__ float s_fg0[MAX_INSTANCES];
+  for (int o = threadIdx.x; o < ids.n; o += blockDim.x)
+    s_fg0[o] = volume_interp(pool, vols[ids.v[o]], mk3(0.f, 0.f, 0.f), 1);
+  __syncthreads();
+  if (x >= a.W || y >= a.H) return;
+  const int p = x + y * a.W;
+  const size_t WH = (size_t)a.W * a.H;
+  const float INVALID = -2;
+  float nearest = 1.0e3f;
+  double high_fg = 0.f;
+  int miss = 0;
+  unsigned winners = 0;   // every instance that became the running winner
+  unsigned zeroh = 0;     // ... with the zero hit of a march bounded before its crossing
+  int win = -1;
+  F4 win_hit = F4{0, 0, 0, 0};
+  for (int o = 0; o < ids.n; ++o) {
+    const InstFrame& F = frames[ids.v[o]];
+    const float nfar = fmn(nearest, a.farPlane);
+    const float2 tf = rec.tf[o * WH + p];
+    F4 hit = F4{0, 0, 0, 0};
+    double fg = s_fg0[o];
+    const bool crossed = tf.x < nfar;
+    if (crossed) {
+      hit = rec.hit[o * WH + p];
+      fg = tf.y;
+    }
+    const float hd = F.label == 0 ? hit.w + 0.05f : hit.w;
+    if (hd > nearest) { miss++; continue; }
+    if (fg <= 0.5f) { miss++; continue; }
+    if (hd == nearest) {
+      if (!(fg > high_fg)) { miss++; continue; }
+    } else if (hd < nearest) {
+      nearest = hd;
+    } else {
+      miss++;
+      continue;
+    }
+    high_fg = fg;
+    winners |= 1u << o;
+    if (!crossed) zeroh |= 1u << o;
+    win = o;
+    win_hit = hit;
+  }
+  if (win < 0) {
+    if (miss == ids.n) {
+      a.vertex[p] = mk3(0.f);
+      a.normal[p] = mk3(INVALID, 0, 0);
+      a.label[p] = (int)INVALID;
+    }
+    return;
+  }
+  const InstFrame& F = frames[ids.v[win]];
+  a.label[p] = F.label;
+  a.vertex[p] = xform(F.T_w_o, mk3(win_hit.x, win_hit.y, win_hit.z));
+  const F3 gn = volume_grad(pool, vols[ids.v[win]], mk3(win_hit.x, win_hit.y, win_hit.z),
+                            s_slot + threadIdx.x, 128);
+  if (length(gn) != 0) {
+    a.normal[p] = normalize(rotate(F.T_w_o, gn));
+    return;
+  }
+  // a zero gradient writes only the normal's x (rendering.cpp:105-107, 126-128):
+  // y and z are those of the latest earlier winner with a nonzero gradient, as
+  // the reference's successive writes leave them, or the map's previous values
+  a.normal[p].x = INVALID;
+  for (int o = win - 1; o >= 0; --o) {
+    if (!(winners & (1u << o))) continue;
+    const InstFrame& Fo = frames[ids.v[o]];
+    const F4 hit = (zeroh & (1u << o)) ? F4{0, 0, 0, 0} : rec.hit[o * WH + p];
+    const F3 g2 = volume_grad(pool, vols[ids.v[o]], mk3(hit.x, hit.y, hit.z),
+                              s_slot + threadIdx.x, 128);
+    if (length(g2) != 0) {
+      const F3 n2 = normalize(rotate(Fo.T_w_o, g2));
+      a.normal[p].y = n2.y;
+      a.normal[p].z = n2.z;
+      return;
+    }
+  }
+}
+
+// Algorithmic bytes of one composite raycast (the per-unit figures of the
+// raycast's roofline): the same march as raycast_objects_kernel, counting
+// instead of writing.  Per ray and instance: 8 B for every voxel read of the
+// march (tsdf + weight of Volume::get), 32 B for every trilinear TSDF
+// interpolation (8 taps), 64 B for the foreground interpolation of a
+// candidate hit (8 FP64 taps) and 192 B for its gradient (48 voxel reads);
+// per pixel 28 B of output (vertex, normal, label).  Counted on the device
+// after the timed launches (profile_raycast), never inside a frame.
+__device__ __noinline__ void march_count(const Pool& P, const Volume& V, F3 origin, F3 direction,
+                                         float nearPlane, float farPlane, float mu, float step,
+                                         float largestep, unsigned long long* cnt, F4* out) {
+  const F3 invR = mk3(1.0f / direction.x, 1.0f / direction.y, 1.0f / direction.z);
+  const F3 tbot = (-1.f * invR) * origin;
+  const F3 ttop = invR * (V.dim - origin);
+  const F3 tmin = mk3(fmn(ttop.x, tbot.x), fmn(ttop.y, tbot.y), fmn(ttop.z, tbot.z));
+  const F3 tmax = mk3(fmx(ttop.x, tbot.x), fmx(ttop.y, tbot.y), fmx(ttop.z, tbot.z));
+  const float largest_tmin = fmx(fmx(tmin.x, tmin.y), fmx(tmin.x, tmin.z));
+  const float smallest_tmax = fmn(fmn(tmax.x, tmax.y), fmn(tmax.x, tmax.z));
+  const float tnear = fmx(largest_tmin, nearPlane);
+  const float tfar = fmn(smallest_tmax, farPlane);
+  const float inv = V.size / V.dim;
+  unsigned long long samples = 0, interps = 0;
+  *out = F4{0, 0, 0, 0};
+  if (tnear < tfar) {
+    BlockMemo memo;
+    float t = tnear, stepsize = largestep;
+    F3 position = origin + direction * t;
+    float f_t = volume_interp_m<0>(P, V, position, memo), f_tt = 0;
+    ++interps;
+    if (f_t > 0) {
+      for (int guard = 0; t < tfar && guard < (1 << 20); t += stepsize, ++guard) {
+        const I3 s = to_i3(mk3(position.x * inv, position.y * inv, position.z * inv));
+        f_tt = tsdf_at_m(P, V, memo, s.x, s.y, s.z);
+        ++samples;
+        if (f_tt < 0.1f && f_tt >= -0.5f) {
+          f_tt = volume_interp_m<0>(P, V, position, memo);
+          ++interps;
+        }
+        if (f_tt < 0) break;
+        stepsize = fmx(f_tt * mu, step);
+        position = position + stepsize * direction;
+        f_t = f_tt;
+      }
+      if (f_tt < 0) {
+        t = t + stepsize * f_tt / (f_t - f_tt);
+        const F3 p = origin + direction * t;
+        *out = F4{p.x, p.y, p.z, t};
+      }
+    }
+  }
+  cnt[0] += samples;
+  cnt[1] += interps;
+}
+
+__global__ void raycast_count_kernel(Pool pool, const Volume* __restrict__ vols,
+                                     const InstFrame* __restrict__ frames, IdList ids, RayArgs a,
+                                     int* __restrict__ status,
+                                     unsigned long long* __restrict__ totals) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+  unsigned long long c[4] = {0, 0, 0, 0};  // samples, interps, fg reads, gradients
+  if (x < a.W) {
+    float nearest = 1.0e3f;
+    double high_fg = 0.f;
+    const M4 view = frames[ids.v[0]].view;
+    const F3 w_dir = rotate(view, mk3((float)x, (float)y, 1.f));
+    for (int o = 0; o < ids.n; ++o) {
+      const int i = ids.v[o];
+      const Volume& V = vols[i];
+      const InstFrame& F = frames[i];
+      const float step = V.dim / V.size;
+      const F3 o_dir = normalize(rotate(F.inv_T_w_o, w_dir));
+      const float nfar = fmn(nearest, a.farPlane);
+      const float t_min = ray_first_block(V, F.o_origin, o_dir, a.nearPlane, nfar, a.epsilon,
+                                          status);
+      F4 hit = F4{0, 0, 0, 0};
+      if (t_min > 0.f)
+        march_count(pool, V, F.o_origin, o_dir, t_min * V.dim / (unsigned)V.size, nfar, a.mu,
+                    step, step * 8, c, &hit);
+      const float hd = F.label == 0 ? hit.w + 0.05f : hit.w;
+      if (hd > nearest) continue;
+      const double fg = volume_interp(pool, V, mk3(hit.x, hit.y, hit.z), 1);
+      ++c[2];
+      if (fg <= 0.5f) continue;
+      if (hd == nearest) {
+        if (!(fg > high_fg)) continue;
+      } else if (hd < nearest) {
+        nearest = hd;
+      } else {
+        continue;
+      }
+      high_fg = fg;
+      ++c[3];
+    }
+  }
+  for (int k = 0; k < 4; ++k) {
+    unsigned long long v = c[k];
+    for (int off = 16; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if ((threadIdx.x & 31) == 0) atomicAdd(totals + k, v);
+  }
+}
+
+static int count_raycast_bytes(Context* ctx, const IdList& ids, double* bytes) {
+  const mf_config& c = ctx->cfg;
+  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H, c.near_plane,
+            c.far_plane, c.mu, ctx->ray_epsilon};
+  unsigned long long* d = nullptr;
+  MF_CUDA(cudaMalloc(&d, 4 * sizeof(unsigned long long)));
+  cudaMemsetAsync(d, 0, 4 * sizeof(unsigned long long), ctx->stream);
+  raycast_count_kernel<<<dim3((ctx->W + 127) / 128, ctx->H), 128, 0, ctx->stream>>>(
+      ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, ctx->d_status, d);
+  unsigned long long h[4] = {0, 0, 0, 0};
+  cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    ctx->last_error = std::string("raycast byte count: ") + cudaGetErrorString(e);
+    return MF_E_CUDA;
+  }
+  *bytes = 8.0 * h[0] + 32.0 * h[1] + 64.0 * h[2] + 192.0 * h[3] + 28.0 * ctx->W * ctx->H;
+  return MF_OK;
+}
+
+int profile_raycast(Context* ctx, int reps, double* us, double* bytes) {
   IdList all;
   all.n = (int)ctx->inst.size();
   for (int i = 0; i < all.n; ++i) all.v[i] = i;
@@ -301,25 +573,39 @@ int profile_raycast(Context* ctx, int reps, double* us) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   *us = 1e3 * ms / reps;
-  return MF_OK;
+  return bytes ? count_raycast_bytes(ctx, all, bytes) : MF_OK;
 }
 
 int stage_raycast(Context* ctx, const IdList& ids, float epsilon) {
   return stage_raycast_to(ctx, ids, epsilon, ctx->d_vertex, ctx->d_normal, ctx->d_label);
 }
 
-// Launch-shape candidates of raycast_objects_kernel: tile width x register
-// bound.  Entry 0 is the default.
+// Launch-shape candidates of the composite raycast: the one-kernel path
+// (raycast_objects_kernel) by tile width x register bound, and the phased path
+// (raycast_hits_kernel + raycast_fold_kernel) by tile width.  Entry 0 is the
+// default.
+using RayFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, int*);
+using HitsFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, RayRec, int*);
+using FoldFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, RayRec);
 struct RayVariant {
   int tw, minb;
-  void (*fn)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, int*);
+  RayFn fn;        // one kernel, or nullptr for the phased path
+  HitsFn hits;
+  FoldFn fold;
 };
 static const RayVariant ray_variants[] = {
-    {16, 1, raycast_objects_kernel<16, 1>}, {32, 1, raycast_objects_kernel<32, 1>},
-    {8, 1, raycast_objects_kernel<8, 1>},   {16, 6, raycast_objects_kernel<16, 6>},
-    {32, 6, raycast_objects_kernel<32, 6>}, {8, 6, raycast_objects_kernel<8, 6>},
-    {16, 8, raycast_objects_kernel<16, 8>}, {32, 8, raycast_objects_kernel<32, 8>},
-    {8, 8, raycast_objects_kernel<8, 8>},
+    {16, 1, raycast_objects_kernel<16, 1>, nullptr, nullptr},
+    {32, 1, raycast_objects_kernel<32, 1>, nullptr, nullptr},
+    {8, 1, raycast_objects_kernel<8, 1>, nullptr, nullptr},
+    {16, 6, raycast_objects_kernel<16, 6>, nullptr, nullptr},
+    {32, 6, raycast_objects_kernel<32, 6>, nullptr, nullptr},
+    {8, 6, raycast_objects_kernel<8, 6>, nullptr, nullptr},
+    {16, 8, raycast_objects_kernel<16, 8>, nullptr, nullptr},
+    {32, 8, raycast_objects_kernel<32, 8>, nullptr, nullptr},
+    {8, 8, raycast_objects_kernel<8, 8>, nullptr, nullptr},
+    {16, 0, nullptr, raycast_hits_kernel<16>, raycast_fold_kernel<16>},
+    {32, 0, nullptr, raycast_hits_kernel<32>, raycast_fold_kernel<32>},
+    {8, 0, nullptr, raycast_hits_kernel<8>, raycast_fold_kernel<8>},
 };
 constexpr int N_RAY_VARIANTS = (int)(sizeof(ray_variants) / sizeof(ray_variants[0]));
 static_assert(N_RAY_VARIANTS <= MAX_TUNE_VARIANTS, "raycast candidate table too long");
@@ -328,7 +614,10 @@ int ray_variant_count() { return N_RAY_VARIANTS; }
 
 void ray_variant_describe(int v, char* buf, int cap) {
   const RayVariant& r = ray_variants[v];
-  if (r.minb > 1)
+  if (!r.fn)
+    snprintf(buf, cap, "raycast phased (per-instance hits, then the composite fold), tile %dx%d",
+             r.tw, 128 / r.tw);
+  else if (r.minb > 1)
     snprintf(buf, cap, "raycast tile %dx%d, registers bounded for %d CTAs/SM", r.tw, 128 / r.tw,
              r.minb);
   else
@@ -343,8 +632,16 @@ int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex,
   const RayVariant& r = ray_variants[ctx->tune.ray];
   const int th = 128 / r.tw;
   dim3 grid((ctx->W + r.tw - 1) / r.tw, (ctx->H + th - 1) / th);
-  r.fn<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a,
-                                      ctx->d_status);
+  if (r.fn) {
+    r.fn<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a,
+                                        ctx->d_status);
+  } else {
+    if (ids.n > ctx->cfg.max_instances) return MF_E_ARG;
+    const RayRec rec{ctx->d_rayhit, ctx->d_raytf};
+    r.hits<<<dim3(grid.x, grid.y, ids.n), 128, 0, ctx->stream>>>(
+        ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec, ctx->d_status);
+    r.fold<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec);
+  }
   MF_CUDA(cudaGetLastError());
   return MF_OK;
 }

@@ -59,6 +59,8 @@ struct GNState {
   M4 evalTf;         // the pose of the last GN evaluation (Tf when gn_step ran)
   M4 T_w_r, inv_T_w_r, view;               // camera: reference pose, K * inverse(T_w_r)
   M4 T_c1_o1, inv_T_c1_o1, inv_T_w_o1, T_w_c2;  // object constants
+  M4 T_w_o1;         // object: the volume pose before this frame's tracking
+  M4 T_virtual;      // object: virtual camera pose T_w_o1 inverse(T_c2_o2) after tracking
   double sums[MAX_PYR][32];
 };
 
@@ -84,6 +86,8 @@ struct TrackState {
   F3* rV[MAX_INSTANCES][MAX_PYR] = {};
   GNState* d_state = nullptr;       // MAX_INSTANCES (slot 0: camera, slot i: object i)
   int slot_kind[MAX_INSTANCES];     // per slot: -1 never set up, else the GNState kind
+  unsigned* d_gnbar = nullptr;      // 2 x MAX_PYR grid-barrier counters (camera, objects)
+  int coop_blocks[2] = {0, 0};      // co-resident CTAs of gn_level_kernel<0> / <1>
   double* d_partials = nullptr;     // MAX_INSTANCES x max_tiles x 32
   int max_tiles = 0;
   float2* d_zr = nullptr;           // MAX_PYR x max_tiles live depth range per CTA tile
@@ -350,6 +354,7 @@ __global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __r
   S.T_c1_o1 = mul(S.inv_T_w_r, T_wo1);
   S.inv_T_c1_o1 = inverse(S.T_c1_o1);
   S.inv_T_w_o1 = inverse(T_wo1);
+  S.T_w_o1 = T_wo1;
   const M4 T0 = mul(inverse(T_w_c2), T_wo1);
   for (int i = 0; i < 16; ++i) {
     S.T[i] = (double)m_at(T0, i / 4, i % 4);
@@ -365,11 +370,15 @@ __global__ void finalize_camera_kernel(const GNState* st, float* __restrict__ Tw
 }
 
 // volume_pose_ = T_w_c2 * T_c2_o2, tracking.cpp:695.
-__global__ void finalize_objects_kernel(const GNState* st, IdList slots, float* __restrict__ Two) {
+// trackEachObject's outputs, tracking.cpp:695-696: the volume pose
+// T_w_c2 T_c2_o2 and the virtual camera pose T_w_o1 inverse(T_c2_o2).
+__global__ void finalize_objects_kernel(GNState* st, IdList slots, float* __restrict__ Two) {
   const int t = threadIdx.x;
   if (t >= slots.n) return;
   const int s = slots.v[t];
-  store_m4(Two + 16 * s, mul(st[s].T_w_c2, to_m4f(st[s].T)));
+  const M4 Tco = to_m4f(st[s].T);
+  store_m4(Two + 16 * s, mul(st[s].T_w_c2, Tco));
+  st[s].T_virtual = mul(st[s].T_w_o1, inverse(Tco));
 }
 
 // ------------------------------------------------------------------ GN step
@@ -783,30 +792,27 @@ __device__ __forceinline__ double warp_sum_fp64(const float* acc, const int* cnt
   return v;
 }
 
-// KIND 0: the camera problem; KIND 1: object problems (one instantiation each
-// keeps the kernel's code small).
+// The FP64 sums of one tile (CTA) of a problem at level L: every thread
+// evaluates the ICP and photometric rows of its pixels, weights them and
+// accumulates in FP32 (at most 6 rows per thread); the sums are FP64 from the
+// warp level up, in a fixed order.  Thread i < 32 returns sum i (29 sums, then
+// the 3 counts).  Object problems skip a tile that cannot hold a valid row.
 template <int KIND>
-__global__ void __launch_bounds__(GN_THREADS, MF_GN_MINB)
-gn_iter_kernel(GNArgs a, IdList slots, int L) {
-  const int s = slots.v[blockIdx.y];
-  GNState& S = a.st[s];
-  if (S.done && !a.first_iter) return;
+__device__ __forceinline__ double gn_tile_sums(const GNArgs& a, const GNState& S, int s, int L,
+                                               int tile, double (*sh)[32],
+                                               float (*red)[32][33]) {
   const int w = a.pyr.w[L], h = a.pyr.h[L];
   const int n = w * h;
-  // object problems: a tile that cannot hold a valid row skips its pixels
   bool live = true;
   if (KIND == 1) {
     __shared__ int s_live;
     if (threadIdx.x < 32) {
-      const bool lv = object_tile_live(a, S, L, blockIdx.x, w, n);
+      const bool lv = object_tile_live(a, S, L, tile, w, n);
       if (threadIdx.x == 0) s_live = lv ? 1 : 0;
     }
     __syncthreads();
     live = s_live != 0;
   }
-  // FP64 from the warp level up
-  __shared__ double sh[GN_THREADS / 32][32];
-  __shared__ float red[GN_THREADS / 32][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (live) {
     float acc[29];
@@ -817,7 +823,7 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
     const int ppt = gn_pix(L);
 #pragma unroll 1
     for (int k = 0; k < ppt; ++k) {
-      const int p = blockIdx.x * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
+      const int p = tile * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
       if (p >= n) break;
       Row r;
       if (a.use_icp) {
@@ -837,11 +843,63 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
     sh[warp][lane] = 0.0;
   }
   __syncthreads();
-  __shared__ bool last;
+  double v = 0;
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int wi = 0; wi < GN_THREADS / 32; ++wi) v += sh[wi][threadIdx.x];
+  }
+  return v;
+}
+
+// The 32 sums of a problem over its `ntiles` tile partials, in a fixed order,
+// by the whole CTA (the last CTA of the problem): tot[i] = sum i.  The loads
+// of 16 tiles are issued before their in-order additions, so the tail waits on
+// about ntiles / 128 L2 round trips instead of ntiles / 64.
+__device__ __forceinline__ void gn_tail_sums(const GNArgs& a, int s, int ntiles,
+                                             double (*sh)[32], double* tot) {
+  constexpr int G = GN_THREADS / 32, U = 16;
+  {
+    const int i = threadIdx.x & 31, g = threadIdx.x >> 5;  // 8 groups of tiles
+    const double* col = a.partials + (size_t)s * a.max_tiles * 32 + i;
+    double v = 0;
+    int b = g;
+    for (; b + (U - 1) * G < ntiles; b += U * G) {
+      double t[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) t[u] = __ldcg(col + (size_t)(b + u * G) * 32);
+#pragma unroll
+      for (int u = 0; u < U; ++u) v += t[u];
+    }
+    for (; b < ntiles; b += G) v += __ldcg(col + (size_t)b * 32);
+    sh[g][i] = v;
+  }
+  __syncthreads();
   if (threadIdx.x < 32) {
     double v = 0;
 #pragma unroll
-    for (int wi = 0; wi < GN_THREADS / 32; ++wi) v += sh[wi][threadIdx.x];
+    for (int g = 0; g < G; ++g) v += sh[g][threadIdx.x];
+    tot[threadIdx.x] = v;
+  }
+  __syncthreads();
+}
+
+// One GN iteration of every problem in `slots` (grid.y = problem): the rows of
+// every tile, the tile partials, and in the CTA that finishes last for a
+// problem (ticket counter) the sum over the tiles and, with device_step, the
+// problem's GN step on the device.
+// KIND 0: the camera problem; KIND 1: object problems (one instantiation each
+// keeps the kernel's code small).
+template <int KIND>
+__global__ void __launch_bounds__(GN_THREADS, MF_GN_MINB)
+gn_iter_kernel(GNArgs a, IdList slots, int L) {
+  const int s = slots.v[blockIdx.y];
+  GNState& S = a.st[s];
+  if (S.done && !a.first_iter) return;
+  __shared__ double sh[GN_THREADS / 32][32];
+  __shared__ float red[GN_THREADS / 32][32][33];
+  const double v = gn_tile_sums<KIND>(a, S, s, L, blockIdx.x, sh, red);
+  __shared__ bool last;
+  if (threadIdx.x < 32) {
     a.partials[((size_t)s * a.max_tiles + blockIdx.x) * 32 + threadIdx.x] = v;
     __threadfence();
   }
@@ -853,41 +911,118 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // last block: sum the block partials in a fixed order with all threads;
-  // the loads of 16 tiles are issued before their in-order additions, so the
-  // tail waits on about n / 128 L2 round trips instead of n / 64
-  {
-    constexpr int G = GN_THREADS / 32, U = 16;
-    const int i = threadIdx.x & 31, g = threadIdx.x >> 5;  // 8 groups of tiles
-    const double* col = a.partials + (size_t)s * a.max_tiles * 32 + i;
-    double v = 0;
-    int b = g;
-    for (; b + (U - 1) * G < (int)gridDim.x; b += U * G) {
-      double t[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) t[u] = __ldcg(col + (size_t)(b + u * G) * 32);
-#pragma unroll
-      for (int u = 0; u < U; ++u) v += t[u];
-    }
-    for (; b < (int)gridDim.x; b += G) v += __ldcg(col + (size_t)b * 32);
-    sh[g][i] = v;
-  }
-  __syncthreads();
   __shared__ double tot[32];
-  if (threadIdx.x < 32) {
-    double v = 0;
-#pragma unroll
-    for (int g = 0; g < GN_THREADS / 32; ++g) v += sh[g][threadIdx.x];
-    tot[threadIdx.x] = v;
-    S.sums[L][threadIdx.x] = v;
-  }
-  __syncthreads();
+  gn_tail_sums(a, s, (int)gridDim.x, sh, tot);
+  if (threadIdx.x < 32) S.sums[L][threadIdx.x] = tot[threadIdx.x];
   if (threadIdx.x == 0) {
     S.ticket = 0;
     if (a.device_step) {
       if (a.first_iter) S.prev_err = INFINITY;
       gn_step_dev(S, tot, L);
     }
+  }
+}
+
+// ------------------------------------------------------------------ persistent level
+// All GN iterations of one pyramid level for every problem in `slots`, in one
+// cooperative launch (every CTA resident): the (problem, tile) items of an
+// iteration are spread over the grid, the CTA that finishes a problem's last
+// tile sums its partials and runs its step (as gn_iter_kernel does), and a
+// grid barrier separates the iterations.  After each barrier the CTAs read the
+// problems' `done` flags; when every problem has stopped, the level ends
+// without launching the remaining iterations.  The per-pixel rows, the tile
+// partials, their sum and the step are gn_iter_kernel's, so the poses equal
+// the per-iteration launches' bit for bit.
+// Every wait is bounded: a barrier that does not complete within
+// GN_BAR_SPINS polls sets MF_STATUS_GN_TIMEOUT and the CTA returns.
+constexpr unsigned GN_BAR_SPINS = 1u << 22;   // x >= 64 ns sleeps: about 0.3 s
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// GNState copied between global memory (through L2: other SMs write it within
+// the launch) and shared memory, by the whole CTA.
+__device__ __forceinline__ void state_load(const GNState* g, GNState* sm) {
+  static_assert(sizeof(GNState) % 4 == 0, "GNState is copied as words");
+  const int* src = reinterpret_cast<const int*>(g);
+  int* dst = reinterpret_cast<int*>(sm);
+  for (int i = threadIdx.x; i < (int)(sizeof(GNState) / 4); i += blockDim.x) dst[i] = __ldcg(src + i);
+  __syncthreads();
+}
+__device__ __forceinline__ void state_store(const GNState* sm, GNState* g) {
+  const int* src = reinterpret_cast<const int*>(sm);
+  int* dst = reinterpret_cast<int*>(g);
+  for (int i = threadIdx.x; i < (int)(sizeof(GNState) / 4); i += blockDim.x) __stcg(dst + i, src[i]);
+  __threadfence();
+  __syncthreads();
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(GN_THREADS, MF_GN_MINB)
+gn_level_kernel(GNArgs a, IdList slots, int L, int iters, int ntiles, unsigned* __restrict__ bar,
+                int* __restrict__ status) {
+  __shared__ GNState sS;
+  __shared__ double sh[GN_THREADS / 32][32];
+  __shared__ float red[GN_THREADS / 32][32][33];
+  __shared__ double tot[32];
+  __shared__ int s_flag;
+  const int items = slots.n * ntiles;
+  for (int it = 0; it < iters; ++it) {
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+      const int pi = item / ntiles, tile = item - pi * ntiles;
+      const int s = slots.v[pi];
+      state_load(a.st + s, &sS);
+      // a stopped problem runs again in the level's first iteration (the
+      // level's reset, tracking.cpp:247-249, 624-627)
+      if (sS.done && it > 0) continue;
+      const double v = gn_tile_sums<KIND>(a, sS, s, L, tile, sh, red);
+      if (threadIdx.x < 32) {
+        a.partials[((size_t)s * a.max_tiles + tile) * 32 + threadIdx.x] = v;
+        __threadfence();
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) s_flag = atomicAdd(&a.st[s].ticket, 1) == ntiles - 1;
+      __syncthreads();
+      if (!s_flag) continue;
+      __threadfence();
+      gn_tail_sums(a, s, ntiles, sh, tot);
+      if (threadIdx.x < 32) sS.sums[L][threadIdx.x] = tot[threadIdx.x];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        sS.ticket = 0;
+        if (it == 0) sS.prev_err = INFINITY;
+        gn_step_dev(sS, tot, L);
+      }
+      __syncthreads();
+      state_store(&sS, a.st + s);
+    }
+    // grid barrier; then every CTA reads the same `done` flags
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(bar, 1u);
+      const unsigned target = (unsigned)(it + 1) * gridDim.x;
+      int flag = 0;
+      for (unsigned spins = 0; ld_acquire_u32(bar) < target; ++spins) {
+        if (spins >= GN_BAR_SPINS) {
+          atomicOr(status, MF_STATUS_GN_TIMEOUT);
+          flag = -1;
+          break;
+        }
+        __nanosleep(64);
+      }
+      if (flag == 0) {
+        int all = 1;
+        for (int i = 0; i < slots.n; ++i) all &= __ldcg(&a.st[slots.v[i]].done) != 0;
+        flag = all;
+      }
+      s_flag = flag;
+    }
+    __syncthreads();
+    if (s_flag != 0) return;
   }
 }
 
@@ -941,6 +1076,17 @@ int track_init(Context* ctx) {
   if (talloc(ctx, &ts->d_zr, (size_t)MAX_PYR * ts->max_tiles)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_Twc_prev, 16)) return MF_E_CUDA;
   if (talloc(ctx, &ts->d_mask0, (size_t)ctx->W * ctx->H)) return MF_E_CUDA;
+  if (talloc(ctx, &ts->d_gnbar, 2 * MAX_PYR)) return MF_E_CUDA;
+  // the persistent GN launch needs every CTA resident: its grid is at most
+  // the SM count times the CTAs one SM holds
+  {
+    int sms = 0, b0 = 0, b1 = 0;
+    MF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    MF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, gn_level_kernel<0>, GN_THREADS, 0));
+    MF_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, gn_level_kernel<1>, GN_THREADS, 0));
+    ts->coop_blocks[0] = sms * b0;
+    ts->coop_blocks[1] = sms * b1;
+  }
   // Tracking::Tracking, tracking.cpp:77-84: gaussian[i] = expf(-(x*x) / (2 delta^2)),
   // x = i - 2, delta = 4 (computed on the host exactly as the reference does).
   for (int i = 0; i < 5; ++i) {
@@ -1148,13 +1294,51 @@ static int tile_depth_range(Context* ctx) {
 }
 
 // Coarse-to-fine GN of every problem in `slots`, all on the device
-// (trackLiveFrame :240-335 / trackEachObject :629-694).
+// (trackLiveFrame :240-335 / trackEachObject :629-694): one cooperative
+// launch per level (gn_level_kernel), or, with gn_persistent off, one launch
+// per iteration (gn_iter_kernel); both give the same poses bit for bit.
+template <int KIND>
+static cudaError_t launch_gn_level(const GNArgs& a, const IdList& slots, int L, int iters,
+                                   int ntiles, unsigned* bar, int* status, int grid,
+                                   cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(GN_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, gn_level_kernel<KIND>, a, slots, L, iters, ntiles, bar,
+                            status);
+}
+
 static int gn_device(Context* ctx, const IdList& slots, int kind) {
   TrackState& T = *ctx->track;
+  const bool persistent = ctx->gn_persistent && T.coop_blocks[kind] > 0;
+  unsigned* bar = T.d_gnbar + kind * MAX_PYR;
+  if (persistent) MF_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned) * MAX_PYR, ctx->stream));
   for (int L = T.levels - 1; L >= 0; --L) {
     GNArgs a = make_args(ctx, L, 1);
     const int tiles = div_up((long long)T.pyr.w[L] * T.pyr.h[L], GN_THREADS * gn_pix(L));
-    for (int it = 0; it < ctx->cfg.gn_iterations[L]; ++it) {
+    const int iters = ctx->cfg.gn_iterations[L];
+    if (persistent) {
+      if (iters <= 0) continue;
+      const int grid = std::min(tiles * slots.n, T.coop_blocks[kind]);
+      const cudaError_t e =
+          kind == 0 ? launch_gn_level<0>(a, slots, L, iters, tiles, bar + L, ctx->d_status, grid,
+                                         ctx->stream)
+                    : launch_gn_level<1>(a, slots, L, iters, tiles, bar + L, ctx->d_status, grid,
+                                         ctx->stream);
+      if (e != cudaSuccess) {
+        ctx->last_error = std::string("persistent GN launch: ") + cudaGetErrorString(e);
+        return MF_E_CUDA;
+      }
+      continue;
+    }
+    for (int it = 0; it < iters; ++it) {
       a.first_iter = it == 0;  // the level's reset happens in its first iteration
       if (kind == 0) gn_iter_kernel<0><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
       else gn_iter_kernel<1><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
@@ -1801,8 +1985,12 @@ struct MotionArgs {
   PyrPtrs pyr;
   int cur, W, H;
   const F3* mvertex; const F3* mnormal;   // model maps at T_w_r
+  const int* mlabel;
   const F3* lvert;                          // model vertices raycast at T_w_l
   const int* llabel;
+  int obj_label;    // >= 0: one object's maps (its pixels of the composite maps,
+                    // m_vertex / m_normal, and of the live raycast,
+                    // m_vertex_bef_integ, rendering.cpp:152-176), no counts
   M4 T_w_l, T_w_r, inv_T_w_r, K, invK;
   float sigma_bright, threshold;
   int use_icp, use_rgb;
@@ -1835,8 +2023,9 @@ __global__ void motion_residual_kernel(MotionArgs a) {
           ri = -2;
         } else {
           const int q = (int)((unsigned)px + (unsigned)py * a.W);
-          const F3 rn = a.mnormal[q];
-          const F3 rv = a.mvertex[q];
+          const bool own = a.obj_label < 0 || a.mlabel[q] == a.obj_label;
+          const F3 rn = own ? a.mnormal[q] : mk3(INVALIDF, 0.f, 0.f);
+          const F3 rv = own ? a.mvertex[q] : mk3(0.f);
           if (rn.x == INVALIDF) {
             ri = -3;
           } else {
@@ -1857,7 +2046,7 @@ __global__ void motion_residual_kernel(MotionArgs a) {
     }
     if (a.use_rgb) {
       // rendered live vertex -> depth relative to T_w_r -> vertex
-      const F3 vl = a.lvert[p];
+      const F3 vl = (a.obj_label < 0 || a.llabel[p] == a.obj_label) ? a.lvert[p] : mk3(0.f);
       const float d = vl.z > 0.0 ? xform(a.inv_T_w_r, vl).z : 0.f;
       const F3 ref = d > 0 ? d * rotate(a.invK, mk3((float)x, (float)y, 1.f)) : mk3(0.f);
       const F3 live = a.pyr.V[a.cur][0][p];
@@ -1883,7 +2072,8 @@ __global__ void motion_residual_kernel(MotionArgs a) {
     }
   }
   a.res[p] = ri; a.res[n + p] = rr;
-  a.err[p] = ei; a.err[n + p] = er;
+  if (a.err) { a.err[p] = ei; a.err[n + p] = er; }
+  if (a.obj_label >= 0) return;
   // check_static_state: an object pixel of the live render is an inlier when
   // its rows' results are > -3
   const int l = a.llabel[p];
@@ -1907,6 +2097,10 @@ __global__ void refine_mask_kernel(float* __restrict__ mask, const int8_t* __res
   if (use_icp && (res[p] == -4 || res[p] == -6)) { mask[p] = -1; return; }
   if (use_rgb && res[n + p] < -3) mask[p] = -1;
 }
+
+// Object::static_object, object.cpp:326: classes that never move (tv 63,
+// and 69, 70)
+static bool never_moving_class(int c) { return c == 63 || c == 69 || c == 70; }
 
 int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
                      uint32_t* moving) {
@@ -1957,8 +2151,10 @@ int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
   a.H = ctx->H;
   a.mvertex = ctx->d_vertex;
   a.mnormal = ctx->d_normal;
+  a.mlabel = ctx->d_label;
   a.lvert = T.d_lvert;
   a.llabel = T.d_llabel;
+  a.obj_label = -1;
   a.T_w_l = load_m4(Tl);
   a.T_w_r = load_m4(Tr);
   a.inv_T_w_r = inverse(a.T_w_r);
@@ -1977,18 +2173,71 @@ int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
   MF_CUDA(cudaMemcpyAsync(cnt, T.d_mcount, sizeof(cnt), cudaMemcpyDeviceToHost, ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
   // kfusion.cpp:312-338: an object in view (with pixels in the live render)
-  // moves when move-out threshold 0.05 < inliers / pixels < `moved`
+  // moves when move-out threshold 0.05 < inliers / pixels < `moved` and its
+  // class is not one of the never-moving classes (Object::static_object)
   uint32_t mv = 0;
   for (int i = 0; i < (int)ctx->inst.size(); ++i) {
     const int l = ctx->inst[i].label;
     float r = -1.f;
     if (i >= 1 && l >= 1 && l < 32 && cnt[l] > 0) {
       r = static_cast<float>(cnt[32 + l]) / (cnt[l]);
-      if (r < moved && r > 0.05f) mv |= 1u << l;
+      if (r < moved && r > 0.05f && !never_moving_class(ctx->inst[i].class_id)) mv |= 1u << l;
     }
     if (ratio) ratio[i] = r;
   }
   if (moving) *moving = mv;
+  return MF_OK;
+}
+
+// kfusion.cpp:446-466: a moving object's result rows recomputed after its
+// tracking, Tracking::compute_residuals at the object's virtual camera pose
+// (tracking.cpp:696) against its own model maps (m_vertex / m_normal: its
+// pixels of the last frame's composite maps) and its pixels of the live
+// raycast (m_vertex_bef_integ, the raycast at the current camera pose and the
+// objects' new poses, i.e. the last mf_motion_residuals).  Rows (2 x W*H
+// int8) to d_rows; the virtual pose (16 floats) to T_virtual when given.
+int object_residuals(Context* ctx, int i, float threshold, int8_t* d_rows, float* T_virtual) {
+  TrackState* T = ctx->track;
+  if (!T || !T->have_ref || !T->d_mres || T->slot_kind[i] != 1) {
+    ctx->last_error = "mf_object_residuals: needs the object tracked (mf_track_objects) and "
+                      "the live raycast of mf_motion_residuals";
+    return MF_E_STATE;
+  }
+  GNState S;
+  MF_CUDA(cudaMemcpyAsync(&S, T->d_state + i, sizeof(GNState), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  float Tr[16];
+  MF_CUDA(cudaMemcpyAsync(Tr, T->d_Twc_prev, 64, cudaMemcpyDeviceToHost, ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  const mf_config& c = ctx->cfg;
+  const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
+  MotionArgs a;
+  a.pyr = T->pyr;
+  a.cur = T->cur;
+  a.W = ctx->W;
+  a.H = ctx->H;
+  a.mvertex = ctx->d_vertex;
+  a.mnormal = ctx->d_normal;
+  a.mlabel = ctx->d_label;
+  a.lvert = T->d_lvert;
+  a.llabel = T->d_llabel;
+  a.obj_label = ctx->inst[i].label;
+  a.T_w_l = S.T_virtual;
+  a.T_w_r = load_m4(Tr);
+  a.inv_T_w_r = inverse(a.T_w_r);
+  a.K = camera_matrix(k);
+  a.invK = inverse_camera_matrix(k);
+  a.sigma_bright = (float)(sqrtf(100.0f) / 255.0);  // tracking.cpp:766-772
+  a.threshold = threshold;
+  a.use_icp = c.use_icp;
+  a.use_rgb = c.use_rgb;
+  a.res = d_rows;
+  a.err = nullptr;
+  a.count = nullptr;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  motion_residual_kernel<<<div_up((long long)WH, 256), 256, 0, ctx->stream>>>(a);
+  MF_CUDA(cudaGetLastError());
+  if (T_virtual) store_m4(T_virtual, S.T_virtual);
   return MF_OK;
 }
 

@@ -64,7 +64,23 @@ bool outside(F3 p, float dim) {  // meshing::checkVertex, meshing.hpp:148-150
 
 }  // namespace
 
+// The triangulation table or_mesh uses: the built-in one, or a caller's
+// (or_mesh_set_table: 256 x 16 ints, edge triples ended by -1).
+int8_t g_tris[256][3 * MF_MC_MAX_TRIS];
+bool g_tris_set = false;
+
 extern "C" {
+
+void or_mesh_set_table(const int* table) {
+  for (int r = 0; r < 256; ++r)
+    for (int e = 0; e < 3 * MF_MC_MAX_TRIS; ++e) {
+      if (!table) { g_tris[r][e] = MF_MC_TRIS[r][e]; continue; }
+      int n = 0;
+      while (n < 16 && table[16 * r + n] != -1) ++n;
+      g_tris[r][e] = e < n ? (int8_t)table[16 * r + e] : (int8_t)-1;
+    }
+  g_tris_set = true;
+}
 
 int or_mc_index(void* h, int x, int y, int z) {
   const Volume& v = *(const Volume*)h;
@@ -98,7 +114,7 @@ long long or_mesh(void* h, float* out, long long cap, int float_bounds) {
       for (int y = B.cy; y < yb; ++y)
         for (int z = B.cz; z < zb; ++z) {
           const int idx = mc_index(v, x, y, z);
-          const int8_t* t = MF_MC_TRIS[idx];
+          const int8_t* t = g_tris_set ? g_tris[idx] : MF_MC_TRIS[idx];
           for (int e = 0; e < 3 * MF_MC_MAX_TRIS && t[e] != -1; e += 3) {
             const F3 p0 = mc_vertex(v, x, y, z, t[e]);
             const F3 p1 = mc_vertex(v, x, y, z, t[e + 1]);

@@ -246,6 +246,10 @@ void ref_mc_vertex(void* h, int x, int y, int z, int edge, float* out) {
   const float3 p = meshing::interp_vertexes(vol._map_index, select, x, y, z, edge);
   out[0] = p.x; out[1] = p.y; out[2] = p.z;
 }
+// The reference's own triangulation table (lib/algorithms/edge_tables.h
+// triTable, compiled in with meshing.hpp): 256 x 16 ints into out.
+void ref_tri_table(int* out) { std::memcpy(out, triTable, sizeof(triTable)); }
+
 // algorithms::marching_cube as Kfusion::dump_mesh calls it: the triangle count,
 // and up to cap triangles (9 floats each) into out
 long long ref_marching_cube(void* h, float* out, long long cap) {

@@ -165,3 +165,93 @@ def test_autograd_function_matches_adjoint_and_fp64():
         fd[i] = _central(f)
     np.testing.assert_allclose(twist.grad.numpy(), fd, rtol=0, atol=2e-3 * np.abs(fd).max())
     ctx.close()
+
+
+def _setup_headline():
+    """The headline scene at 640x480 (background 512^3 @ 1 cm + 3 objects at
+    256^3 @ 2 mm), frame 0 integrated, frame 1 live."""
+    import os
+    import sys
+    import torch  # noqa: F401
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    s = bench.scene_for(0, 2)
+    Wf, Hf = s.width, s.height
+    labels = [i.label for i in s.instances]
+    ctx = Context(Wf, Hf, k=s.k, pool_blocks=1 << 16, robust="huber")
+    orc = O.oracle()
+    vols = []
+    for inst, T in zip(s.instances, s.volume_poses(0)):
+        ctx.add_instance(inst.size, inst.dim, T, inst.label)
+        vols.append(orc.volume(inst.size, inst.dim))
+    T0 = s.cam_poses[0].astype(np.float32)
+    d, rgb, lab = s.render(0)
+    masks = generalize_masks(lab, labels)
+    ctx.set_camera_pose(T0)
+    ctx.upload(d, rgb, masks)
+    ctx.integrate(list(range(len(labels))))
+    rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+    for i, v in enumerate(vols):
+        v.integrate(d, rgb3, masks[i], T0, s.volume_poses(0)[i], s.k, 0.1)
+    ctx.preprocess()
+    live = {"ref_intensity": ctx.pyramid(0, 1).copy(), "ref_vertex": ctx.pyramid(0, 2).copy()}
+    ctx.set_ref_from_current()
+    d1, rgb1, lab1 = s.render(1)
+    ctx.upload(d1, rgb1, generalize_masks(lab1, labels))
+    ctx.preprocess()
+    live.update(vertex=ctx.pyramid(0, 2).copy(), normal=ctx.pyramid(0, 3).copy(),
+                cov=ctx.pyramid(0, 6).copy(), intensity=ctx.pyramid(0, 1).copy())
+    return s, ctx, vols, labels, T0, live
+
+
+def test_twist_gradient_at_640x480_on_perturbed_pairs():
+    """The differentiation workload's shape: 640x480 frames of the headline
+    scene, live poses perturbed by N(0, 5 mm) and N(0, 0.5 deg); the cost and
+    dE/d twist against the FP64 oracle (central differences), on 2 pairs."""
+    s, ctx, vols, labels, T0, live = _setup_headline()
+    Wf, Hf = s.width, s.height
+    rng = np.random.default_rng(64)
+    for pair in range(2):
+        xi = np.concatenate([rng.normal(size=3) * 0.005,
+                             rng.normal(size=3) * np.deg2rad(0.5)])
+        T = (se3_exp(xi) @ s.cam_poses[1]).astype(np.float32)
+        E, g, rows = ctx.camera_cost(T)
+
+        def cost(Tl):
+            return O.camera_cost(vols, s.volume_poses(0), labels, T0, Tl, s.k, Wf, Hf, live)
+
+        E64, rows64 = cost(T.astype(np.float64))
+        assert rows > 10000 and abs(rows - rows64) <= max(2, 2e-3 * rows64), (rows, rows64)
+        assert abs(E - E64) <= 2e-3 * E64, (pair, E, E64)
+        fd = np.zeros(6)
+        T64 = T.astype(np.float64)
+        for i in range(6):
+            def f(h, i=i):
+                d = np.zeros(6)
+                d[i] = h
+                return cost(se3_exp(d) @ T64)[0]
+            fd[i] = _central(f)
+        np.testing.assert_allclose(g, fd, rtol=0, atol=2e-3 * np.abs(fd).max(),
+                                   err_msg=f"pair {pair}: {g} vs {fd}")
+    assert ctx.status() == 0
+    ctx.close()
+
+
+def test_photometric_twist_gradient_against_the_gn_system():
+    """With the photometric term alone: dE/d twist of the adjoint (the exact
+    derivative of the bilinear interpolation through the projection) against
+    -J^T W r of the Gauss-Newton system (mf_track_eval), whose photometric J
+    uses the reference's precomputed gradient images (tracking.cpp:1123-1150).
+    The two agree up to that difference of image derivatives: direction within
+    a few degrees, magnitude within a few per cent."""
+    s, ctx, vols, labels, T0, live = _setup(use_icp=False, use_rgb=True)
+    T = _live_pose(s)
+    _, g, rows = ctx.camera_cost(T)
+    sums = ctx.track_eval(0, 0, T)
+    jtwr = -np.asarray(sums[1:7])
+    cos = float(g @ jtwr / (np.linalg.norm(g) * np.linalg.norm(jtwr)))
+    rel = float(np.linalg.norm(g - jtwr) / np.linalg.norm(jtwr))
+    print(f"photometric: cos {cos:.6f}, relative difference {rel:.4f}")
+    assert cos > 0.99 and rel < 0.1, (cos, rel)
+    assert ctx.status() == 0
+    ctx.close()

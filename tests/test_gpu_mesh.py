@@ -64,3 +64,58 @@ def test_mesh_matches_oracle(tmp_path):
         assert text[0] == "# vtk DataFile Version 1.0" and text[4].startswith("POINTS ")
     assert ctx.status() == 0
     ctx.close()
+
+
+def test_mesh_with_the_reference_table_is_the_reference_mesh():
+    """mf_mesh_set_triangle_table with the reference's own triTable (read from
+    its compiled mesher, oracle/_ref): the device's triangles equal the
+    oracle's with the same table triangle for triangle, and the reference's
+    algorithms::marching_cube as a set (its order follows its block list)."""
+    import ctypes as C
+    ref = O.reference()
+    if ref is None:
+        pytest.skip("oracle/_ref not built")
+    t = np.zeros((256, 16), np.int32)
+    ref.lib.ref_tri_table.argtypes = [C.c_void_p]
+    ref.lib.ref_tri_table(t.ctypes.data_as(C.c_void_p))
+    s = make_scene("room", 160, 120, n_frames=4, seed=4, bg_size=128)
+    inst = s.instances[0]
+    ctx = Context(160, 120, k=s.k, pool_blocks=1 << 13)
+    ctx.add_instance(inst.size, inst.dim, np.eye(4), inst.label)
+    orc = O.oracle()
+    a, b = orc.volume(inst.size, inst.dim), ref.volume(inst.size, inst.dim)
+    for f in range(4):
+        d, rgb, lab = s.render(f)
+        m = generalize_masks(lab, [inst.label])
+        T = s.cam_poses[f].astype(np.float32)
+        ctx.set_camera_pose(T)
+        ctx.upload(d, rgb, m)
+        ctx.integrate([0])
+        rgb3 = rgb.astype(np.float32) / np.float32(255)
+        for v in (a, b):
+            v.integrate(d, rgb3, m[0], T, np.eye(4), s.k, 0.1)
+    ctx.set_triangle_table(t)
+    got = ctx.mesh(0)
+    lib = orc.lib
+    lib.or_mesh_set_table.argtypes = [C.c_void_p]
+    lib.or_mesh_set_table(t.ctypes.data_as(C.c_void_p))
+    try:
+        want = O.mesh(orc, a)
+    finally:
+        lib.or_mesh_set_table(None)
+    assert len(got) == len(want) > 1000 and np.array_equal(got, want)
+    mb = O.mesh(ref, b)
+
+    def canon(x):
+        flat = x.reshape(len(x), 9)
+        return flat[np.lexsort(flat.T[::-1])]
+    assert np.array_equal(canon(got), canon(mb))
+    # NULL restores the built-in table; a malformed row is rejected
+    ctx.set_triangle_table(None)
+    assert np.array_equal(ctx.mesh(0), O.mesh(orc, a))
+    bad = t.copy()
+    bad[7, :] = 3
+    with pytest.raises(Exception):
+        ctx.set_triangle_table(bad)
+    assert ctx.status() == 0
+    ctx.close()

@@ -171,3 +171,48 @@ def test_track_results_and_mask_refinement_match_oracle():
         assert np.array_equal(ctx.mask(i), O.refine_mask_use_motion(mi, ci.reshape(-1))), i
     assert ctx.status() == 0
     ctx.close()
+
+
+def test_object_residuals_at_the_virtual_pose_match_oracle():
+    """mf_object_residuals (kfusion.cpp:446-466): after the objects are
+    tracked and the live raycast is redone at their new poses, each object's
+    rows recomputed by compute_residuals at its virtual camera pose against
+    its own pixels of the model maps and of the live raycast, against the
+    oracle's compute_residuals on the same inputs, bit-exact; and the
+    never-moving classes (Object::static_object) never move."""
+    import torch
+    e = _setup()
+    ctx, labels = e["ctx"], e["labels"]
+    ids = list(range(1, len(labels)))
+    ctx.track_objects(ids)
+    ctx.motion_residuals(1.5, 0.9)   # the live raycast at the objects' new poses
+    _, _, lvert, llab = ctx.motion_download()
+    v, n, lab = e["model"]
+    T_w_r = e["T0"]
+    buf = torch.zeros(2 * W * H, dtype=torch.int8, device="cuda")
+    checked = 0
+    for i in ids:
+        T_virt = ctx.object_residuals(i, buf.data_ptr(), 1.5)
+        got = buf.cpu().numpy().reshape(2, H, W)
+        l = labels[i]
+        own = (lab == l)[..., None]
+        mv = np.where(own, v, np.float32(0)).astype(np.float32)
+        mn = np.where(own, n, np.array([-2.0, 0, 0], np.float32)).astype(np.float32)
+        lv = np.where((llab == l)[..., None], lvert, np.float32(0)).astype(np.float32)
+        want, _ = e["trk"].motion_residuals(T_virt, T_w_r, mv, mn, lv, 1.5)
+        assert np.array_equal(got, want), (i, np.count_nonzero(got != want))
+        # the virtual pose maps the object's last pose to the new relative view
+        T_wo1 = e["poses"][i].astype(np.float64)
+        T_wo2 = ctx.instance_pose(i).astype(np.float64)
+        T_c = ctx.camera_pose().astype(np.float64)
+        np.testing.assert_allclose(np.linalg.inv(T_virt) @ T_wo1, np.linalg.inv(T_c) @ T_wo2,
+                                   atol=1e-4)
+        checked += int(np.count_nonzero(got[0] == 1) > 0)
+    assert checked >= 2
+    # a never-moving class: the same frame reports no motion for that object
+    for i in ids:
+        ctx.lib.mf_instance_set_semantics(ctx.h, i, 63, None, 0)
+    _, bits = ctx.motion_residuals(1.5, 1.01)   # every object with inliers "moves"...
+    assert bits == 0                             # ...unless its class never moves
+    assert ctx.status() == 0
+    ctx.close()

@@ -4,7 +4,8 @@ flow driven step by step through the separate entry points (each of them
 checked against the oracle in tests/test_gpu_motion.py and
 tests/test_gpu_volume.py): camera track, motion residuals and moving labels,
 masked camera re-track, tracking of the moving objects only, residuals again,
-mask refinement from the third frame on, integration, raycast, new reference.
+each moving object's rows recomputed at its virtual camera pose, mask
+refinement from the third frame on, integration, raycast, new reference.
 Moving bits, camera and volume poses, the refined masks, every voxel of
 every volume and the model maps agree bit for bit; the scene's objects move,
 so the moving branch runs (checked), and frames 2-5 refine the masks.
@@ -72,7 +73,7 @@ def _step_by_step(ctx, s, f, frame, buf0, buf1):
             for i in range(n):
                 rows = rows0
                 if i in moving:
-                    ctx.track_results(i, buf1.data_ptr())
+                    ctx.object_residuals(i, buf1.data_ptr(), 1.5)
                     rows = buf1.data_ptr()
                 ctx.refine_mask_use_motion(i, rows)
     ctx.integrate(list(range(n)))

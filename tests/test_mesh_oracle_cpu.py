@@ -82,3 +82,40 @@ def test_cells_and_mesh_match_reference():
     (aa, xa), (ab, xb) = _area_volume(ma), _area_volume(mb)
     assert abs(aa - ab) <= 1e-3 * ab, (aa, ab)
     assert abs(xa - xb) <= 1e-3 * abs(xb), (xa, xb)
+
+
+def ref_triangle_table():
+    """The reference's own triTable (lib/algorithms/edge_tables.h), read from
+    the reference's compiled mesher (oracle/_ref/libmf_ref.so)."""
+    import ctypes as C
+    t = np.zeros((256, 16), np.int32)
+    ref.lib.ref_tri_table.argtypes = [C.c_void_p]
+    ref.lib.ref_tri_table(t.ctypes.data_as(C.c_void_p))
+    return t
+
+
+def sorted_triangles(tris):
+    """Triangles (n, 3, 3) in a canonical order (the reference's order depends
+    on its block list and OpenMP): rows sorted lexicographically."""
+    flat = tris.reshape(len(tris), 9)
+    return flat[np.lexsort(flat.T[::-1])]
+
+
+@pytest.mark.skipif(ref is None, reason="oracle/_ref not built (no reference tree)")
+def test_mesh_with_the_reference_table_matches_reference_triangle_for_triangle():
+    """With the reference's own triangulation table the oracle's mesher emits
+    the reference's triangles: the same triangle (same vertices, same vertex
+    order) for every triangle, bit for bit."""
+    import ctypes as C
+    inst, a, b = _volumes()
+    lib = O.oracle().lib
+    lib.or_mesh_set_table.argtypes = [C.c_void_p]
+    t = ref_triangle_table()
+    assert (t[:, 15] == -1).all() and (t >= -1).all() and (t <= 11).all()
+    lib.or_mesh_set_table(t.ctypes.data_as(C.c_void_p))
+    try:
+        ma, mb = O.mesh(O.oracle(), a), O.mesh(ref, b)
+    finally:
+        lib.or_mesh_set_table(None)
+    assert len(ma) == len(mb) > 5000
+    assert np.array_equal(sorted_triangles(ma), sorted_triangles(mb))
