@@ -119,6 +119,43 @@ int mf_alloc_update(mf_context* ctx, int id, const uint64_t* keys, int n);
  * the current camera pose: composite vertex/normal/label maps stay on the
  * device as the tracking model. */
 int mf_raycast(mf_context* ctx);
+/* --- instance-sharded raycast (no counterpart in the reference, which runs
+ * on one host) ------------------------------------------------------------
+ * The composite of raycastObjectList (rendering.cpp:9-181) split into a part
+ * per instance, which the GPU that holds the instance's volume computes, and
+ * an ordered per-pixel fold, which needs no volume: across GPUs, each rank
+ * records its own instances, the records are gathered (e.g. an NCCL
+ * all-gather), and every rank folds all of them into the same maps.
+ * The reference bounds each instance's march by the nearest hit so far; a
+ * record holds the march to the far plane and the parameter at which it
+ * crossed the surface, and the fold applies the bound afterwards: the
+ * bounded march finds that crossing exactly when it lies before the bound,
+ * and otherwise returns the zero hit, whose values the origin record holds. */
+typedef struct mf_ray_record {
+  float hit[4];      /* (x, y, z, t) in the instance's frame; 0 without a crossing */
+  float tc;          /* march parameter of the crossing sample; +inf: none */
+  float fg;          /* foreground probability interpolated at the hit */
+  float normal[3];   /* world normal normalize(R_wo grad(hit)) */
+  int zero_grad;     /* 1: the gradient is zero (the reference writes only normal.x) */
+  int pad[2];
+} mf_ray_record;     /* 48 bytes */
+typedef struct mf_ray_origin {
+  float fg;          /* foreground probability at the volume origin (the zero hit) */
+  float normal[3];   /* world normal at the zero hit */
+  int zero_grad;
+  int pad[3];
+} mf_ray_origin;     /* 32 bytes */
+/* Records of instances ids[0..n) at the current camera pose into device
+ * memory: d_records[k * W * H + p] for instance ids[k] and pixel p, and
+ * d_origins[k]. */
+int mf_raycast_records(mf_context* ctx, const int* ids, int n, mf_ray_record* d_records,
+                       mf_ray_origin* d_origins);
+/* The composite maps from the records of EVERY instance of the context, in
+ * instance order (d_records[i * W * H + p], d_origins[i], device memory), with
+ * the context's instance poses and labels: the maps mf_raycast makes, bit for
+ * bit.  They replace the context's model maps. */
+int mf_raycast_fold(mf_context* ctx, const mf_ray_record* d_records,
+                    const mf_ray_origin* d_origins);
 /* Copy the composite maps to the host (any pointer may be NULL). */
 int mf_download_raycast(mf_context* ctx, float* vertex, float* normal, int32_t* label);
 

@@ -44,6 +44,7 @@ EXPORTS = [
     "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh", "mf_tune_candidates", "mf_tune_describe",
     "mf_autotune", "mf_tune_get", "mf_tune_set", "mf_process_frame_motion",
     "mf_set_gn_persistent", "mf_object_residuals", "mf_mesh_set_triangle_table",
+    "mf_raycast_records", "mf_raycast_fold",
 ]
 
 TUNE_RAYCAST, TUNE_INTEGRATE, TUNE_MAX_VARIANTS = 0, 1, 16
@@ -201,6 +202,18 @@ class Context:
 
     def raycast(self):
         self._check(self.lib.mf_raycast(self.h))
+
+    def raycast_records(self, ids, d_records, d_origins):
+        """Records of instances `ids` into device memory (mf_ray_record: 48 B
+        per instance and pixel; mf_ray_origin: 32 B per instance)."""
+        arr = np.ascontiguousarray(ids, np.int32)
+        self._check(self.lib.mf_raycast_records(self.h, _ptr(arr, np.int32), len(arr),
+                                                C.c_void_p(d_records), C.c_void_p(d_origins)))
+
+    def raycast_fold(self, d_records, d_origins):
+        """The composite maps from every instance's records (device memory)."""
+        self._check(self.lib.mf_raycast_fold(self.h, C.c_void_p(d_records),
+                                             C.c_void_p(d_origins)))
 
     def download_raycast(self):
         v = np.zeros((self.H, self.W, 3), np.float32)

@@ -391,6 +391,26 @@ int mf_raycast(mf_context* ctx) {
   return stage_raycast(ctx, l, ctx->ray_epsilon);
 }
 
+int mf_raycast_records(mf_context* ctx, const int* ids, int n, mf_ray_record* d_records,
+                       mf_ray_origin* d_origins) {
+  if (check(ctx) || !ids || n <= 0 || n > MAX_INSTANCES || !d_records || !d_origins)
+    return MF_E_ARG;
+  IdList l;
+  l.n = n;
+  for (int k = 0; k < n; ++k) {
+    if (ids[k] < 0 || ids[k] >= (int)ctx->inst.size()) return MF_E_NOT_FOUND;
+    l.v[k] = ids[k];
+  }
+  return raycast_records(ctx, l, d_records, d_origins);
+}
+
+int mf_raycast_fold(mf_context* ctx, const mf_ray_record* d_records,
+                    const mf_ray_origin* d_origins) {
+  if (check(ctx) || !d_records || !d_origins) return MF_E_ARG;
+  if (ctx->inst.empty()) return MF_E_STATE;
+  return raycast_fold(ctx, d_records, d_origins);
+}
+
 int mf_download_raycast(mf_context* ctx, float* vertex, float* normal, int32_t* label) {
   if (check(ctx)) return MF_E_ARG;
   const size_t WH = (size_t)ctx->W * ctx->H;

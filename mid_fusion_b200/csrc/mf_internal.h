@@ -166,6 +166,9 @@ int motion_download(Context* ctx, int8_t* res, float* err, float* lvert, int32_t
 int track_results(Context* ctx, int slot, int8_t* d_out, float* d_err, float* pose_eval);
 int object_residuals(Context* ctx, int i, float threshold, int8_t* d_rows, float* T_virtual);
 int mesh_set_table(Context* ctx, const int* table);
+int raycast_records(Context* ctx, const IdList& ids, mf_ray_record* d_records,
+                    mf_ray_origin* d_origins);
+int raycast_fold(Context* ctx, const mf_ray_record* d_records, const mf_ray_origin* d_origins);
 int motion_planes(Context* ctx, const int8_t** res, const float** err);
 // headless renders (mf_render.cu; the shaded volume render in mf_raycast.cu)
 // formats (mf_io.cu)

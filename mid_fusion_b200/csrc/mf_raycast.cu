@@ -433,6 +433,192 @@ raycast_fold_kernel(Pool pool, const Volume* __restrict__ vols,
   }
 }
 
+// ------------------------------------------------------------------------
+// Instance-sharded raycast (mf_raycast_records / mf_raycast_fold): the
+// phased path's records, with the world normal of every crossing computed by
+// the GPU that holds the volume, so that the fold needs no volume.
+__global__ void __launch_bounds__(128)
+raycast_records_kernel(Pool pool, const Volume* __restrict__ vols,
+                       const InstFrame* __restrict__ frames, IdList ids, M4 view, RayArgs a,
+                       mf_ray_record* __restrict__ rec, int* __restrict__ status) {
+  __shared__ int s_slot[8 * 128];
+  const int x = blockIdx.x * 16 + (threadIdx.x % 16);
+  const int y = blockIdx.y * 8 + (threadIdx.x / 16);
+  if (x >= a.W || y >= a.H) return;
+  const int o = blockIdx.z;
+  const int i = ids.v[o];
+  const Volume& V = vols[i];
+  const InstFrame& F = frames[i];
+  const int p = x + y * a.W;
+  const F3 w_dir = rotate(view, mk3((float)x, (float)y, 1.f));
+  const float step = V.dim / V.size;
+  const F3 o_dir = normalize(rotate(F.inv_T_w_o, w_dir));
+  const float t_min =
+      ray_misses_blocks(V, V.bbox, F.o_origin, o_dir, a.nearPlane, a.farPlane, a.epsilon)
+          ? -1.f
+          : ray_first_block(V, F.o_origin, o_dir, a.nearPlane, a.farPlane, a.epsilon, status);
+  F4 hit = F4{0, 0, 0, 0};
+  float tc = INFINITY;
+  if (t_min > 0.f)
+    hit = raycast_volume<true>(pool, V, F.o_origin, o_dir, t_min * V.dim / (unsigned)V.size,
+                               a.farPlane, a.mu, step, step * 8, &tc);
+  mf_ray_record r;
+  r.hit[0] = hit.x; r.hit[1] = hit.y; r.hit[2] = hit.z; r.hit[3] = hit.w;
+  r.tc = tc;
+  r.fg = 0.f;
+  r.normal[0] = r.normal[1] = r.normal[2] = 0.f;
+  r.zero_grad = 1;
+  r.pad[0] = r.pad[1] = 0;
+  if (tc < INFINITY) {
+    const F3 h = mk3(hit.x, hit.y, hit.z);
+    r.fg = volume_interp(pool, V, h, 1);
+    const F3 gn = volume_grad(pool, V, h, s_slot + threadIdx.x, 128);
+    if (length(gn) != 0) {
+      const F3 n = normalize(rotate(F.T_w_o, gn));
+      r.normal[0] = n.x; r.normal[1] = n.y; r.normal[2] = n.z;
+      r.zero_grad = 0;
+    }
+  }
+  rec[(size_t)o * a.W * a.H + p] = r;
+}
+
+// foreground and world normal of each listed instance at the zero hit
+__global__ void raycast_origins_kernel(Pool pool, const Volume* __restrict__ vols,
+                                       const InstFrame* __restrict__ frames, IdList ids,
+                                       mf_ray_origin* __restrict__ out) {
+  __shared__ int s_slot[8 * 32];
+  const int o = threadIdx.x;
+  if (o >= ids.n) return;
+  const Volume& V = vols[ids.v[o]];
+  const InstFrame& F = frames[ids.v[o]];
+  mf_ray_origin r;
+  r.fg = volume_interp(pool, V, mk3(0.f, 0.f, 0.f), 1);
+  const F3 gn = volume_grad(pool, V, mk3(0.f, 0.f, 0.f), s_slot + threadIdx.x, 32);
+  r.zero_grad = length(gn) == 0 ? 1 : 0;
+  const F3 n = r.zero_grad ? mk3(0.f) : normalize(rotate(F.T_w_o, gn));
+  r.normal[0] = n.x; r.normal[1] = n.y; r.normal[2] = n.z;
+  r.pad[0] = r.pad[1] = r.pad[2] = 0;
+  out[o] = r;
+}
+
+// the composite of raycast_fold_kernel from records (all instances, in order)
+__global__ void __launch_bounds__(128)
+raycast_fold_records_kernel(const InstFrame* __restrict__ frames, IdList ids, RayArgs a,
+                            const mf_ray_record* __restrict__ rec,
+                            const mf_ray_origin* __restrict__ orig) {
+  const int x = blockIdx.x * 16 + (threadIdx.x % 16);
+  const int y = blockIdx.y * 8 + (threadIdx.x / 16);
+  if (x >= a.W || y >= a.H) return;
+  const int p = x + y * a.W;
+  const size_t WH = (size_t)a.W * a.H;
+  const float INVALID = -2;
+  float nearest = 1.0e3f;
+  double high_fg = 0.f;
+  int miss = 0;
+  int win = -1;
+  F4 win_hit = F4{0, 0, 0, 0};
+  F3 win_n = mk3(0.f), last_full = mk3(0.f);
+  bool win_zero = true, have_full = false;
+  for (int o = 0; o < ids.n; ++o) {
+    const InstFrame& F = frames[ids.v[o]];
+    const float nfar = fmn(nearest, a.farPlane);
+    const mf_ray_record& r = rec[o * WH + p];
+    F4 hit = F4{0, 0, 0, 0};
+    double fg;
+    F3 n;
+    bool zero;
+    if (r.tc < nfar) {
+      hit = F4{r.hit[0], r.hit[1], r.hit[2], r.hit[3]};
+      fg = r.fg;
+      n = mk3(r.normal[0], r.normal[1], r.normal[2]);
+      zero = r.zero_grad != 0;
+    } else {
+      fg = orig[o].fg;
+      n = mk3(orig[o].normal[0], orig[o].normal[1], orig[o].normal[2]);
+      zero = orig[o].zero_grad != 0;
+    }
+    const float hd = F.label == 0 ? hit.w + 0.05f : hit.w;
+    if (hd > nearest) { miss++; continue; }
+    if (fg <= 0.5f) { miss++; continue; }
+    if (hd == nearest) {
+      if (!(fg > high_fg)) { miss++; continue; }
+    } else if (hd < nearest) {
+      nearest = hd;
+    } else {
+      miss++;
+      continue;
+    }
+    high_fg = fg;
+    // the reference writes each winner's normal as it wins (only x when its
+    // gradient is zero): y and z end as the latest full write's
+    if (win >= 0 && !win_zero) { last_full = win_n; have_full = true; }
+    win = o;
+    win_hit = hit;
+    win_n = n;
+    win_zero = zero;
+  }
+  if (win < 0) {
+    if (miss == ids.n) {
+      a.vertex[p] = mk3(0.f);
+      a.normal[p] = mk3(INVALID, 0, 0);
+      a.label[p] = (int)INVALID;
+    }
+    return;
+  }
+  const InstFrame& F = frames[ids.v[win]];
+  a.label[p] = F.label;
+  a.vertex[p] = xform(F.T_w_o, mk3(win_hit.x, win_hit.y, win_hit.z));
+  if (!win_zero) {
+    a.normal[p] = win_n;
+  } else {
+    a.normal[p].x = INVALID;
+    if (have_full) {
+      a.normal[p].y = last_full.y;
+      a.normal[p].z = last_full.z;
+    }
+  }
+}
+
+int raycast_records(Context* ctx, const IdList& ids, mf_ray_record* d_records,
+                    mf_ray_origin* d_origins) {
+  if (ids.n == 0) return MF_OK;
+  IdList all;
+  all.n = (int)ctx->inst.size();
+  for (int i = 0; i < all.n; ++i) all.v[i] = i;
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  const mf_config& c = ctx->cfg;
+  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H, c.near_plane,
+            c.far_plane, c.mu, ctx->ray_epsilon};
+  // every instance's frame holds the same camera view (rendering.cpp:17)
+  InstFrame f0;
+  MF_CUDA(cudaMemcpyAsync(&f0, ctx->d_frames, sizeof(InstFrame), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  dim3 grid((ctx->W + 15) / 16, (ctx->H + 7) / 8, ids.n);
+  raycast_records_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames,
+                                                         ids, f0.view, a, d_records,
+                                                         ctx->d_status);
+  raycast_origins_kernel<<<1, 32, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids,
+                                                    d_origins);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int raycast_fold(Context* ctx, const mf_ray_record* d_records, const mf_ray_origin* d_origins) {
+  IdList all;
+  all.n = (int)ctx->inst.size();
+  for (int i = 0; i < all.n; ++i) all.v[i] = i;
+  if (int rc = stage_prepare(ctx, all)) return rc;
+  const mf_config& c = ctx->cfg;
+  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H, c.near_plane,
+            c.far_plane, c.mu, ctx->ray_epsilon};
+  dim3 grid((ctx->W + 15) / 16, (ctx->H + 7) / 8);
+  raycast_fold_records_kernel<<<grid, 128, 0, ctx->stream>>>(ctx->d_frames, all, a, d_records,
+                                                             d_origins);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
 // Algorithmic bytes of one composite raycast (the per-unit figures of the
 // raycast's roofline): the same march as raycast_objects_kernel, counting
 // instead of writing.  Per ray and instance: 8 B for every voxel read of the

@@ -100,6 +100,17 @@ void or_raycast_objects(void** vols, const float* Two, const int* labels, int n,
                       F4{k4[0], k4[1], k4[2], k4[3]}, W, H, nearp, farp, mu, eps);
 }
 
+void or_raycast_records(void* vol, const float* Two, int label, const float* Twc,
+                        const float* k4, int W, int H, float nearp, float farp, float mu,
+                        float eps, float* rec, float* origin) {
+  RaycastInstance in;
+  in.vol = (const Volume*)vol;
+  in.T_w_o = load_m4(Two);
+  in.label = label;
+  raycast_records(in, load_m4(Twc), F4{k4[0], k4[1], k4[2], k4[3]}, W, H, nearp, farp, mu, eps,
+                  rec, origin);
+}
+
 void or_raycast_oob_mask(void** vols, const float* Two, int n, const float* Twc,
                          const float* k4, int W, int H, float nearp, float farp, float mu,
                          float eps, unsigned char* mask) {

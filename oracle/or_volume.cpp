@@ -464,7 +464,8 @@ static float get_tsdf_at(const Volume& v, F3 p) {  // volume_template.hpp:83-88
 
 // apps/kfusion/src/cpp/kfusion/rendering_impl.hpp:80-140
 F4 raycast(const Volume& v, F3 origin, F3 direction, float nearPlane, float farPlane,
-           float mu, float step, float largestep) {
+           float mu, float step, float largestep, float* tc) {
+  if (tc) *tc = INFINITY;
   const F3 invR = mk3(1.0f / direction.x, 1.0f / direction.y, 1.0f / direction.z);
   const F3 tbot = (-1.f * invR) * origin;
   const F3 ttop = invR * (v.dim - origin);
@@ -487,6 +488,7 @@ F4 raycast(const Volume& v, F3 origin, F3 direction, float nearPlane, float farP
         f_t = f_tt;
       }
       if (f_tt < 0) {
+        if (tc) *tc = t;
         t = t + stepsize * f_tt / (f_t - f_tt);
         const F3 p = origin + direction * t;
         return F4{p.x, p.y, p.z, t};
@@ -551,6 +553,54 @@ void raycast_object_list(const RaycastInstance* inst, int n, F3* vertex, F3* nor
         label_img[p] = (int)INVALID;
       }
     }
+}
+
+// Test support, no reference counterpart: one instance's records of the
+// instance-sharded composite (the device's mf_raycast_records): per pixel 12
+// floats -- the hit (x, y, z, t) of the march to the far plane, the march
+// parameter of its crossing sample (+inf: none), the foreground at the hit,
+// the world normal, a zero-gradient flag and 2 zeros -- and 8 floats of the
+// zero hit: foreground and world normal at the volume origin, its flag, 3 zeros.
+void raycast_records(const RaycastInstance& in, const M4& T_w_c, F4 k, int W, int H,
+                     float nearPlane, float farPlane, float mu, float epsilon, float* rec,
+                     float* origin) {
+  const Volume& vol = *in.vol;
+  const M4 view = mul(T_w_c, inverse_camera_matrix(k));
+  const M4 inv = inverse(in.T_w_o);
+  const float step = vol.dim / vol.size;
+  auto normal_of = [&](F3 h, float* out) {
+    const F3 gn = grad_tsdf(vol, h);
+    if (length(gn) == 0) { out[0] = out[1] = out[2] = 0.f; out[3] = 1.f; return; }
+    const F3 n = normalize(rotate(in.T_w_o, gn));
+    out[0] = n.x; out[1] = n.y; out[2] = n.z; out[3] = 0.f;
+  };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      float* r = rec + 12 * (size_t)(x + y * W);
+      const F3 o_origin = inv * get_translation(view);
+      const F3 w_dir = rotate(view, mk3((float)x, (float)y, 1.f));
+      const F3 o_dir = normalize(rotate(inv, w_dir));
+      const float t_min = ray_first_block(vol, o_origin, o_dir, nearPlane, farPlane, epsilon);
+      float tc = INFINITY;
+      const F4 hit = t_min > 0.f ? raycast(vol, o_origin, o_dir,
+                                           t_min * vol.dim / (unsigned)vol.size, farPlane, mu,
+                                           step, step * 8, &tc)
+                                 : F4{0, 0, 0, 0};
+      r[0] = hit.x; r[1] = hit.y; r[2] = hit.z; r[3] = hit.w;
+      r[4] = tc;
+      r[5] = 0.f;
+      r[6] = r[7] = r[8] = 0.f; r[9] = 1.f;
+      r[10] = r[11] = 0.f;
+      if (tc < INFINITY) {
+        const F3 h = mk3(hit.x, hit.y, hit.z);
+        r[5] = interp(vol, h, 1);
+        normal_of(h, r + 6);
+      }
+    }
+  origin[0] = interp(vol, mk3(0.f, 0.f, 0.f), 1);
+  normal_of(mk3(0.f, 0.f, 0.f), origin + 1);
+  origin[5] = origin[6] = origin[7] = 0.f;
 }
 
 // Test support, no reference counterpart: marks the pixels where any

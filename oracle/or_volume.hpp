@@ -112,7 +112,7 @@ F3 grad_tsdf(const Volume& v, F3 pos_m);
 float ray_first_block(const Volume& v, F3 origin, F3 dir, float nearp, float farp,
                       float epsilon);
 F4 raycast(const Volume& v, F3 origin, F3 dir, float nearp, float farp, float mu,
-           float step, float largestep);
+           float step, float largestep, float* tc = nullptr);
 
 struct RaycastInstance {
   const Volume* vol;
@@ -122,6 +122,10 @@ struct RaycastInstance {
 void raycast_object_list(const RaycastInstance* inst, int n, F3* vertex, F3* normal,
                          int* label_img, const M4& T_w_c, F4 k, int W, int H,
                          float nearp, float farp, float mu, float epsilon);
+// one instance's records of the instance-sharded composite (test support)
+void raycast_records(const RaycastInstance& in, const M4& T_w_c, F4 k, int W, int H,
+                     float nearp, float farp, float mu, float epsilon, float* rec,
+                     float* origin);
 // pixels whose raycast reads voxels outside [0, size) (test support)
 void raycast_oob_mask(const RaycastInstance* inst, int n, unsigned char* mask, const M4& T_w_c,
                       F4 k, int W, int H, float nearp, float farp, float mu, float epsilon);
