@@ -566,6 +566,102 @@ def run_reference(args):
     }
 
 
+def run_shard(args, rank, world, local_rank):
+    """One sequence split over the ranks by instance (mid_fusion_b200.shard):
+    every rank tracks the camera (the same result everywhere), tracks and
+    integrates its own instances, records its instances' raycasts; the
+    object poses and the records are all-gathered (NCCL), and every rank
+    folds the same composite maps.  Timed per frame on the device (CUDA
+    events on the library's stream, which also carries the collectives),
+    max over ranks; total work is fixed as N grows ("scaling": "strong").
+    At N = 1 the poses are checked against the batched one-GPU frame."""
+    import ctypes
+    import torch
+    import torch.distributed as dist
+    from mid_fusion_b200 import build, shard
+    from mid_fusion_b200.capi import Context
+    n_frames = 1 + args.warmup + args.steps
+    frames = render_frames(0, {"multi": n_frames}, args.workers)["multi"]
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    build.build()
+    s = scene_for(0, n_frames)
+    n = len(s.instances)
+    labels = [i.label for i in s.instances]
+    parts = shard.partition([i.size for i in s.instances], world)
+    mine = parts[rank]
+    objs = [i for i in mine if i > 0]
+    ctx = Context(W, H, k=s.k, pool_blocks=args.pool_blocks, batched=True, robust="huber")
+    for inst, T in zip(s.instances, s.volume_poses(0)):
+        ctx.add_instance(inst.size, inst.dim, T, inst.label)
+    ctx.set_camera_pose(s.cam_poses[0])
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    rec = torch.zeros((max(len(mine), 1), H, W, shard.RECORD_BYTES), dtype=torch.uint8, device=dev)
+    org = torch.zeros((max(len(mine), 1), shard.ORIGIN_BYTES), dtype=torch.uint8, device=dev)
+    times, cams = [], []
+    for f in range(n_frames):
+        d, rgb, lab = frames[f]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            ctx.upload(d, rgb, None)
+            ctx.upload_labels(lab.astype(np.uint16))
+            ctx.preprocess()
+            if f > 0:
+                ctx.track_camera(labels[1:])
+                ctx.track_objects(objs)
+                own = torch.from_numpy(np.stack([ctx.instance_pose(i) for i in mine])).to(dev)
+                allp = shard.gather_poses(own, parts, n).cpu().numpy()
+                for i in range(n):
+                    if i not in mine:
+                        ctx.set_instance_pose(i, allp[i])
+            ctx.integrate(mine)
+            ctx.raycast_records(mine, rec.data_ptr(), org.data_ptr())
+            grec, gorg = shard.gather_records(rec[:len(mine)], org[:len(mine)], parts, n)
+            ctx.raycast_fold(grec.data_ptr(), gorg.data_ptr())
+            ctx.set_ref_from_current()
+            e1.record(stream)
+        e1.synchronize()
+        if f >= 1 + args.warmup:
+            times.append(e0.elapsed_time(e1) * 1e-3)
+        cams.append(ctx.camera_pose().copy())
+    st = ctx.status()
+    ctx.close()
+    total = reduce_max(sum(times), world)
+    check = None
+    if world == 1:  # the same frames through the batched one-GPU frame
+        c1 = Context(W, H, k=s.k, pool_blocks=args.pool_blocks, batched=True, robust="huber")
+        for inst, T in zip(s.instances, s.volume_poses(0)):
+            c1.add_instance(inst.size, inst.dim, T, inst.label)
+        c1.set_camera_pose(s.cam_poses[0])
+        diff = 0.0
+        for f in range(n_frames):
+            d, rgb, lab = frames[f]
+            rc = c1.lib.mf_process_frame(c1.h, ctypes.c_void_p(d.ctypes.data),
+                                         ctypes.c_void_p(np.ascontiguousarray(rgb).ctypes.data),
+                                         ctypes.c_void_p(np.ascontiguousarray(
+                                             lab.astype(np.uint16)).ctypes.data))
+            if rc != 0:
+                raise RuntimeError("mf_process_frame failed")
+            diff = max(diff, float(np.abs(c1.camera_pose() - cams[f]).max()))
+        c1.close()
+        check = {"camera_pose_diff_vs_batched_frame": diff}
+    return {"metric": METRIC, "value": round(args.steps / total, 2), "unit": "frames/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * total / args.steps, 4), "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded analytic RGB-D scenes)",
+            "config": {"workload": WORKLOAD, "frame": [W, H], "instances": n,
+                       "parallelism": f"instance-sharded x{world}",
+                       "instances_per_rank": [len(p) for p in parts]},
+            "mode": "instance-sharded frame (host-driven stages, NCCL all-gather of poses "
+                    "and raycast records, per-pixel fold)",
+            "status_flags": st, "check": check}
+
+
 def traffic_from_profiles(name):
     """DRAM bytes per launch recorded from an ncu capture in profiles/<name>."""
     p = os.path.join(ROOT, "profiles", name)
@@ -620,6 +716,8 @@ def main():
                     help="multi: background + 3 objects (the headline); uneven: + 12 objects")
     ap.add_argument("--profile", action="store_true",
                     help="run only the batched device-resident path (profiler runs)")
+    ap.add_argument("--shard", action="store_true",
+                    help="one sequence split over the ranks by instance (strong scaling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -638,6 +736,15 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.shard:
+        out = run_shard(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(out))
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
 
     r = run_ours(args, rank, world, local_rank)
     if world > 1:
