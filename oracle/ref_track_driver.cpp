@@ -365,6 +365,32 @@ void rt_render_track(unsigned char* out, const int* res, const float* err, int W
   free(d);
 }
 
+// renderInstanceMaskKernel (mode 0, rendering.cpp:797-820),
+// renderMaskWithImageKernel (1, :679-723) and renderMaskMotionWithImageKernel
+// (2, :725-795) of a label image; mode 2 reads objs[label]'s trackresult_.
+void rt_render_mask(unsigned char* out, const float* rgb3, const int* label, int W, int H,
+                    int mode, const unsigned char* colors, int ncolors, void** objs, int nobjs) {
+  SegmentationResult seg(make_uint2(W, H));
+  seg.labelImg = cv::Mat(H, W, CV_32SC1, (void*)label);
+  std::vector<uchar4> col((size_t)ncolors);
+  std::memcpy(col.data(), colors, 4 * (size_t)ncolors);
+  if (mode == 0) {
+    renderInstanceMaskKernel((uchar4*)out, make_uint2(W, H), seg, col);
+  } else if (mode == 1) {
+    renderMaskWithImageKernel((uchar4*)out, make_uint2(W, H), (const float3*)rgb3, seg, col);
+  } else {
+    ObjectList l = borrowed_list(objs, nobjs);
+    renderMaskMotionWithImageKernel((uchar4*)out, make_uint2(W, H), (const float3*)rgb3, seg, l,
+                                    col);
+  }
+}
+
+// An object's trackresult_ result codes (2 x W x H: ICP rows, then photometric).
+void rt_object_set_results(void* o, const int* res, int W, int H) {
+  Object* ob = (Object*)o;
+  for (size_t i = 0; i < 2 * (size_t)W * H; ++i) ob->trackresult_[i].result = res[i];
+}
+
 // check_static_state (rendering.cpp:907-947): the inlier mask (255 / 0) of an
 // 8-bit object mask under the camera's residual rows (2 x W x H codes).
 void rt_check_static_state(unsigned char* inlier, const unsigned char* object_mask,

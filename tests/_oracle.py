@@ -452,6 +452,9 @@ def reference_tracking(path=REF_TRACK_SO):
         fn("rt_render_normal", None, U8P, FP, C.c_int, C.c_int)
         fn("rt_render_track", None, U8P, I32, FP, C.c_int, C.c_int, C.c_int)
         fn("rt_check_static_state", None, U8P, U8P, I32, C.c_int, C.c_int, C.c_int, C.c_int)
+        fn("rt_render_mask", None, U8P, FP, I32, C.c_int, C.c_int, C.c_int, U8P, C.c_int, V,
+           C.c_int)
+        fn("rt_object_set_results", None, P, I32, C.c_int, C.c_int)
         _cache[key] = lib
     return _cache[key]
 
@@ -576,6 +579,10 @@ class RefObject:
         self.lib.rt_object_pose(self.h, a, b)
         return a.reshape(4, 4), b.reshape(4, 4)
 
+    def set_results(self, res):
+        self.lib.rt_object_set_results(self.h, np.ascontiguousarray(res, np.int32).reshape(-1),
+                                       self.W, self.H)
+
     def take_results(self, trk):
         self.lib.rt_object_take_results(self.h, trk.h)
 
@@ -648,6 +655,16 @@ class RefRender:
         out = np.zeros((self.H, self.W, 4), np.uint8)
         self.lib.rt_render_track(out, np.ascontiguousarray(res, np.int32), _f32(err), self.W,
                                  self.H, int(mode))
+        return out
+
+    def mask(self, label, rgb3, mode, colors, objs=()):
+        """renderInstanceMaskKernel (0), renderMaskWithImageKernel (1),
+        renderMaskMotionWithImageKernel (2, objs[label]'s result rows)."""
+        out = np.zeros((self.H, self.W, 4), np.uint8)
+        col = np.ascontiguousarray(colors, np.uint8).reshape(-1, 4)
+        arr = self._objs(objs) if objs else None
+        self.lib.rt_render_mask(out, _f32(rgb3), np.ascontiguousarray(label, np.int32), self.W,
+                                self.H, int(mode), col, len(col), arr, len(objs))
         return out
 
     def static_inliers(self, object_mask, res, use_icp=True, use_rgb=True):

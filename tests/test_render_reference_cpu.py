@@ -126,3 +126,36 @@ def test_track_renders_and_static_state_match_reference(env):
             inl = e["RR"].static_inliers(om, res, icp, rgb)
             ratio = np.float32(np.count_nonzero(inl)) / np.float32(np.count_nonzero(om))
             assert ratio == np.float32(O.inlier_ratio(res.astype(np.int8), lm, label, icp, rgb))
+
+
+def test_mask_renders_match_reference(env):
+    """renderInstanceMaskKernel, renderMaskWithImageKernel and
+    renderMaskMotionWithImageKernel (rendering.cpp:679-820) against the
+    oracle, on the composite label image and every instance's residual rows.
+    Labels index the colour table; the reference reads colors[-2] (before the
+    vector) for an invalid label in the instance mask, undefined, so the
+    instance-mask comparison leaves those pixels out."""
+    e = env
+    s, k, T0 = e["s"], e["s"].k, e["T0"]
+    vm, nm, lm = e["RR"].raycast(e["objs"], T0, k, NEAR, FAR, MU)
+    assert (lm == -2).any() and (lm >= 0).all(where=lm != -2)
+    d1, rgb1, _ = s.render(1)
+    trk = O.RefTracker(W, H, k)
+    trk.set_frame(e["rgb"], e["d"])
+    trk.set_ref()
+    trk.set_frame(rgb1, d1)
+    Tc = trk.track_camera(T0, T0, vm, nm)
+    lv, _, _ = e["RR"].raycast(e["objs"], Tc, k, NEAR, FAR, MU)
+    res, _, _ = trk.compute_residuals(Tc, T0, vm, nm, lv)
+    for o in e["objs"]:
+        o.set_results(res)
+    rows = [res.astype(np.int8)] * len(e["objs"])
+    rgb3 = e["rgb3"]
+    ok = lm != -2
+    want = e["RR"].mask(lm, rgb3, 0, e["colors"])
+    got = e["R"].mask(lm, rgb3, 0, e["colors"])
+    assert np.array_equal(got[ok], want[ok])
+    for mode in (1, 2):
+        want = e["RR"].mask(lm, rgb3, mode, e["colors"], e["objs"] if mode == 2 else ())
+        got = e["R"].mask(lm, rgb3, mode, e["colors"], rows if mode == 2 else ())
+        assert np.array_equal(got, want), mode
