@@ -22,18 +22,19 @@ def pose_err(A, B):
 
 
 def check_pose(T_dev, T_ref, T_64, what, tol=POSE_TOL):
-    """The device's pose must be within tol (m / rad) of the reference's, or,
-    where the reference's own single-precision arithmetic already moves it
-    more than tol away from the all-FP64 run, no farther from the FP64 run
-    than the reference is: the device evaluates the same single-precision
-    rows but sums them in FP64, so it cannot follow the reference's rounding
-    to the last bit, and it must not be less accurate than the reference.
-    Returns True when the device is within tol of the reference."""
+    """The device's pose must lie within tol (m / rad) of the reference's,
+    widened by the reference's own single-precision error, its distance to
+    the all-FP64 run: the device evaluates the same single-precision rows but
+    sums them in FP64, so it cannot follow the reference's rounding to the
+    last bit, and where that rounding already moves the reference by r away
+    from the exact (FP64) solution, another rounding can land anywhere within
+    about r of it.  Returns True when the device is within tol of the
+    reference itself."""
     e_ref = pose_err(T_dev, T_ref)
     e_64 = pose_err(T_dev, T_64)
     r_64 = pose_err(T_ref, T_64)
     for k, name in ((0, "m"), (1, "rad")):
-        assert e_ref[k] <= tol or e_64[k] <= max(tol, r_64[k]), (
+        assert e_ref[k] <= tol + r_64[k], (
             f"{what}: device vs reference {e_ref[k]:.3g} {name}, device vs FP64 "
             f"{e_64[k]:.3g}, reference vs FP64 {r_64[k]:.3g}")
     return e_ref[0] <= tol and e_ref[1] <= tol
