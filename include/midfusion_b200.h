@@ -228,6 +228,18 @@ int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose
  * photometric reference depth of every pixel.  Voxel colours do not enter E.
  * The camera GN problem's state is overwritten.  Synchronises. */
 int mf_camera_cost(mf_context* ctx, const float T_live[16], double* out, float* d_grad_tsdf);
+/* Diagnostic, no reference counterpart: one GN step (the decision logic of
+ * tracking.cpp:287-335 / :657-686: cost test with step back, 6x6 solve,
+ * convergence test, SE(3) update) on given inputs, once by the device step
+ * that the batched GN runs (one warp per problem) and once by the host step of
+ * the plain path; the two must agree bit for bit.  state: n x 36 doubles
+ * (T[16], prevT[16], prev_err, kind 0 camera / 1 object, first iteration of a
+ * level 0/1, level); sums: n x 32 (the reduceKernel layout).  out_device,
+ * out_host: n x 68 doubles (T[16], prevT[16], prev_err, done, fallback to the
+ * truncated solve, iterations at the level, float pose[16], its inverse[16]).
+ * Allocates and synchronises. */
+int mf_debug_gn_step(mf_context* ctx, int n, const double* state, const double* sums,
+                     double* out_device, double* out_host);
 
 /* --- motion segmentation ------------------------------------------------
  * Tracking::compute_residuals (tracking/tracking.cpp:1535-1747) with the

@@ -35,6 +35,7 @@ EXPORTS = [
     "mf_track_info", "mf_track_eval", "mf_download_pyramid", "mf_process_frame",
     "mf_process_frame_device", "mf_get_poses", "mf_frame_stats", "mf_set_graphs",
     "mf_profile", "mf_track_eval_static", "mf_camera_cost", "mf_pool_tsdf", "mf_pool_slots",
+    "mf_debug_gn_step",
     "mf_motion_residuals", "mf_motion_download", "mf_track_results",
     "mf_refine_mask_use_motion", "mf_download_mask", "mf_retrack_camera",
     "mf_render_volume", "mf_render_depth", "mf_render_intensity", "mf_render_normal",
@@ -322,6 +323,19 @@ class Context:
         self._check(self.lib.mf_track_eval(self.h, slot, level, _ptr(p, np.float32),
                                            _ptr(sums, np.float64)))
         return sums
+
+    def debug_gn_step(self, state, sums):
+        """mf_debug_gn_step: state (n, 36), sums (n, 32) -> (device, host)
+        outputs, each (n, 68)."""
+        state = np.ascontiguousarray(state, np.float64)
+        sums = np.ascontiguousarray(sums, np.float64)
+        n = state.shape[0]
+        dev = np.zeros((n, 68), np.float64)
+        host = np.zeros((n, 68), np.float64)
+        self._check(self.lib.mf_debug_gn_step(self.h, n, _ptr(state, np.float64),
+                                              _ptr(sums, np.float64), _ptr(dev, np.float64),
+                                              _ptr(host, np.float64)))
+        return dev, host
 
     def camera_cost(self, T_live, grad_tsdf_ptr=None):
         """E, dE/d twist (6) and the number of rows (mf_camera_cost); when

@@ -648,6 +648,14 @@ int mf_track_eval_static(mf_context* ctx, int slot, int level, const float* pose
   return track_eval_static(ctx, slot, level, pose, sums);
 }
 
+int mf_debug_gn_step(mf_context* ctx, int n, const double* state, const double* sums,
+                     double* out_device, double* out_host) {
+  if (check(ctx) || n < 0 || n > 65535 || (n > 0 && (!state || !sums || !out_device || !out_host)))
+    return MF_E_ARG;
+  if (n == 0) return MF_OK;
+  return gn_step_check(ctx, n, state, sums, out_device, out_host);
+}
+
 int mf_camera_cost(mf_context* ctx, const float* T_live, double* out, float* d_grad_tsdf) {
   if (check(ctx) || !T_live || !out) return MF_E_ARG;
   if (ctx->inst.empty()) return MF_E_STATE;

@@ -159,6 +159,8 @@ int track_objects(Context* ctx, const IdList& ids);
 int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double* sums);
+int gn_step_check(Context* ctx, int n, const double* state, const double* sums, double* out_dev,
+                  double* out_host);
 int camera_cost(Context* ctx, const float* T_live16, int want_grad, double* out8, float* d_grad);
 int motion_residuals(Context* ctx, float threshold, float moved, float* ratio,
                      uint32_t* moving);

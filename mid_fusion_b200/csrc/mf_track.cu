@@ -432,8 +432,191 @@ MF_HD void gn_step(GNState& S, const double* s, int level) {
   S.invTf = inverse(Tf);
 }
 
-__device__ __noinline__ void gn_step_dev(GNState& S, const double* s, int level) {
-  gn_step(S, s, level);
+// gn_step by one whole warp (every lane of the calling warp, converged), with
+// the same operations in the same order on every value, so the results equal
+// the serial gn_step's bit for bit.  The serial step holds the 6x6 system, its
+// factor, the poses and the update in one thread and spills at the GN
+// kernels' register budget; here lane i < 6 holds row i of the factor, lane
+// l < 16 element l of the poses, and values move by shuffles.
+// first: the level's first iteration (prev_err starts at infinity).
+constexpr unsigned FULL_MASK = 0xffffffffu;
+
+// A[i][j] of the symmetric normal matrix from the 21 packed sums (makeJTJ).
+__device__ __forceinline__ double jtj_at(const double* v21, int i, int j) {
+  const int a = i < j ? i : j, b = i < j ? j : i;
+  return v21[a * 6 - a * (a - 1) / 2 + (b - a)];
+}
+
+// solve6 with the factor's rows on lanes 0..5; x (all lanes) and the
+// fallback flag as solve6 gives them.
+__device__ __forceinline__ bool solve6_warp(const double* s, int lane, double x[6]) {
+  const double* v21 = s + 7;
+  const int r = lane < 6 ? lane : 5;
+  double Lr[6], d[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) Lr[k] = 0.0;
+  double dmax = 0;
+  bool ok = true;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    double Lj[6];
+#pragma unroll
+    for (int k = 0; k < j; ++k) Lj[k] = __shfl_sync(FULL_MASK, Lr[k], j);
+    double dj = v21[j * 6 - j * (j - 1) / 2];
+#pragma unroll
+    for (int k = 0; k < j; ++k) dj -= Lj[k] * Lj[k] * d[k];
+    d[j] = dj;
+    dmax = fmax(dmax, dj);
+    ok = ok && (dj > 0);
+    const double inv = 1.0 / dj;
+    if (r > j) {
+      double v = jtj_at(v21, r, j);
+#pragma unroll
+      for (int k = 0; k < j; ++k) v -= Lr[k] * Lj[k] * d[k];
+      Lr[j] = v * inv;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) ok = ok && (d[j] > 1e-5 * dmax);
+  if (!ok) {  // the rare truncated eigen solve, serially on lane 0
+    if (lane == 0) {
+      double A[6][6], b[6];
+      make_jtj(v21, A);
+      for (int i = 0; i < 6; ++i) b[i] = s[1 + i];
+      solve6_eigen(A, b, 1e6, x);
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) x[i] = __shfl_sync(FULL_MASK, x[i], 0);
+    return true;
+  }
+  // forward substitution: y[i] on lane i, broadcast
+  double y[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double v = s[1 + i];
+#pragma unroll
+    for (int k = 0; k < i; ++k) v -= Lr[k] * y[k];
+    y[i] = __shfl_sync(FULL_MASK, v, i);
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) y[i] /= d[i];
+  // back substitution: the products L[k][i] x[k] on lane k, summed in order
+#pragma unroll
+  for (int i = 5; i >= 0; --i) {
+    double v = y[i];
+#pragma unroll
+    for (int k = i + 1; k < 6; ++k) v -= __shfl_sync(FULL_MASK, Lr[i] * x[k], k);
+    x[i] = v;
+  }
+  return false;
+}
+
+// W = [w]x of the rotation part, entry (i, j) for runtime i, j < 3.
+__device__ __forceinline__ double skew_at(int i, int j, double w0, double w1, double w2) {
+  if (i == j) return 0.0;
+  if (i == 0) return j == 1 ? -w2 : w1;
+  if (i == 1) return j == 0 ? w2 : -w0;
+  return j == 0 ? -w1 : w0;
+}
+
+__device__ __noinline__ void gn_step_warp(GNState* Sp, const double* s, int level, int first) {
+  GNState& S = *Sp;
+  const int lane = threadIdx.x & 31;
+  const int e = lane & 15;                 // pose element of this lane
+  const int kind = S.kind;
+  const double prev_err = first ? INFINITY : S.prev_err;
+  const double err = s[0] / s[28];
+  const float tf_old = reinterpret_cast<const float*>(&S.Tf)[e];
+  double Tl = S.T[e], Pl = S.prevT[e];
+  __syncwarp();
+  if (lane < 16) reinterpret_cast<float*>(&S.evalTf)[e] = tf_old;
+  if (kind == 1 && s[28] == 0) {  // no valid row: the object loop stops (:674-676)
+    if (lane == 0) {
+      S.prev_err = prev_err;
+      S.done = 1;
+      S.iters[level] += 1;
+    }
+    __syncwarp();
+    return;
+  }
+  int done = 0, fallback = 0;
+  double new_err = prev_err;
+  if (err > prev_err) {
+    Tl = Pl;
+    done = 1;
+  } else {
+    new_err = err;
+    double x[6];
+    if (solve6_warp(s, lane, x)) fallback = 1;
+    double nx = 0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) nx += x[i] * x[i];
+    if (sqrt(nx) < (double)1e-05f && sqrt(s[0] / s[28]) < 2e-3) {
+      done = 1;
+    } else {
+      // se3_exp(x): element (i, j) of the update on lane 4 i + j
+      const double w0 = x[3], w1 = x[4], w2 = x[5];
+      const double th2 = w0 * w0 + w1 * w1 + w2 * w2;
+      double A, B, C;
+      if (th2 < 1e-10) {
+        A = 1 - th2 / 6; B = 0.5 - th2 / 24; C = 1.0 / 6 - th2 / 120;
+      } else {
+        const double th = sqrt(th2);
+        double sn, cs;
+        sincos(th, &sn, &cs);
+        A = sn / th; B = (1 - cs) / th2; C = (1 - A) / th2;
+      }
+      const int i = e >> 2, j = e & 3;
+      double El;
+      if (i == 3) {
+        El = j == 3 ? 1.0 : 0.0;
+      } else if (j < 3) {
+        const double W2 = skew_at(i, 0, w0, w1, w2) * skew_at(0, j, w0, w1, w2) +
+                          skew_at(i, 1, w0, w1, w2) * skew_at(1, j, w0, w1, w2) +
+                          skew_at(i, 2, w0, w1, w2) * skew_at(2, j, w0, w1, w2);
+        const double I = i == j ? 1.0 : 0.0;
+        El = I + A * skew_at(i, j, w0, w1, w2) + B * W2;
+      } else {
+        double t = 0;
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+          const double W2 = skew_at(i, 0, w0, w1, w2) * skew_at(0, jj, w0, w1, w2) +
+                            skew_at(i, 1, w0, w1, w2) * skew_at(1, jj, w0, w1, w2) +
+                            skew_at(i, 2, w0, w1, w2) * skew_at(2, jj, w0, w1, w2);
+          const double I = i == jj ? 1.0 : 0.0;
+          t += (I + B * skew_at(i, jj, w0, w1, w2) + C * W2) * x[jj];
+        }
+        El = t;
+      }
+      // R = E T (mul4d)
+      double R = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        R += __shfl_sync(FULL_MASK, El, 4 * i + k) * __shfl_sync(FULL_MASK, Tl, 4 * k + j);
+      Pl = Tl;
+      Tl = R;
+    }
+  }
+  const float tf = (float)Tl;
+  float a[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) a[k] = __shfl_sync(FULL_MASK, tf, k);
+  if (lane < 16) {
+    S.T[e] = Tl;
+    S.prevT[e] = Pl;
+    reinterpret_cast<float*>(&S.Tf)[e] = tf;
+  }
+  if (lane == 0) {
+    M4 m;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) m.r[r] = F4{a[4 * r], a[4 * r + 1], a[4 * r + 2], a[4 * r + 3]};
+    S.invTf = inverse(m);
+    S.prev_err = new_err;
+    S.done = done;
+    if (fallback) S.fallback = 1;
+    S.iters[level] += 1;
+  }
+  __syncwarp();
 }
 
 // ------------------------------------------------------------------ residuals
@@ -913,13 +1096,10 @@ gn_iter_kernel(GNArgs a, IdList slots, int L) {
   __threadfence();
   __shared__ double tot[32];
   gn_tail_sums(a, s, (int)gridDim.x, sh, tot);
-  if (threadIdx.x < 32) S.sums[L][threadIdx.x] = tot[threadIdx.x];
-  if (threadIdx.x == 0) {
-    S.ticket = 0;
-    if (a.device_step) {
-      if (a.first_iter) S.prev_err = INFINITY;
-      gn_step_dev(S, tot, L);
-    }
+  if (threadIdx.x < 32) {
+    S.sums[L][threadIdx.x] = tot[threadIdx.x];
+    if (threadIdx.x == 0) S.ticket = 0;
+    if (a.device_step) gn_step_warp(&S, tot, L, a.first_iter);
   }
 }
 
@@ -968,7 +1148,7 @@ gn_level_kernel(GNArgs a, IdList slots, int L, int iters, int ntiles, unsigned* 
   __shared__ double sh[GN_THREADS / 32][32];
   __shared__ float red[GN_THREADS / 32][32][33];
   __shared__ double tot[32];
-  __shared__ int s_flag;
+  __shared__ int s_flag, s_done;
   const int items = slots.n * ntiles;
   for (int it = 0; it < iters; ++it) {
     for (int item = blockIdx.x; item < items; item += gridDim.x) {
@@ -991,10 +1171,9 @@ gn_level_kernel(GNArgs a, IdList slots, int L, int iters, int ntiles, unsigned* 
       gn_tail_sums(a, s, ntiles, sh, tot);
       if (threadIdx.x < 32) sS.sums[L][threadIdx.x] = tot[threadIdx.x];
       __syncthreads();
-      if (threadIdx.x == 0) {
-        sS.ticket = 0;
-        if (it == 0) sS.prev_err = INFINITY;
-        gn_step_dev(sS, tot, L);
+      if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) sS.ticket = 0;
+        gn_step_warp(&sS, tot, L, it == 0);
       }
       __syncthreads();
       state_store(&sS, a.st + s);
@@ -1014,15 +1193,19 @@ gn_level_kernel(GNArgs a, IdList slots, int L, int iters, int ntiles, unsigned* 
         }
         __nanosleep(64);
       }
-      if (flag == 0) {
-        int all = 1;
-        for (int i = 0; i < slots.n; ++i) all &= __ldcg(&a.st[slots.v[i]].done) != 0;
-        flag = all;
-      }
       s_flag = flag;
     }
     __syncthreads();
     if (s_flag != 0) return;
+    // the problems' done flags, one lane per problem
+    if (threadIdx.x < 32) {
+      int all = 1;
+      for (int i = threadIdx.x; i < slots.n; i += 32) all &= __ldcg(&a.st[slots.v[i]].done) != 0;
+      all = __all_sync(FULL_MASK, all);
+      if (threadIdx.x == 0) s_done = all;
+    }
+    __syncthreads();
+    if (s_done) return;
   }
 }
 
@@ -1751,6 +1934,89 @@ int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double
   MF_CUDA(cudaMemcpyAsync(sums, scratch + EVAL_SUMS_OFF, 32 * sizeof(double),
                           cudaMemcpyDeviceToHost, ctx->stream));
   MF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return MF_OK;
+}
+
+// ------------------------------------------------------------------------
+// The GN step on given inputs, on the device (gn_step_warp, one warp per
+// problem) and on the host (gn_step), for checking that the two agree.
+// state: n x 36 doubles: T[16], prevT[16], prev_err, kind, first, level;
+// sums: n x 32.  out_dev / out_host: n x 68 doubles: T[16], prevT[16],
+// prev_err, done, fallback, iterations at the level, Tf[16], invTf[16].
+__global__ void gn_step_check_kernel(GNState* st, const double* __restrict__ sums,
+                                     const int* __restrict__ first, const int* __restrict__ level) {
+  const int i = blockIdx.x;
+  gn_step_warp(st + i, sums + 32 * i, level[i], first[i]);
+}
+
+static void gn_step_out(const GNState& S, int level, double* o) {
+  for (int k = 0; k < 16; ++k) { o[k] = S.T[k]; o[16 + k] = S.prevT[k]; }
+  o[32] = S.prev_err;
+  o[33] = S.done;
+  o[34] = S.fallback;
+  o[35] = S.iters[level];
+  for (int k = 0; k < 16; ++k) {
+    o[36 + k] = m_at(S.Tf, k / 4, k % 4);
+    o[52 + k] = m_at(S.invTf, k / 4, k % 4);
+  }
+}
+
+int gn_step_check(Context* ctx, int n, const double* state, const double* sums, double* out_dev,
+                  double* out_host) {
+  std::vector<GNState> hs(n);
+  std::vector<int> first(n), level(n);
+  for (int i = 0; i < n; ++i) {
+    GNState& S = hs[i];
+    std::memset(&S, 0, sizeof(GNState));
+    const double* q = state + 36 * i;
+    for (int k = 0; k < 16; ++k) { S.T[k] = q[k]; S.prevT[k] = q[16 + k]; }
+    S.prev_err = q[32];
+    S.kind = (int)q[33];
+    first[i] = (int)q[34];
+    level[i] = (int)q[35];
+    if (level[i] < 0 || level[i] >= MAX_PYR || (S.kind != 0 && S.kind != 1)) {
+      ctx->last_error = "mf_debug_gn_step: level or kind out of range";
+      return MF_E_ARG;
+    }
+    S.Tf = to_m4f(S.T);
+    S.invTf = inverse(S.Tf);
+  }
+  GNState* d_st = nullptr;
+  double* d_sums = nullptr;
+  int* d_int = nullptr;
+  int rc = MF_OK;
+  if (cudaMalloc(&d_st, sizeof(GNState) * n) != cudaSuccess ||
+      cudaMalloc(&d_sums, sizeof(double) * 32 * n) != cudaSuccess ||
+      cudaMalloc(&d_int, sizeof(int) * 2 * n) != cudaSuccess) {
+    ctx->last_error = "mf_debug_gn_step: allocation failed";
+    rc = MF_E_CUDA;
+  }
+  std::vector<GNState> ds(n);
+  if (rc == MF_OK) {
+    cudaMemcpyAsync(d_st, hs.data(), sizeof(GNState) * n, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_sums, sums, sizeof(double) * 32 * n, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_int, first.data(), sizeof(int) * n, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_int + n, level.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
+                    ctx->stream);
+    gn_step_check_kernel<<<n, 32, 0, ctx->stream>>>(d_st, d_sums, d_int, d_int + n);
+    cudaMemcpyAsync(ds.data(), d_st, sizeof(GNState) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      ctx->last_error = std::string("mf_debug_gn_step: ") + cudaGetErrorString(e);
+      rc = MF_E_CUDA;
+    }
+  }
+  if (d_st) cudaFree(d_st);
+  if (d_sums) cudaFree(d_sums);
+  if (d_int) cudaFree(d_int);
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i) {
+    GNState& S = hs[i];
+    if (first[i]) S.prev_err = INFINITY;
+    gn_step(S, sums + 32 * i, level[i]);
+    gn_step_out(S, level[i], out_host + 68 * i);
+    gn_step_out(ds[i], level[i], out_dev + 68 * i);
+  }
   return MF_OK;
 }
 

@@ -110,10 +110,14 @@ class Shape:
     tint: np.ndarray     # rgb tint in [0,1]
     label: int = 0       # 0: part of the background instance
     twist: np.ndarray = None  # per-frame body twist (moving objects)
+    sway: float = 0.0    # > 0: the motion swings back and forth with this period (frames)
 
     def pose_at(self, f):
         if self.twist is None:
             return self.pose
+        if self.sway > 0:  # peak speed `twist` per frame, bounded excursion
+            t = self.sway / (2 * math.pi) * math.sin(2 * math.pi * f / self.sway)
+            return self.pose @ se3_exp(self.twist * t)
         return self.pose @ se3_exp(self.twist * f)
 
     def half_extent(self):
@@ -317,14 +321,16 @@ def _smooth_path(rng, n, base, target, max_step=0.009, max_rot_deg=0.9):
 
 
 def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_objects=3,
-               bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512, noise=True):
+               bg_size=512, bg_dim=5.12, obj_size=256, obj_dim=0.512, noise=True, sway=0.0):
     """``preset='room'``: one static room (plain method, one octree).
     ``preset='multi'``: background room + moving rigid objects, one octree each.
     ``preset='uneven'``: background room + ``n_objects`` (default use: 12) rigid
     primitives of seeded kinds and sizes (0.05-0.4 m), each with its own octree
     of 32^3, 64^3, 128^3 or 256^3 voxels at 2-5 mm; the largest object sits in
     the centre, the others on an ellipse around it, at depths chosen so that
-    their mask areas span about 0.5 %-25 % of the frame."""
+    their mask areas span about 0.5 %-25 % of the frame.  ``sway`` > 0 (frames):
+    each object swings along its twist with that period instead of moving at
+    a constant twist, so that long sequences keep every object in view."""
     rng = np.random.default_rng(seed)
     scale = width / 640.0
     k = (525.0 * scale, 525.0 * scale, (width - 1) / 2.0, (height - 1) / 2.0)
@@ -410,7 +416,8 @@ def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_ob
             p[:3, 3] = (cam0 @ np.array([x, y, z, 1.0]))[:3]
             tw = np.concatenate([rng.uniform(-1, 1, 3) * 0.004, rng.uniform(-1, 1, 3) *
                                  math.radians(0.6)])
-            sh = Shape(kind, size, p, rng.uniform(0.3, 1.0, 3), label=i + 1, twist=tw)
+            sh = Shape(kind, size, p, rng.uniform(0.3, 1.0, 3), label=i + 1, twist=tw,
+                       sway=sway)
             movers.append(sh)
             instances.append(Instance(i + 1, octree, dim, sh))
     return Scene(width, height, k, lo, hi, statics, movers, instances, cams, seed, noise)
