@@ -8,7 +8,8 @@
 * object tracking of every object against the reference (the
   single-precision oracle, equal to the reference's tracking.cpp bit for bit)
   and the all-FP64 oracle (tests/_pose.py: within 1e-5 m / rad of the
-  reference widened by the reference's own distance to the FP64 run).
+  reference, or no farther from the FP64 run than 1e-5 plus the reference's
+  own distance to it).
 """
 import ctypes as C
 
