@@ -305,12 +305,15 @@ def generalize_masks(labels, instance_labels):
 
 
 # --------------------------------------------------------------------------- presets
-def _smooth_path(rng, n, base, target, max_step=0.009, max_rot_deg=0.9):
-    amp = rng.uniform(0.5, 1.0, 3) * max_step * n / (2 * math.pi) * 0.9
+def _smooth_path(rng, n, base, target, max_step=0.009, max_rot_deg=0.9, period=0.0):
+    """One closed loop over the n frames (or, with period > 0, a loop every
+    `period` frames) of at most max_step per frame."""
+    per = period if period > 0 else n
+    amp = rng.uniform(0.5, 1.0, 3) * max_step * per / (2 * math.pi) * 0.9
     ph = rng.uniform(0, 2 * math.pi, 3)
     poses = []
     for f in range(n):
-        s = f / max(n, 1) * 2 * math.pi
+        s = f / max(per, 1) * 2 * math.pi
         eye = np.asarray(base) + amp * (np.sin(s + ph) - np.sin(ph))
         T = look_at(eye, target)
         ang = math.radians(max_rot_deg) * 0.3 * math.sin(0.7 * f + ph[0]) * min(f, 5) / 5
@@ -328,9 +331,10 @@ def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_ob
     primitives of seeded kinds and sizes (0.05-0.4 m), each with its own octree
     of 32^3, 64^3, 128^3 or 256^3 voxels at 2-5 mm; the largest object sits in
     the centre, the others on an ellipse around it, at depths chosen so that
-    their mask areas span about 0.5 %-25 % of the frame.  ``sway`` > 0 (frames):
-    each object swings along its twist with that period instead of moving at
-    a constant twist, so that long sequences keep every object in view."""
+    their mask areas span about 0.5 %-25 % of the frame.  ``sway`` > 0 (frames,
+    'uneven' only): each object swings along its twist with that period
+    instead of moving at a constant twist, and the camera loops with that
+    period, so that long sequences keep the objects in view."""
     rng = np.random.default_rng(seed)
     scale = width / 640.0
     k = (525.0 * scale, 525.0 * scale, (width - 1) / 2.0, (height - 1) / 2.0)
@@ -355,7 +359,7 @@ def make_scene(preset="multi", width=640, height=480, n_frames=100, seed=1, n_ob
         statics.append(Shape("box", (side, side, side), p, rng.uniform(0.4, 1.0, 3)))
     eye = np.array([c, c + 0.3, lo[2] + 0.7])
     target = np.array([c, c + 0.5, hi[2]])
-    cams = _smooth_path(rng, n_frames, eye, target)
+    cams = _smooth_path(rng, n_frames, eye, target, period=sway if preset == "uneven" else 0.0)
     instances = [Instance(0, bg_size, bg_dim)]
     movers = []
     if preset == "multi":

@@ -40,6 +40,18 @@ def test_uneven_workload_has_12_objects():
     assert {i.size for i in s.instances[1:]} <= {32, 64, 128, 256}
 
 
+def test_uneven_sequence_keeps_its_objects_in_view():
+    """The 200-frame uneven sequence: objects swing along their twists and the
+    camera loops, so most objects stay in view to the end."""
+    assert bench.UNEVEN_FRAMES == 200 and "200 frames" in bench.UNEVEN
+    s = bench.scene_for(0, bench.UNEVEN_FRAMES, "uneven")
+    for f in (0, 100, 199):
+        _, _, lab = s.render(f)
+        areas = [float((lab == i.label).mean()) for i in s.instances[1:]]
+        assert sum(a > 0.001 for a in areas) >= 9, (f, areas)
+        assert max(areas) > 0.15
+
+
 def test_launch_shape_options_parse():
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--help"],
                          capture_output=True, text=True, cwd=ROOT, timeout=120)
