@@ -149,10 +149,10 @@ def pose_check(scene, frames, gpu_cam, gpu_obj, gpu_maps, n, tol=1e-5):
     camera and objects separately, of device vs reference, device vs FP64 and
     reference vs FP64; one record per (frame, problem) with the three errors;
     and the criterion: a pose passes when it lies within `tol` of the
-    reference's, or no farther from the FP64 oracle's than tol plus the
-    reference's own distance to it (where the reference's single-precision
-    rounding already moves it by more than tol, no implementation with
-    another summation order can follow it to tol)."""
+    reference's and of the FP64 oracle's, widened by twice the reference's
+    own distance r to the FP64 oracle (where the reference's single-precision
+    rounding already moves it by r, another summation order lands elsewhere
+    within about r of the exact answer)."""
     _tests_path()
     import _oracle as O
     s = scene
@@ -175,7 +175,7 @@ def pose_check(scene, frames, gpu_cam, gpu_obj, gpu_maps, n, tol=1e-5):
             rec["device_vs_reference"] = [round(v, 9) for v in er]
             rec["reference_vs_fp64"] = [round(v, 9) for v in r64]
             rec["within_tol_of_reference"] = bool(max(er) <= tol)
-            rec["passes"] = bool(all(er[k] <= tol or e64[k] <= tol + r64[k] for k in (0, 1)))
+            rec["passes"] = bool(all(max(er[k], e64[k]) <= tol + 2 * r64[k] for k in (0, 1)))
         records.append(rec)
 
     have_ref = O.reference_tracking() is not None

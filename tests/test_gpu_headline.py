@@ -7,8 +7,8 @@ Frame by frame, in lockstep with the oracle:
 
 * camera and object poses against the reference and the all-FP64 oracle,
   each tracked from the device's previous-frame poses and model maps
-  (tests/_pose.py: within 1e-5 m / rad of the reference, or no farther from
-  the FP64 run than 1e-5 plus the reference's own distance to it);
+  (tests/_pose.py: within 1e-5 m / rad of the reference and of the FP64 run,
+  widened by twice the reference's own distance to the FP64 run);
 * integration of all four volumes at the device's poses: block keys, corner
   coordinates, active flags and every voxel field, bit-exact;
 * the composite raycast at the device's poses: vertex, normal and label

@@ -6,8 +6,8 @@ Frame by frame, through the whole pipeline (mf_process_frame), against the
 oracle in lockstep: camera tracking from the same model maps against the
 reference (the single-precision oracle, equal to the reference's
 tracking.cpp bit for bit) and the all-FP64 oracle (tests/_pose.py: within
-1e-5 m / rad of the reference, or no farther from the FP64 run than 1e-5
-plus the reference's own distance to it, which its single-precision
+1e-5 m / rad of the reference and of the FP64 run, widened by twice the
+reference's own distance r to the FP64 run, which its single-precision
 arithmetic makes up to ~1e-4 on this room's poorly conditioned poses;
 iteration counts equal where the
 reference and the FP64 run agree on them), then integration at the device's

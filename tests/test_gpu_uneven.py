@@ -7,9 +7,8 @@
   batched against plain: identical poses and volumes;
 * object tracking of every object against the reference (the
   single-precision oracle, equal to the reference's tracking.cpp bit for bit)
-  and the all-FP64 oracle (tests/_pose.py: within 1e-5 m / rad of the
-  reference, or no farther from the FP64 run than 1e-5 plus the reference's
-  own distance to it).
+  and the all-FP64 oracle (tests/_pose.py: within 1e-5 m / rad of both,
+  widened by twice the reference's own distance to the FP64 run).
 """
 import ctypes as C
 
