@@ -513,8 +513,11 @@ int mf_set_graphs(mf_context* ctx, int enable);
 /* No counterpart in the reference.  Batched GN runs every iteration of a
  * pyramid level in one cooperative launch per level and stage, with a grid
  * barrier between iterations and an early end once every problem has stopped
- * (1, the default), or one launch per iteration (0).  Both give the same
- * poses bit for bit.  Applies to frames captured after the call. */
+ * (1), or one launch per iteration, each chained to the previous one by
+ * programmatic dependent launch (0, the default: faster on B200, where the
+ * frame graph already removes the launch overhead and the grid barrier costs
+ * more than a launch boundary).  Both give the same poses bit for bit.
+ * Applies to frames captured after the call. */
 int mf_set_gn_persistent(mf_context* ctx, int enable);
 
 /* --- launch-shape autotuner (no counterpart in the reference) ----------

@@ -114,7 +114,7 @@ struct Context {
   float ray_epsilon = 0.f;          // ray iterator direction epsilon (first volume)
   void* graphs = nullptr;           // captured frame graphs (mf_pipeline.cu)
   bool use_graphs = true;
-  bool gn_persistent = true;        // batched GN: one cooperative launch per level
+  bool gn_persistent = false;       // batched GN: one cooperative launch per level
   TrackState* track = nullptr;
   Tune tune;                        // autotuned launch shapes
   // mf_process_frame_motion: frames it has processed, and two planes of

@@ -115,7 +115,13 @@ struct Gauss5 { float g[5]; };
 // bilateralFilterKernel, preprocessing.cpp:11-50 (e_d = 0.1, r = 2) on the
 // intensity (z = 0) and the depth (z = 1).  Neighbour coordinates clamp to the
 // image (the reference's host clamp on unsigned values goes through int min/max,
-// utils/cutil_math.h:51-57, 987-989).
+// utils/cutil_math.h:51-57, 987-989).  The range weight is the reference's
+// expf of the same float argument, evaluated as the double-precision exp
+// rounded to float: the host's expf returns the nearest float in all but rare
+// cases, and so does this (measured on a 640x480 frame: 99.94 % of the filtered
+// pixels equal the reference's bit for bit, against 72 % with the
+// single-precision expf, whose results differ from the nearest float by up to
+// 2 ulp); every later stage inherits the difference.
 __global__ void bilateral_kernel(const float* __restrict__ grey, const float* __restrict__ depth,
                                  float* __restrict__ out_i, float* __restrict__ out_d, int W,
                                  int H, Gauss5 gs) {
@@ -135,7 +141,7 @@ __global__ void bilateral_kernel(const float* __restrict__ grey, const float* __
       const float cur = in[cx + cy * W];
       if (cur > 0) {
         const float mod = sq(cur - center);
-        const float factor = gs.g[i + 2] * gs.g[j + 2] * expf(-mod / e2);
+        const float factor = gs.g[i + 2] * gs.g[j + 2] * (float)exp((double)(-mod / e2));
         t += factor * cur;
         sum += factor;
       }
@@ -511,12 +517,66 @@ __device__ __forceinline__ bool solve6_warp(const double* s, int lane, double x[
   return false;
 }
 
-// W = [w]x of the rotation part, entry (i, j) for runtime i, j < 3.
-__device__ __forceinline__ double skew_at(int i, int j, double w0, double w1, double w2) {
-  if (i == j) return 0.0;
-  if (i == 0) return j == 1 ? -w2 : w1;
-  if (i == 1) return j == 0 ? w2 : -w0;
-  return j == 0 ? -w1 : w0;
+// inverse(M4) by the lanes of one warp, the same operations on the same values
+// (so the same bits): lane j < 8 holds column j of [A | I] and the elimination
+// updates every column at once; the pivot column is broadcast by shuffles.
+// m_e: element (lane & 15) of A, row-major; returns element (lane & 15) of the
+// inverse.
+__device__ __forceinline__ float inverse_warp(float m_e, int lane) {
+  const int col = lane & 7;
+  float c[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float v = __shfl_sync(FULL_MASK, m_e, 4 * r + (col & 3));
+    c[r] = col < 4 ? v : (r == col - 4 ? 1.f : 0.f);
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float ac[4];
+#pragma unroll
+    for (int r = k; r < 4; ++r) ac[r] = __shfl_sync(FULL_MASK, c[r], k);
+    int p = k;
+    float best = fabsf(ac[k]);
+#pragma unroll
+    for (int r = k + 1; r < 4; ++r)
+      if (fabsf(ac[r]) > best) { best = fabsf(ac[r]); p = r; }
+#pragma unroll
+    for (int r = k + 1; r < 4; ++r) {
+      if (p == r) {
+        float t = c[k]; c[k] = c[r]; c[r] = t;
+        t = ac[k]; ac[k] = ac[r]; ac[r] = t;
+      }
+    }
+    // the columns of A left of k are not updated (inverse() starts at j = k)
+#pragma unroll
+    for (int r = k + 1; r < 4; ++r) {
+      const float f = ac[r] / ac[k];
+      if (col >= k) c[r] -= f * c[k];
+    }
+  }
+  // back substitution on the identity's columns (lanes 4..7), with the upper
+  // triangle of the eliminated A from lanes 0..3
+  float U[4][4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int k = r; k < 4; ++k) U[r][k] = __shfl_sync(FULL_MASK, c[r], k);
+  float R[4];
+#pragma unroll
+  for (int r = 3; r >= 0; --r) {
+    float s = c[r];
+#pragma unroll
+    for (int k = r + 1; k < 4; ++k) s -= U[r][k] * R[k];
+    R[r] = s / U[r][r];
+  }
+  const int i = (lane >> 2) & 3;
+  float out = 0.f;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float v = __shfl_sync(FULL_MASK, R[r], 4 + (lane & 3));
+    if (r == i) out = v;
+  }
+  return out;
 }
 
 __device__ __noinline__ void gn_step_warp(GNState* Sp, const double* s, int level, int first) {
@@ -566,27 +626,23 @@ __device__ __noinline__ void gn_step_warp(GNState* Sp, const double* s, int leve
         sincos(th, &sn, &cs);
         A = sn / th; B = (1 - cs) / th2; C = (1 - A) / th2;
       }
+      // every lane evaluates se3_exp's elements in its order (no divergence)
+      // and keeps element (i, j)
       const int i = e >> 2, j = e & 3;
-      double El;
-      if (i == 3) {
-        El = j == 3 ? 1.0 : 0.0;
-      } else if (j < 3) {
-        const double W2 = skew_at(i, 0, w0, w1, w2) * skew_at(0, j, w0, w1, w2) +
-                          skew_at(i, 1, w0, w1, w2) * skew_at(1, j, w0, w1, w2) +
-                          skew_at(i, 2, w0, w1, w2) * skew_at(2, j, w0, w1, w2);
-        const double I = i == j ? 1.0 : 0.0;
-        El = I + A * skew_at(i, j, w0, w1, w2) + B * W2;
-      } else {
+      const double W[3][3] = {{0, -w2, w1}, {w2, 0, -w0}, {-w1, w0, 0}};
+      double El = (i == 3 && j == 3) ? 1.0 : 0.0;
+#pragma unroll
+      for (int ii = 0; ii < 3; ++ii) {
         double t = 0;
 #pragma unroll
         for (int jj = 0; jj < 3; ++jj) {
-          const double W2 = skew_at(i, 0, w0, w1, w2) * skew_at(0, jj, w0, w1, w2) +
-                            skew_at(i, 1, w0, w1, w2) * skew_at(1, jj, w0, w1, w2) +
-                            skew_at(i, 2, w0, w1, w2) * skew_at(2, jj, w0, w1, w2);
-          const double I = i == jj ? 1.0 : 0.0;
-          t += (I + B * skew_at(i, jj, w0, w1, w2) + C * W2) * x[jj];
+          const double W2 = W[ii][0] * W[0][jj] + W[ii][1] * W[1][jj] + W[ii][2] * W[2][jj];
+          const double I = ii == jj ? 1.0 : 0.0;
+          const double v = I + A * W[ii][jj] + B * W2;
+          if (ii == i && jj == j) El = v;
+          t += (I + B * W[ii][jj] + C * W2) * x[jj];
         }
-        El = t;
+        if (ii == i && j == 3) El = t;
       }
       // R = E T (mul4d)
       double R = 0;
@@ -598,19 +654,14 @@ __device__ __noinline__ void gn_step_warp(GNState* Sp, const double* s, int leve
     }
   }
   const float tf = (float)Tl;
-  float a[16];
-#pragma unroll
-  for (int k = 0; k < 16; ++k) a[k] = __shfl_sync(FULL_MASK, tf, k);
+  const float itf = inverse_warp(tf, lane);
   if (lane < 16) {
     S.T[e] = Tl;
     S.prevT[e] = Pl;
     reinterpret_cast<float*>(&S.Tf)[e] = tf;
+    reinterpret_cast<float*>(&S.invTf)[e] = itf;
   }
   if (lane == 0) {
-    M4 m;
-#pragma unroll
-    for (int r = 0; r < 4; ++r) m.r[r] = F4{a[4 * r], a[4 * r + 1], a[4 * r + 2], a[4 * r + 3]};
-    S.invTf = inverse(m);
     S.prev_err = new_err;
     S.done = done;
     if (fallback) S.fallback = 1;
@@ -1072,12 +1123,54 @@ __device__ __forceinline__ void gn_tail_sums(const GNArgs& a, int s, int ntiles,
 // problem's GN step on the device.
 // KIND 0: the camera problem; KIND 1: object problems (one instantiation each
 // keeps the kernel's code small).
+// Programmatic dependent launch: the iterations of a level are chained so that
+// the next launch's CTAs start while the previous one finishes (its tail and
+// step), issue the prefetch of their pose-independent pixel data, and wait
+// (griddepcontrol.wait) before they read anything the previous launch writes
+// (the problem states, the partials).  Without the launch attribute the wait
+// returns at once.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.L1 [%0];" :: "l"(p));
+}
+
+// The pixel data of a tile that does not depend on the pose (live vertex,
+// normal, covariance and mask; rendered and live reference vertex, reference
+// intensity) into L1.  Written before the GN launches of a frame start.
+__device__ __forceinline__ void gn_prefetch(const GNArgs& a, int s, int L, int tile) {
+  const int n = a.pyr.w[L] * a.pyr.h[L];
+  const int ppt = gn_pix(L);
+#pragma unroll 1
+  for (int k = 0; k < ppt; ++k) {
+    const int p = tile * (GN_THREADS * ppt) + k * GN_THREADS + threadIdx.x;
+    if (p >= n) break;
+    if (a.use_icp) {
+      prefetch_l1(a.pyr.N[L] + p);
+      prefetch_l1(a.pyr.V[a.cur][L] + p);
+      prefetch_l1(a.pyr.COV[L] + p);
+      prefetch_l1(a.pyr.MASK[L] + p);
+    }
+    if (a.use_rgb) {
+      prefetch_l1(a.rV[s] + p);
+      prefetch_l1(a.pyr.V[1 - a.cur][L] + p);
+      prefetch_l1(a.pyr.I[1 - a.cur][L] + p);
+    }
+  }
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(GN_THREADS, MF_GN_MINB)
 gn_iter_kernel(GNArgs a, IdList slots, int L) {
   const int s = slots.v[blockIdx.y];
+  gn_prefetch(a, s, L, blockIdx.x);
+  griddep_wait();
   GNState& S = a.st[s];
   if (S.done && !a.first_iter) return;
+  // every CTA of this launch is resident: the next iteration may start
+  griddep_launch_dependents();
   __shared__ double sh[GN_THREADS / 32][32];
   __shared__ float red[GN_THREADS / 32][32][33];
   const double v = gn_tile_sums<KIND>(a, S, s, L, blockIdx.x, sh, red);
@@ -1498,8 +1591,25 @@ static cudaError_t launch_gn_level(const GNArgs& a, const IdList& slots, int L, 
                             status);
 }
 
+template <int KIND>
+static cudaError_t launch_gn_iter(const GNArgs& a, const IdList& slots, int L, int tiles,
+                                  bool overlap, cudaStream_t stream) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tiles, slots.n);
+  cfg.blockDim = dim3(GN_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = overlap ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, gn_iter_kernel<KIND>, a, slots, L);
+}
+
 static int gn_device(Context* ctx, const IdList& slots, int kind) {
   TrackState& T = *ctx->track;
+  bool chained = false;
   const bool persistent = ctx->gn_persistent && T.coop_blocks[kind] > 0;
   unsigned* bar = T.d_gnbar + kind * MAX_PYR;
   if (persistent) MF_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned) * MAX_PYR, ctx->stream));
@@ -1523,10 +1633,17 @@ static int gn_device(Context* ctx, const IdList& slots, int kind) {
     }
     for (int it = 0; it < iters; ++it) {
       a.first_iter = it == 0;  // the level's reset happens in its first iteration
-      if (kind == 0) gn_iter_kernel<0><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
-      else gn_iter_kernel<1><<<dim3(tiles, slots.n), GN_THREADS, 0, ctx->stream>>>(a, slots, L);
+      // every launch but the first of the chain overlaps its predecessor, a
+      // GN launch (which writes only problem states and partials)
+      const bool overlap = chained;
+      chained = true;
+      const cudaError_t e = kind == 0 ? launch_gn_iter<0>(a, slots, L, tiles, overlap, ctx->stream)
+                                      : launch_gn_iter<1>(a, slots, L, tiles, overlap, ctx->stream);
+      if (e != cudaSuccess) {
+        ctx->last_error = std::string("GN launch: ") + cudaGetErrorString(e);
+        return MF_E_CUDA;
+      }
     }
-    MF_CUDA(cudaGetLastError());
   }
   return MF_OK;
 }

@@ -1,5 +1,5 @@
 """Batched GN in one cooperative launch per pyramid level (mf_set_gn_persistent
-1, the default) against one launch per iteration (0) and against the plain
+1) against one launch per iteration (0, the default) and against the plain
 host-driven loop: the same poses bit for bit, frame after frame, for the
 3-object and the 12-object workloads; no barrier timed out."""
 import ctypes as C

@@ -92,6 +92,11 @@ def test_pyramid_matches_oracle():
             o = p.trk32.level(l, which)
             assert np.array_equal(g == 0, o == 0), f"{name} L{l}: zero pattern differs"
             np.testing.assert_allclose(g, o, rtol=2e-5, atol=1e-6, err_msg=f"{name} L{l}")
+            # the reference's arithmetic bit for bit except where the host's expf
+            # (bilateral range weights) misses the nearest float
+            if which in (0, 1, 2):
+                same = float(np.mean(g.view(np.int32) == o.view(np.int32)))
+                assert same >= 0.995, f"{name} L{l}: {same:.5f} of the values bit-equal"
         gn = p.ctx.pyramid(l, 3)
         on = p.trk32.level(l, 3)
         inv_g, inv_o = gn[..., 0] == -2, on[..., 0] == -2
