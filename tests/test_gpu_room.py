@@ -19,7 +19,7 @@ import numpy as np
 import pytest
 
 import _oracle as O
-from _pose import check_pose
+from _pose import camera_cost, check_pose
 from mid_fusion_b200 import build
 from mid_fusion_b200.capi import Context
 from mid_fusion_b200.scene import generalize_masks, make_scene
@@ -73,9 +73,10 @@ def test_room_sequence_in_lockstep_with_oracle(batched):
             T32 = trk32.track_camera(T_prev, T_prev, model[0], model[1])
             it32 = trk32.iterations()
             it, _, _ = ctx.track_info(0)
-            if it32 == it64:
+            ok = check_pose(T, T32, T_or, f"frame {f}",
+                            cost=camera_cost(trk, T_prev, model[0], model[1]))
+            if ok and it32 == it64:
                 assert list(it[:3]) == it64, (f, list(it[:3]), it64)
-            check_pose(T, T32, T_or, f"frame {f}")
         # integration and raycast at the device's pose, bit-exact
         mask = generalize_masks(lab, [0])[0]
         vol.integrate(d, rgb.astype(np.float32) / np.float32(255.0), mask, T, np.eye(4), s.k,

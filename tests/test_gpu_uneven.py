@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 import _oracle as O
-from _pose import check_pose
+from _pose import check_pose, object_cost
 from mid_fusion_b200 import build
 from mid_fusion_b200.capi import Context
 from mid_fusion_b200.scene import generalize_masks, make_scene
@@ -177,7 +177,8 @@ def test_uneven_objects_track_like_fp64_oracle(batched):
         it32 = trk[False].iterations()
         it, _, T_c2o2 = ctx.track_info(i)
         T_gpu = T1.astype(np.float64) @ T_c2o2
-        ok = check_pose(T_gpu, T32, T64, f"object {i} ({s.instances[i].size}^3)")
+        ok = check_pose(T_gpu, T32, T64, f"object {i} ({s.instances[i].size}^3)",
+                        cost=object_cost(trk[True], T_wo, T1, T0, v, n, lbl, labels[i]))
         if ok and it32 == it64:
             assert list(it[:3]) == it64, (i, list(it[:3]), it64)
         strict += ok
