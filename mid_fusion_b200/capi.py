@@ -35,7 +35,7 @@ EXPORTS = [
     "mf_track_info", "mf_track_eval", "mf_download_pyramid", "mf_process_frame",
     "mf_process_frame_device", "mf_get_poses", "mf_frame_stats", "mf_set_graphs",
     "mf_profile", "mf_track_eval_static", "mf_camera_cost", "mf_pool_tsdf", "mf_pool_slots",
-    "mf_debug_gn_step",
+    "mf_debug_gn_step", "mf_set_overlap",
     "mf_motion_residuals", "mf_motion_download", "mf_track_results",
     "mf_refine_mask_use_motion", "mf_download_mask", "mf_retrack_camera",
     "mf_render_volume", "mf_render_depth", "mf_render_intensity", "mf_render_normal",
@@ -271,6 +271,11 @@ class Context:
 
     def tune_set(self, stage, variant):
         self._check(self.lib.mf_tune_set(self.h, int(stage), int(variant)))
+
+    def set_overlap(self, ctas):
+        """mf_set_overlap: background integration overlapped with object
+        tracking on a low-priority stream with `ctas` CTAs (0: off)."""
+        self._check(self.lib.mf_set_overlap(self.h, int(ctas)))
 
     def set_gn_persistent(self, enable):
         self._check(self.lib.mf_set_gn_persistent(self.h, int(enable)))

@@ -122,9 +122,18 @@ int mf_create(const mf_config* cfg, mf_context** out) {
   ctx->H = cfg->height;
   cudaGetDevice(&ctx->device);
   auto fail = [&](int rc) { mf_destroy(ctx); return rc; };
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+  // the main stream at the highest priority, the side stream of the overlapped
+  // background integration at the lowest: pending CTAs of the frame's
+  // critical path (tracking) are dispatched first
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, prio_high) != cudaSuccess)
     return fail(MF_E_CUDA);
   ctx->own_stream = true;
+  if (cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess)
+    return fail(MF_E_CUDA);
   const size_t WH = (size_t)ctx->W * ctx->H;
   const size_t cap = (size_t)cfg->pool_blocks;
   Pool& P = ctx->pool;
@@ -205,6 +214,9 @@ int mf_destroy(mf_context* ctx) {
                 ctx->d_mc_tris};
   for (void* p : ps) if (p) cudaFree(p);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   delete ctx;
   return MF_OK;
 }
@@ -554,6 +566,15 @@ int mf_set_gn_persistent(mf_context* ctx, int enable) {
   if (check(ctx)) return MF_E_ARG;
   if (ctx->gn_persistent != (enable != 0)) {
     ctx->gn_persistent = enable != 0;
+    ++ctx->tune.gen;  // captured frame graphs are rebuilt
+  }
+  return MF_OK;
+}
+
+int mf_set_overlap(mf_context* ctx, int ctas) {
+  if (check(ctx) || ctas < 0 || ctas > 65535) return MF_E_ARG;
+  if (ctx->overlap_ctas != ctas) {
+    ctx->overlap_ctas = ctas;
     ++ctx->tune.gen;  // captured frame graphs are rebuilt
   }
   return MF_OK;

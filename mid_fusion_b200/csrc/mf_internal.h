@@ -115,6 +115,12 @@ struct Context {
   void* graphs = nullptr;           // captured frame graphs (mf_pipeline.cu)
   bool use_graphs = true;
   bool gn_persistent = false;       // batched GN: one cooperative launch per level
+  // batched frames: the background's allocation and integration run on a
+  // low-priority side stream while the objects are tracked (overlap_ctas:
+  // CTAs of that integration launch; 0 = in order on the main stream)
+  int overlap_ctas = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   TrackState* track = nullptr;
   Tune tune;                        // autotuned launch shapes
   // mf_process_frame_motion: frames it has processed, and two planes of
@@ -138,7 +144,7 @@ struct Context {
 // kernels / stages implemented in the .cu files
 int stage_prepare(Context* ctx, const IdList& ids);
 int stage_alloc(Context* ctx, const IdList& ids);
-int stage_integrate(Context* ctx, const IdList& ids);
+int stage_integrate(Context* ctx, const IdList& ids, int ctas = 0);
 int stage_raycast(Context* ctx, const IdList& ids, float epsilon);
 // The same raycast into other map buffers.
 int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex, F3* normal,
@@ -221,7 +227,7 @@ int int_variant_count();
 void int_variant_describe(int v, char* buf, int cap);
 // integrate_blocks_kernel alone, on `pool` (the live pool or a scratch copy),
 // over the visit list of the last stage_integrate / visit_list
-int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant);
+int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant, int ctas = 0);
 int build_visit_list(Context* ctx, uint32_t inst_mask);
 // the autotuner (mf_tune.cu)
 int tune_variant_count(int stage);

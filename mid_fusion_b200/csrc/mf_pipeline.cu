@@ -57,6 +57,41 @@ static int frame_body(Context* ctx, bool track, bool labels) {
   if (int rc = track_preprocess(ctx)) return rc;
   if (track) {
     if (int rc = track_camera(ctx, moving)) return rc;
+    if (objs.n && ctx->cfg.batched && ctx->overlap_ctas > 0) {
+      // The background's allocation and integration need the camera pose and
+      // the frame only, and object tracking reads neither the volumes nor the
+      // allocation and integration scratch: the background runs on the side
+      // stream (lowest priority, overlap_ctas integration CTAs) while the
+      // objects are tracked on the main stream; the objects' allocation and
+      // integration follow the join.  The values are those of the in-order
+      // frame (pool slots are handed out in another order).
+      IdList bg;
+      bg.n = 1;
+      bg.v[0] = 0;
+      MF_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
+      MF_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+      cudaStream_t main = ctx->stream;
+      ctx->stream = ctx->side;
+      int rc = stage_prepare(ctx, bg);
+      if (!rc) rc = stage_alloc(ctx, bg);
+      if (!rc) rc = stage_integrate(ctx, bg, ctx->overlap_ctas);
+      const cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->side);
+      ctx->stream = main;
+      if (!rc) rc = track_objects(ctx, objs);
+      // the side stream joins the main stream before any return, so that a
+      // stream capture ends cleanly
+      const cudaError_t j = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
+      if (rc) return rc;
+      if (e != cudaSuccess || j != cudaSuccess) {
+        ctx->last_error = "overlapped background integration: stream fork / join failed";
+        return MF_E_CUDA;
+      }
+      if (int rc2 = stage_prepare(ctx, objs)) return rc2;
+      if (int rc2 = stage_alloc(ctx, objs)) return rc2;
+      if (int rc2 = stage_integrate(ctx, objs)) return rc2;
+      if (int rc2 = stage_raycast(ctx, all, ctx->ray_epsilon)) return rc2;
+      return track_set_ref(ctx);
+    }
     if (objs.n)
       if (int rc = track_objects(ctx, objs)) return rc;
   }

@@ -714,15 +714,18 @@ void int_variant_describe(int v, char* buf, int cap) {
            int_variants[v].prefetch ? ", next block's fields prefetched to L2" : "");
 }
 
-int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant) {
+// ctas > 0: that many CTAs instead of the variant's residency times the SM
+// count (the grid-stride loop over the visit list gives the same voxels).
+int launch_integrate_blocks(Context* ctx, const Pool& pool, int variant, int ctas) {
   const mf_config& c = ctx->cfg;
   SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
   const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
   const IntVariant& v = int_variants[variant];
-  v.fn<<<sms * v.minb, 512, 0, ctx->stream>>>(pool, ctx->d_vols, ctx->d_frames, a, k,
-                                              ctx->d_visit, ctx->d_visit_count);
+  const int grid = ctas > 0 ? ctas : sms * v.minb;
+  v.fn<<<grid, 512, 0, ctx->stream>>>(pool, ctx->d_vols, ctx->d_frames, a, k, ctx->d_visit,
+                                      ctx->d_visit_count);
   MF_CUDA(cudaGetLastError());
   return MF_OK;
 }
@@ -737,7 +740,7 @@ int build_visit_list(Context* ctx, uint32_t inst_mask) {
   return MF_OK;
 }
 
-int stage_integrate(Context* ctx, const IdList& ids) {
+int stage_integrate(Context* ctx, const IdList& ids, int ctas) {
   if (ids.n == 0) return MF_OK;
   const mf_config& c = ctx->cfg;
   uint32_t mask = 0;
@@ -747,7 +750,7 @@ int stage_integrate(Context* ctx, const IdList& ids) {
     max_nodes = std::max(max_nodes, ctx->inst[ids.v[i]].vol.n_nodes);
   }
   if (int rc = build_visit_list(ctx, mask)) return rc;
-  if (int rc = launch_integrate_blocks(ctx, ctx->pool, ctx->tune.integrate)) return rc;
+  if (int rc = launch_integrate_blocks(ctx, ctx->pool, ctx->tune.integrate, ctas)) return rc;
   SdfArgs a{ctx->d_depth, ctx->d_rgb, ctx->d_masks, ctx->W, ctx->H, c.mu, (float)c.max_weight};
   const F4 k{c.k[0], c.k[1], c.k[2], c.k[3]};
   if (max_nodes > 0) {
