@@ -184,7 +184,8 @@ def run_ours(args, rank, world, local_rank):
     # device-resident inputs
     d_depth, d_rgb, d_lab = to_device(frames)
 
-    def run(batched, record_poses=True, scene=None, inputs=None, tune=None, persistent=None):
+    def run(batched, record_poses=True, scene=None, inputs=None, tune=None, persistent=None,
+            overlap=None):
         """Frames through mf_process_frame_device; device time per frame after
         1 + warmup untimed frames.  tune="auto": mf_autotune on the last
         warm-up frame (outside the timed region; its report lands in
@@ -193,6 +194,8 @@ def run_ours(args, rank, world, local_rank):
         ctx = make_ctx(batched, scene)
         if persistent is not None:
             ctx.set_gn_persistent(persistent)
+        if overlap is not None:
+            ctx.set_overlap(overlap)
         if isinstance(tune, dict):
             for stage, v in tune.items():
                 ctx.tune_set(stage, v)
@@ -272,6 +275,15 @@ def run_ours(args, rank, world, local_rank):
                                              "status_flags": st_q},
                     "same_poses": bool(same)}
         ctx_q.close()
+        # the background's integration in order instead of overlapped with
+        # object tracking (mf_set_overlap(ctx, 0))
+        ctx_o, t_o, poses_o, st_o = run(True, tune=tune_b, overlap=0)
+        same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                   for a, b in zip(poses_b, poses_o))
+        gn_modes["background_integration_in_order"] = {
+            "ms_per_step": round(1e3 * sum(t_o) / len(t_o), 4), "same_poses": bool(same),
+            "status_flags": st_o}
+        ctx_o.close()
     # ---- plain (one instance per launch, host-driven GN)
     ctx_p, t_p, poses_p, st_p = run(False, tune=tune_b)
     total_p = sum(t_p)

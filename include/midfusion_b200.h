@@ -519,14 +519,15 @@ int mf_set_graphs(mf_context* ctx, int enable);
  * more than a launch boundary).  Both give the same poses bit for bit.
  * Applies to frames captured after the call. */
 int mf_set_gn_persistent(mf_context* ctx, int enable);
-/* No counterpart in the reference.  Batched frames with objects: ctas > 0
- * runs the background's allocation and integration (which need only the
- * camera pose) on a low-priority side stream, with `ctas` integration CTAs,
- * while the objects are tracked on the context's stream (highest priority);
- * the objects' allocation and integration follow.  The volumes and poses are
- * the in-order frame's (pool slots are handed out in another order).
- * 0: everything in order on the context's stream.  Applies to frames
- * captured after the call. */
+/* No counterpart in the reference.  Batched frames with objects: the
+ * background's allocation and integration (which need only the camera pose)
+ * run on a low-priority side stream while the objects are tracked on the
+ * context's stream (highest priority); the objects' allocation and
+ * integration follow.  ctas < 0 (the default): the integration launch shape's
+ * own grid; ctas > 0: that many integration CTAs; 0: everything in order on
+ * the context's stream.  The volumes and poses are the in-order frame's (pool
+ * slots are handed out in another order).  Applies to frames captured after
+ * the call. */
 int mf_set_overlap(mf_context* ctx, int ctas);
 
 /* --- launch-shape autotuner (no counterpart in the reference) ----------

@@ -572,7 +572,8 @@ int mf_set_gn_persistent(mf_context* ctx, int enable) {
 }
 
 int mf_set_overlap(mf_context* ctx, int ctas) {
-  if (check(ctx) || ctas < 0 || ctas > 65535) return MF_E_ARG;
+  if (check(ctx) || ctas > 65535) return MF_E_ARG;
+  if (ctas < 0) ctas = -1;
   if (ctx->overlap_ctas != ctas) {
     ctx->overlap_ctas = ctas;
     ++ctx->tune.gen;  // captured frame graphs are rebuilt

@@ -117,8 +117,9 @@ struct Context {
   bool gn_persistent = false;       // batched GN: one cooperative launch per level
   // batched frames: the background's allocation and integration run on a
   // low-priority side stream while the objects are tracked (overlap_ctas:
-  // CTAs of that integration launch; 0 = in order on the main stream)
-  int overlap_ctas = 0;
+  // CTAs of that integration launch, < 0 the launch shape's own grid;
+  // 0 = in order on the main stream)
+  int overlap_ctas = -1;
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   TrackState* track = nullptr;

@@ -57,11 +57,12 @@ static int frame_body(Context* ctx, bool track, bool labels) {
   if (int rc = track_preprocess(ctx)) return rc;
   if (track) {
     if (int rc = track_camera(ctx, moving)) return rc;
-    if (objs.n && ctx->cfg.batched && ctx->overlap_ctas > 0) {
+    if (objs.n && ctx->cfg.batched && ctx->overlap_ctas != 0) {
       // The background's allocation and integration need the camera pose and
       // the frame only, and object tracking reads neither the volumes nor the
       // allocation and integration scratch: the background runs on the side
-      // stream (lowest priority, overlap_ctas integration CTAs) while the
+      // stream (lowest priority; overlap_ctas integration CTAs, or the launch
+      // shape's own grid) while the
       // objects are tracked on the main stream; the objects' allocation and
       // integration follow the join.  The values are those of the in-order
       // frame (pool slots are handed out in another order).
@@ -74,7 +75,7 @@ static int frame_body(Context* ctx, bool track, bool labels) {
       ctx->stream = ctx->side;
       int rc = stage_prepare(ctx, bg);
       if (!rc) rc = stage_alloc(ctx, bg);
-      if (!rc) rc = stage_integrate(ctx, bg, ctx->overlap_ctas);
+      if (!rc) rc = stage_integrate(ctx, bg, ctx->overlap_ctas > 0 ? ctx->overlap_ctas : 0);
       const cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->side);
       ctx->stream = main;
       if (!rc) rc = track_objects(ctx, objs);
@@ -153,7 +154,9 @@ int process_frame(Context* ctx, bool labels) {
       if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++kernels;
     }
     g.kernel_nodes[parity] = kernels;
-    MF_CUDA(cudaGraphInstantiate(&g.exec[parity], graph, 0));
+    // the kernel nodes keep the priorities of the streams they were captured
+    // from (the overlapped background integration runs at the lowest)
+    MF_CUDA(cudaGraphInstantiate(&g.exec[parity], graph, cudaGraphInstantiateFlagUseNodePriority));
     cudaGraphDestroy(graph);
   }
   MF_CUDA(cudaGraphLaunch(g.exec[parity], ctx->stream));

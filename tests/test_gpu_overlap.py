@@ -54,15 +54,18 @@ def test_overlapped_background_integration_equals_in_order(preset):
         s = make_scene("uneven", W, H, n_frames=3, seed=23, n_objects=12)
     frames = [s.render(f) for f in range(s.n_frames)]
     a, va, sa = _run(s, frames, 0)
-    b, vb, sb = _run(s, frames, 148)
-    assert sa == sb == 0
-    for f, ((ca, oa, ma), (cb, ob, mb)) in enumerate(zip(a, b)):
-        assert np.array_equal(ca, cb), f
-        for i, (x, y) in enumerate(zip(oa, ob)):
-            assert np.array_equal(x, y), (f, i)
-        for x, y in zip(ma, mb):
-            assert np.array_equal(x, y), f
-    for i, ((ka, ca, aa, xa), (kb, cb, ab, xb)) in enumerate(zip(va, vb)):
-        assert np.array_equal(ka, kb) and np.array_equal(ca, cb) and np.array_equal(aa, ab), i
-        for fld in FIELDS:
-            assert np.array_equal(xa[fld], xb[fld]), (i, fld)
+    b, vb, sb = _run(s, frames, -1)    # the default: the launch shape's own grid
+    c, vc, sc = _run(s, frames, 37)    # few CTAs: the background integration outlasts tracking
+    assert sa == sb == sc == 0
+    for other, vother in ((b, vb), (c, vc)):
+        for f, ((ca, oa, ma), (cb, ob, mb)) in enumerate(zip(a, other)):
+            assert np.array_equal(ca, cb), f
+            for i, (x, y) in enumerate(zip(oa, ob)):
+                assert np.array_equal(x, y), (f, i)
+            for x, y in zip(ma, mb):
+                assert np.array_equal(x, y), f
+        for i, ((ka, ca, aa, xa), (kb, cb, ab, xb)) in enumerate(zip(va, vother)):
+            assert np.array_equal(ka, kb) and np.array_equal(ca, cb), i
+            assert np.array_equal(aa, ab), i
+            for fld in FIELDS:
+                assert np.array_equal(xa[fld], xb[fld]), (i, fld)
