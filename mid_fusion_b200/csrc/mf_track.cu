@@ -114,18 +114,9 @@ struct Gauss5 { float g[5]; };
 
 // exp of a float argument, rounded to the nearest float (what the host's expf
 // returns in all but rare cases): the double-precision exp rounded to float.
-// For |x| < 2^-6 (most range weights of a smooth depth map) the degree-6
-// Taylor polynomial in double replaces it: its truncation error x^7 / 7! is
-// below 5e-17 relative, so the rounded results agree (checked against the
-// double exp on 8 million arguments in tests/test_kernel_identities_cpu.py).
-__device__ __forceinline__ float exp_nearest(float xf) {
-  const double x = (double)xf;
-  if (fabs(x) < 0.015625) {
-    return (float)(1.0 + x * (1.0 + x * (0.5 + x * (1.0 / 6 + x * (1.0 / 24 + x * (1.0 / 120 +
-                                                                               x * (1.0 / 720)))))));
-  }
-  return (float)exp(x);
-}
+// (A degree-6 Taylor polynomial for small arguments, which rounds alike, was
+// slower: the lanes of a warp split between the two paths.)
+__device__ __forceinline__ float exp_nearest(float x) { return (float)exp((double)x); }
 
 // bilateralFilterKernel, preprocessing.cpp:11-50 (e_d = 0.1, r = 2) on the
 // intensity (z = 0) and the depth (z = 1).  Neighbour coordinates clamp to the

@@ -44,21 +44,3 @@ def test_floor_test_equals_range_test_and_truncation(size):
     assert np.array_equal(v_r[ok_r], v_k[ok_k])
     assert np.all((v_k[ok_k] >= 0) & (v_k[ok_k] < size))
 
-
-def test_taylor_exp_rounds_like_the_double_exp():
-    """bilateral_kernel's exp_nearest (mf_track.cu): for |x| < 2^-6 the
-    degree-6 Taylor polynomial in double, evaluated in the kernel's order,
-    rounds to the same float as the double-precision exp, on 8 million float
-    arguments (uniform over the range, and small negative ones as smooth depth
-    maps give)."""
-    rng = np.random.default_rng(1)
-    # and the 1000 floats on either side just inside the range's ends
-    edge = (np.uint32(np.float32(2 ** -6).view(np.uint32)) -
-            np.arange(1, 1001, dtype=np.uint32)).view(np.float32).astype(np.float64)
-    x = np.concatenate([rng.uniform(-2 ** -6, 2 ** -6, 4_000_000),
-                        -np.abs(rng.normal(0, 1e-4, 4_000_000)), edge, -edge])
-    x = x.astype(np.float32).astype(np.float64)
-    x = x[np.abs(x) < 2 ** -6]
-    p = 1.0 + x * (1.0 + x * (0.5 + x * (1.0 / 6 + x * (1.0 / 24 + x * (1.0 / 120 +
-                                                                       x * (1.0 / 720))))))
-    assert np.array_equal(p.astype(np.float32), np.exp(x).astype(np.float32))
