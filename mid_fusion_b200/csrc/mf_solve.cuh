@@ -3,9 +3,9 @@
 // The reference solves x = pinv(JtJ) Jtr with TooN::GR_SVD::backsub(b, 1e6)
 // (apps/kfusion/include/commons.h:689-696): singular values below
 // sigma_max / 1e6 are dropped.  Here the well-conditioned case (all LDL^T
-// pivots within 1e-5 of the largest) is solved by LDL^T; otherwise the
-// symmetric matrix is diagonalised by cyclic Jacobi rotations and the same
-// truncated pseudo-inverse is applied.  The update exponentiates the twist
+// pivots within 1e-5 of the largest) is solved by Gauss-Jordan elimination;
+// otherwise the symmetric matrix is diagonalised by cyclic Jacobi rotations
+// and the same truncated pseudo-inverse is applied.  The update exponentiates the twist
 // (v, w) (translation first, as TooN::SE3 does) and left-multiplies the pose
 // (tracking.cpp:333-334).
 #pragma once
@@ -71,52 +71,47 @@ __host__ __device__ __noinline__ inline void solve6_eigen(const double Ain[6][6]
   }
 }
 
-// Returns true when the truncated eigen solve was needed.  All loops have
-// compile-time bounds and are unrolled, so the factorisation stays in registers.
+// Returns true when the truncated eigen solve was needed.  Gauss-Jordan
+// elimination without pivoting (the matrix is symmetric positive definite
+// when the solve is used): at step j every other row i subtracts
+// (a_ij / a_jj) times row j from its columns j..5 and from its right-hand
+// side, so after six steps x_i = b_i / a_ii.  The pivots a_jj are the LDL^T
+// pivots; all within 1e-5 of the largest, else the truncated eigen solve.
+// Each row's operations depend on the pivot row only, so the device runs the
+// rows on six lanes of a warp (gn_step_warp) with the same operations in the
+// same order.  All loops have compile-time bounds and are unrolled.
 MF_HD bool solve6(const double A[6][6], const double b[6], double x[6]) {
-  double L[6][6], d[6];
-  double dmax = 0;
+  double a[6][6], c[6], piv[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    c[i] = b[i];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) a[i][k] = A[i][k];
+  }
+  double pmax = 0;
   bool ok = true;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    double dj = A[j][j];
+    piv[j] = a[j][j];
+    pmax = fmax(pmax, a[j][j]);
+    ok = ok && (a[j][j] > 0);
 #pragma unroll
-    for (int k = 0; k < j; ++k) dj -= L[j][k] * L[j][k] * d[k];
-    d[j] = dj;
-    dmax = fmax(dmax, dj);
-    ok = ok && (dj > 0);
-    const double inv = 1.0 / dj;
+    for (int i = 0; i < 6; ++i) {
+      if (i == j) continue;
+      const double f = a[i][j] / a[j][j];
 #pragma unroll
-    for (int i = j + 1; i < 6; ++i) {
-      double v = A[i][j];
-#pragma unroll
-      for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k] * d[k];
-      L[i][j] = v * inv;
+      for (int k = j; k < 6; ++k) a[i][k] -= f * a[j][k];
+      c[i] -= f * c[j];
     }
   }
 #pragma unroll
-  for (int j = 0; j < 6; ++j) ok = ok && (d[j] > 1e-5 * dmax);
+  for (int j = 0; j < 6; ++j) ok = ok && (piv[j] > 1e-5 * pmax);
   if (!ok) {
     solve6_eigen(A, b, 1e6, x);
     return true;
   }
-  double y[6];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    double v = b[i];
-#pragma unroll
-    for (int k = 0; k < i; ++k) v -= L[i][k] * y[k];
-    y[i] = v;
-  }
-#pragma unroll
-  for (int i = 0; i < 6; ++i) y[i] /= d[i];
-#pragma unroll
-  for (int i = 5; i >= 0; --i) {
-    double v = y[i];
-#pragma unroll
-    for (int k = i + 1; k < 6; ++k) v -= L[k][i] * x[k];
-    x[i] = v;
-  }
+  for (int i = 0; i < 6; ++i) x[i] = c[i] / a[i][i];
   return false;
 }
 

@@ -446,10 +446,10 @@ MF_HD void gn_step(GNState& S, const double* s, int level) {
 
 // gn_step by one whole warp (every lane of the calling warp, converged), with
 // the same operations in the same order on every value, so the results equal
-// the serial gn_step's bit for bit.  The serial step holds the 6x6 system, its
-// factor, the poses and the update in one thread and spills at the GN
-// kernels' register budget; here lane i < 6 holds row i of the factor, lane
-// l < 16 element l of the poses, and values move by shuffles.
+// the serial gn_step's bit for bit.  The serial step holds the 6x6 system, the
+// poses and the update in one thread and spills at the GN kernels' register
+// budget; here lane i < 6 holds row i of the system, lane l < 16 element l of
+// the poses, and values move by shuffles.
 // first: the level's first iteration (prev_err starts at infinity).
 constexpr unsigned FULL_MASK = 0xffffffffu;
 
@@ -459,37 +459,35 @@ __device__ __forceinline__ double jtj_at(const double* v21, int i, int j) {
   return v21[a * 6 - a * (a - 1) / 2 + (b - a)];
 }
 
-// solve6 with the factor's rows on lanes 0..5; x (all lanes) and the
-// fallback flag as solve6 gives them.
+// solve6 with row i of the eliminated system on lane i < 6 (lanes 6..31
+// repeat row 5): the pivot row reaches every lane by shuffles; x (all lanes)
+// and the fallback flag as solve6 gives them.
 __device__ __forceinline__ bool solve6_warp(const double* s, int lane, double x[6]) {
   const double* v21 = s + 7;
   const int r = lane < 6 ? lane : 5;
-  double Lr[6], d[6];
+  double a[6], c = s[1 + r];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) Lr[k] = 0.0;
-  double dmax = 0;
+  for (int k = 0; k < 6; ++k) a[k] = jtj_at(v21, r, k);
+  double piv[6], pmax = 0;
   bool ok = true;
 #pragma unroll
   for (int j = 0; j < 6; ++j) {
-    double Lj[6];
+    double pr[6];
 #pragma unroll
-    for (int k = 0; k < j; ++k) Lj[k] = __shfl_sync(FULL_MASK, Lr[k], j);
-    double dj = v21[j * 6 - j * (j - 1) / 2];
+    for (int k = j; k < 6; ++k) pr[k] = __shfl_sync(FULL_MASK, a[k], j);
+    const double pc = __shfl_sync(FULL_MASK, c, j);
+    piv[j] = pr[j];
+    pmax = fmax(pmax, pr[j]);
+    ok = ok && (pr[j] > 0);
+    if (r != j) {
+      const double f = a[j] / pr[j];
 #pragma unroll
-    for (int k = 0; k < j; ++k) dj -= Lj[k] * Lj[k] * d[k];
-    d[j] = dj;
-    dmax = fmax(dmax, dj);
-    ok = ok && (dj > 0);
-    const double inv = 1.0 / dj;
-    if (r > j) {
-      double v = jtj_at(v21, r, j);
-#pragma unroll
-      for (int k = 0; k < j; ++k) v -= Lr[k] * Lj[k] * d[k];
-      Lr[j] = v * inv;
+      for (int k = j; k < 6; ++k) a[k] -= f * pr[k];
+      c -= f * pc;
     }
   }
 #pragma unroll
-  for (int j = 0; j < 6; ++j) ok = ok && (d[j] > 1e-5 * dmax);
+  for (int j = 0; j < 6; ++j) ok = ok && (piv[j] > 1e-5 * pmax);
   if (!ok) {  // the rare truncated eigen solve, serially on lane 0
     if (lane == 0) {
       double A[6][6], b[6];
@@ -501,25 +499,9 @@ __device__ __forceinline__ bool solve6_warp(const double* s, int lane, double x[
     for (int i = 0; i < 6; ++i) x[i] = __shfl_sync(FULL_MASK, x[i], 0);
     return true;
   }
-  // forward substitution: y[i] on lane i, broadcast
-  double y[6];
+  const double xr = c / a[r];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    double v = s[1 + i];
-#pragma unroll
-    for (int k = 0; k < i; ++k) v -= Lr[k] * y[k];
-    y[i] = __shfl_sync(FULL_MASK, v, i);
-  }
-#pragma unroll
-  for (int i = 0; i < 6; ++i) y[i] /= d[i];
-  // back substitution: the products L[k][i] x[k] on lane k, summed in order
-#pragma unroll
-  for (int i = 5; i >= 0; --i) {
-    double v = y[i];
-#pragma unroll
-    for (int k = i + 1; k < 6; ++k) v -= __shfl_sync(FULL_MASK, Lr[i] * x[k], k);
-    x[i] = v;
-  }
+  for (int i = 0; i < 6; ++i) x[i] = __shfl_sync(FULL_MASK, xr, i);
   return false;
 }
 
