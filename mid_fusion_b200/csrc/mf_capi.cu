@@ -154,6 +154,8 @@ int mf_create(const mf_config* cfg, mf_context** out) {
        cudaMalloc(&ctx->d_inst_label, sizeof(int) * MAX_INSTANCES) == cudaSuccess &&
        cudaMalloc(&ctx->d_visit, sizeof(int) * cap) == cudaSuccess &&
        cudaMalloc(&ctx->d_visit_count, sizeof(int)) == cudaSuccess &&
+       cudaMalloc(&ctx->d_visit_side, sizeof(int) * cap) == cudaSuccess &&
+       cudaMalloc(&ctx->d_visit_count_side, sizeof(int)) == cudaSuccess &&
        cudaMalloc(&ctx->d_depth, 4 * WH) == cudaSuccess &&
        cudaMalloc(&ctx->d_rgb8, 3 * WH) == cudaSuccess &&
        cudaMalloc(&ctx->d_rgb, sizeof(F3) * WH) == cudaSuccess &&
@@ -208,7 +210,7 @@ int mf_destroy(mf_context* ctx) {
   void* ps[] = {P.tsdf, P.wt, P.r, P.g, P.b, P.c, P.fg, P.w, P.meta, P.active, P.count,
                 ctx->d_vols, ctx->d_Two, ctx->d_Twc, ctx->d_frames, ctx->d_status,
                 ctx->d_reserved, ctx->d_inst_label, ctx->d_visit, ctx->d_visit_count,
-                ctx->d_depth, ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, ctx->d_masks,
+                ctx->d_visit_side, ctx->d_visit_count_side, ctx->d_depth, ctx->d_rgb8, ctx->d_rgb, ctx->d_grey, ctx->d_masks,
                 ctx->d_labels, ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->d_export,
                 ctx->d_render, ctx->d_render_small, ctx->d_rayhit, ctx->d_raytf,
                 ctx->d_mc_tris};
@@ -531,10 +533,13 @@ int mf_get_poses(mf_context* ctx, float* T_w_c, float* T_w_o) {
 
 int mf_frame_stats(mf_context* ctx, long long* out, int n) {
   if (check(ctx) || !out || n < 2) return MF_E_ARG;
-  int pc = 0, vc = 0;
+  int pc = 0, vc = 0, vs = 0;
   MF_CUDA(cudaMemcpyAsync(&pc, ctx->pool.count, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   MF_CUDA(cudaMemcpyAsync(&vc, ctx->d_visit_count, sizeof(int), cudaMemcpyDeviceToHost,
                           ctx->stream));
+  if (ctx->visit_side_used)
+    MF_CUDA(cudaMemcpyAsync(&vs, ctx->d_visit_count_side, sizeof(int), cudaMemcpyDeviceToHost,
+                            ctx->stream));
   std::vector<unsigned long long> em(ctx->inst.size(), 0);
   for (size_t i = 0; i < ctx->inst.size(); ++i)
     MF_CUDA(cudaMemcpyAsync(&em[i], ctx->inst[i].vol.emit_total, sizeof(unsigned long long),
@@ -543,7 +548,7 @@ int mf_frame_stats(mf_context* ctx, long long* out, int n) {
   // the device counter keeps counting requests once the pool is full
   // (MF_STATUS_POOL_FULL reports that): the blocks held are at most cap
   out[0] = std::min(pc, ctx->pool.cap);
-  out[1] = vc;
+  out[1] = vc + vs;  // the last frame's visited blocks (both lists when overlapped)
   for (size_t i = 0; i < ctx->inst.size() && (int)i + 2 < n; ++i) out[2 + i] = (long long)em[i];
   if ((int)ctx->inst.size() + 2 < n) out[2 + ctx->inst.size()] = (long long)graph_kernel_nodes(ctx);
   return MF_OK;

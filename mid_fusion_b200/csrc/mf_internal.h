@@ -88,6 +88,9 @@ struct Context {
   size_t export_bytes = 0;
   int* d_visit = nullptr;           // integration visit list
   int* d_visit_count = nullptr;
+  int* d_visit_side = nullptr;      // the side stream's visit list (overlapped frames)
+  int* d_visit_count_side = nullptr;
+  bool visit_side_used = false;     // the last batched frame used it
 
   // frame inputs
   float* d_depth = nullptr;         // W*H metres
@@ -147,6 +150,9 @@ int stage_prepare(Context* ctx, const IdList& ids);
 int stage_alloc(Context* ctx, const IdList& ids);
 int stage_integrate(Context* ctx, const IdList& ids, int ctas = 0);
 int stage_raycast(Context* ctx, const IdList& ids, float epsilon);
+bool raycast_is_phased(const Context* ctx);
+int stage_raycast_hits(Context* ctx, const IdList& ids, int base, float epsilon);
+int stage_raycast_fold(Context* ctx, const IdList& ids, float epsilon);
 // The same raycast into other map buffers.
 int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex, F3* normal,
                      int* label);

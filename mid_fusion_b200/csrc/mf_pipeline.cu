@@ -9,6 +9,7 @@
 // iteration from the host.
 #include <algorithm>
 #include <cstring>
+#include <utility>
 #include <vector>
 #include "mf_internal.h"
 
@@ -41,6 +42,7 @@ void pipeline_free(Context* ctx) {
 // Everything of one frame after the inputs are on the device.
 static int frame_body(Context* ctx, bool track, bool labels) {
   const int n = (int)ctx->inst.size();
+  ctx->visit_side_used = false;
   IdList all, objs;
   all.n = n;
   objs.n = 0;
@@ -58,27 +60,39 @@ static int frame_body(Context* ctx, bool track, bool labels) {
   if (track) {
     if (int rc = track_camera(ctx, moving)) return rc;
     if (objs.n && ctx->cfg.batched && ctx->overlap_ctas != 0) {
-      // The background's allocation and integration need the camera pose and
-      // the frame only, and object tracking reads neither the volumes nor the
-      // allocation and integration scratch: the background runs on the side
-      // stream (lowest priority; overlap_ctas integration CTAs, or the launch
-      // shape's own grid) while the
-      // objects are tracked on the main stream; the objects' allocation and
-      // integration follow the join.  The values are those of the in-order
-      // frame (pool slots are handed out in another order).
+      // The background's allocation, integration and (with the phased
+      // raycast) its marches need the camera pose and the frame only, and
+      // object tracking reads neither the volumes nor that scratch: the
+      // background runs on the side stream (lowest priority; overlap_ctas
+      // integration CTAs, or the launch shape's own grid, and a visit list of
+      // its own) while the objects are tracked, allocated and integrated on
+      // the main stream; the composite's fold follows the join.  The values
+      // are those of the in-order frame (pool slots are handed out in another
+      // order).
       IdList bg;
       bg.n = 1;
       bg.v[0] = 0;
+      const bool phased = raycast_is_phased(ctx);
+      ctx->visit_side_used = true;
       MF_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
       MF_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
       cudaStream_t main = ctx->stream;
       ctx->stream = ctx->side;
+      std::swap(ctx->d_visit, ctx->d_visit_side);
+      std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
       int rc = stage_prepare(ctx, bg);
       if (!rc) rc = stage_alloc(ctx, bg);
       if (!rc) rc = stage_integrate(ctx, bg, ctx->overlap_ctas > 0 ? ctx->overlap_ctas : 0);
+      if (!rc && phased) rc = stage_raycast_hits(ctx, bg, 0, ctx->ray_epsilon);
       const cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->side);
+      std::swap(ctx->d_visit, ctx->d_visit_side);
+      std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
       ctx->stream = main;
       if (!rc) rc = track_objects(ctx, objs);
+      if (!rc) rc = stage_prepare(ctx, objs);
+      if (!rc) rc = stage_alloc(ctx, objs);
+      if (!rc) rc = stage_integrate(ctx, objs);
+      if (!rc && phased) rc = stage_raycast_hits(ctx, objs, 1, ctx->ray_epsilon);
       // the side stream joins the main stream before any return, so that a
       // stream capture ends cleanly
       const cudaError_t j = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
@@ -87,10 +101,9 @@ static int frame_body(Context* ctx, bool track, bool labels) {
         ctx->last_error = "overlapped background integration: stream fork / join failed";
         return MF_E_CUDA;
       }
-      if (int rc2 = stage_prepare(ctx, objs)) return rc2;
-      if (int rc2 = stage_alloc(ctx, objs)) return rc2;
-      if (int rc2 = stage_integrate(ctx, objs)) return rc2;
-      if (int rc2 = stage_raycast(ctx, all, ctx->ray_epsilon)) return rc2;
+      if (int rc2 = phased ? stage_raycast_fold(ctx, all, ctx->ray_epsilon)
+                           : stage_raycast(ctx, all, ctx->ray_epsilon))
+        return rc2;
       return track_set_ref(ctx);
     }
     if (objs.n)

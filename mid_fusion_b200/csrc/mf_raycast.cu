@@ -318,7 +318,7 @@ template <int TW>
 __global__ void __launch_bounds__(128)
 raycast_hits_kernel(Pool pool, const Volume* __restrict__ vols,
                     const InstFrame* __restrict__ frames, IdList ids, RayArgs a, RayRec rec,
-                    int* __restrict__ status) {
+                    int rec_base, int* __restrict__ status) {
   const int x = blockIdx.x * TW + (threadIdx.x % TW);
   const int y = blockIdx.y * (128 / TW) + (threadIdx.x / TW);
   if (x >= a.W || y >= a.H) return;
@@ -342,7 +342,7 @@ raycast_hits_kernel(Pool pool, const Volume* __restrict__ vols,
                                a.farPlane, a.mu, step, step * 8, &tc);
     if (tc < INFINITY) fg = volume_interp(pool, V, mk3(hit.x, hit.y, hit.z), 1);
   }
-  const size_t q = (size_t)o * a.W * a.H + p;
+  const size_t q = (size_t)(rec_base + o) * a.W * a.H + p;
   rec.hit[q] = hit;
   rec.tf[q] = make_float2(tc, fg);
 }
@@ -771,7 +771,8 @@ int stage_raycast(Context* ctx, const IdList& ids, float epsilon) {
 // (raycast_hits_kernel + raycast_fold_kernel) by tile width.  Entry 0 is the
 // default.
 using RayFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, int*);
-using HitsFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, RayRec, int*);
+using HitsFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, RayRec, int,
+                        int*);
 using FoldFn = void (*)(Pool, const Volume*, const InstFrame*, IdList, RayArgs, RayRec);
 struct RayVariant {
   int tw, minb;
@@ -825,9 +826,46 @@ int stage_raycast_to(Context* ctx, const IdList& ids, float epsilon, F3* vertex,
     if (ids.n > ctx->cfg.max_instances) return MF_E_ARG;
     const RayRec rec{ctx->d_rayhit, ctx->d_raytf};
     r.hits<<<dim3(grid.x, grid.y, ids.n), 128, 0, ctx->stream>>>(
-        ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec, ctx->d_status);
+        ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec, 0, ctx->d_status);
     r.fold<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec);
   }
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+bool raycast_is_phased(const Context* ctx) { return ray_variants[ctx->tune.ray].fn == nullptr; }
+
+// The phased composite in parts: the per-instance marches of `ids` into the
+// records of list positions base .. base + ids.n - 1 (each instance's march
+// is independent of the others'), and the fold over the whole list.  Only
+// with a phased launch shape (raycast_is_phased).
+int stage_raycast_hits(Context* ctx, const IdList& ids, int base, float epsilon) {
+  if (ids.n == 0) return MF_OK;
+  const RayVariant& r = ray_variants[ctx->tune.ray];
+  if (r.fn || base < 0 || base + ids.n > ctx->cfg.max_instances) return MF_E_STATE;
+  const mf_config& c = ctx->cfg;
+  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H, c.near_plane,
+            c.far_plane, c.mu, epsilon};
+  const int th = 128 / r.tw;
+  const dim3 grid((ctx->W + r.tw - 1) / r.tw, (ctx->H + th - 1) / th, ids.n);
+  const RayRec rec{ctx->d_rayhit, ctx->d_raytf};
+  r.hits<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec, base,
+                                        ctx->d_status);
+  MF_CUDA(cudaGetLastError());
+  return MF_OK;
+}
+
+int stage_raycast_fold(Context* ctx, const IdList& ids, float epsilon) {
+  if (ids.n == 0) return MF_OK;
+  const RayVariant& r = ray_variants[ctx->tune.ray];
+  if (r.fn || ids.n > ctx->cfg.max_instances) return MF_E_STATE;
+  const mf_config& c = ctx->cfg;
+  RayArgs a{ctx->d_vertex, ctx->d_normal, ctx->d_label, ctx->W, ctx->H, c.near_plane,
+            c.far_plane, c.mu, epsilon};
+  const int th = 128 / r.tw;
+  const dim3 grid((ctx->W + r.tw - 1) / r.tw, (ctx->H + th - 1) / th);
+  const RayRec rec{ctx->d_rayhit, ctx->d_raytf};
+  r.fold<<<grid, 128, 0, ctx->stream>>>(ctx->pool, ctx->d_vols, ctx->d_frames, ids, a, rec);
   MF_CUDA(cudaGetLastError());
   return MF_OK;
 }

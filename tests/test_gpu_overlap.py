@@ -1,14 +1,16 @@
-"""The batched frame with the background's allocation and integration
-overlapped with object tracking (mf_set_overlap: a low-priority side stream
-joined into the frame graph) against the in-order frame: the same camera and
-object poses, the same voxels of every volume and the same model maps, bit for
-bit, frame after frame, for the 3-object and the 12-object workloads."""
+"""The batched frame with the background's allocation, integration and (with
+the phased raycast) its raycast marches overlapped with object tracking
+(mf_set_overlap: a low-priority side stream joined into the frame graph)
+against the in-order frame: the same camera and object poses, the same voxels
+of every volume and the same model maps, bit for bit, frame after frame, for
+the 3-object and the 12-object workloads, with the one-kernel and the phased
+raycast and with the integration's own grid or few CTAs."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
-from mid_fusion_b200 import build
+from mid_fusion_b200 import build, capi
 from mid_fusion_b200.capi import Context
 from mid_fusion_b200.scene import make_scene
 
@@ -22,9 +24,11 @@ def _built():
     build.build()
 
 
-def _run(s, frames, overlap):
+def _run(s, frames, overlap, ray=None):
     ctx = Context(s.width, s.height, k=s.k, pool_blocks=1 << 15, batched=True, robust="huber")
     ctx.set_overlap(overlap)
+    if ray is not None:
+        ctx.tune_set(capi.TUNE_RAYCAST, ray)
     for inst, T in zip(s.instances, s.volume_poses(0)):
         ctx.add_instance(inst.size, inst.dim, T, inst.label)
     ctx.set_camera_pose(s.cam_poses[0])
@@ -44,6 +48,14 @@ def _run(s, frames, overlap):
     return out, vols, st
 
 
+def capi_ray_count():
+    return capi.tune_candidates(capi.TUNE_RAYCAST)
+
+
+def capi_ray_describe(v):
+    return capi.tune_describe(capi.TUNE_RAYCAST, v)
+
+
 @pytest.mark.parametrize("preset", ["multi", "uneven"])
 def test_overlapped_background_integration_equals_in_order(preset):
     W, H = 320, 240
@@ -56,8 +68,12 @@ def test_overlapped_background_integration_equals_in_order(preset):
     a, va, sa = _run(s, frames, 0)
     b, vb, sb = _run(s, frames, -1)    # the default: the launch shape's own grid
     c, vc, sc = _run(s, frames, 37)    # few CTAs: the background integration outlasts tracking
-    assert sa == sb == sc == 0
-    for other, vother in ((b, vb), (c, vc)):
+    # the phased raycast: the background's marches on the side stream too
+    phased = [v for v in range(capi_ray_count()) if "phased" in capi_ray_describe(v)]
+    d, vd, sd = _run(s, frames, -1, ray=phased[-1])
+    e, ve, se = _run(s, frames, 37, ray=phased[0])
+    assert sa == sb == sc == sd == se == 0
+    for other, vother in ((b, vb), (c, vc), (d, vd), (e, ve)):
         for f, ((ca, oa, ma), (cb, ob, mb)) in enumerate(zip(a, other)):
             assert np.array_equal(ca, cb), f
             for i, (x, y) in enumerate(zip(oa, ob)):
