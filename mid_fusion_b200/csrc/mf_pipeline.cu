@@ -54,12 +54,31 @@ static int frame_body(Context* ctx, bool track, bool labels) {
       if (ctx->inst[i].label >= 0 && ctx->inst[i].label < 32) moving |= 1u << ctx->inst[i].label;
     }
   }
-  if (labels && n > 0)
+  const bool overlap = track && objs.n && ctx->cfg.batched && ctx->overlap_ctas != 0;
+  const bool gen = labels && n > 0;
+  if (gen && overlap) {
+    // the integration masks are needed only by allocation and integration:
+    // generalised on the side stream while the pyramid and the camera are
+    // tracked (the main stream waits for them before the objects' allocation)
+    MF_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+    MF_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_start, 0));
+    cudaStream_t main = ctx->stream;
+    ctx->stream = ctx->side;
+    const int rc = launch_generalize(ctx);
+    const cudaError_t e = cudaEventRecord(ctx->ev_gen, ctx->side);
+    ctx->stream = main;
+    if (rc || e != cudaSuccess) {
+      cudaStreamWaitEvent(ctx->stream, ctx->ev_gen, 0);  // joins the side stream
+      if (!rc) ctx->last_error = "overlapped mask generalisation: event record failed";
+      return rc ? rc : MF_E_CUDA;
+    }
+  } else if (gen) {
     if (int rc = launch_generalize(ctx)) return rc;
+  }
   if (int rc = track_preprocess(ctx)) return rc;
   if (track) {
     if (int rc = track_camera(ctx, moving)) return rc;
-    if (objs.n && ctx->cfg.batched && ctx->overlap_ctas != 0) {
+    if (overlap) {
       // The background's allocation, integration and (with the phased
       // raycast) its marches need the camera pose and the frame only, and
       // object tracking reads neither the volumes nor that scratch: the
@@ -89,6 +108,10 @@ static int frame_body(Context* ctx, bool track, bool labels) {
       std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
       ctx->stream = main;
       if (!rc) rc = track_objects(ctx, objs);
+      if (!rc && gen && cudaStreamWaitEvent(ctx->stream, ctx->ev_gen, 0) != cudaSuccess) {
+        ctx->last_error = "overlapped mask generalisation: stream wait failed";
+        rc = MF_E_CUDA;
+      }
       if (!rc) rc = stage_prepare(ctx, objs);
       if (!rc) rc = stage_alloc(ctx, objs);
       if (!rc) rc = stage_integrate(ctx, objs);
