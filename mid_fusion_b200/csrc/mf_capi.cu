@@ -132,6 +132,7 @@ int mf_create(const mf_config* cfg, mf_context** out) {
   ctx->own_stream = true;
   if (cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_pre, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_gen, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess)
@@ -220,6 +221,7 @@ int mf_destroy(mf_context* ctx) {
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+  if (ctx->ev_pre) cudaEventDestroy(ctx->ev_pre);
   if (ctx->ev_gen) cudaEventDestroy(ctx->ev_gen);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);

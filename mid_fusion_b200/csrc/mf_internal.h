@@ -124,7 +124,8 @@ struct Context {
   // 0 = in order on the main stream)
   int overlap_ctas = -1;
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_start = nullptr, ev_gen = nullptr, ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_pre = nullptr, ev_gen = nullptr, ev_fork = nullptr,
+              ev_join = nullptr;
   TrackState* track = nullptr;
   Tune tune;                        // autotuned launch shapes
   // mf_process_frame_motion: frames it has processed, and two planes of
@@ -169,6 +170,13 @@ int track_preprocess(Context* ctx);
 int track_set_ref(Context* ctx);
 int track_camera(Context* ctx, uint32_t moving, int retrack = 0);
 int track_objects(Context* ctx, const IdList& ids);
+// the same in phases, for a frame that runs the pose-independent parts on
+// another stream: track_camera = pre + mask + gn; track_objects = pre + gn
+int track_camera_pre(Context* ctx, int retrack = 0);
+int track_camera_mask(Context* ctx, uint32_t moving);
+int track_camera_gn(Context* ctx);
+int track_objects_pre(Context* ctx, const IdList& ids);
+int track_objects_gn(Context* ctx, const IdList& ids);
 int track_info(Context* ctx, int slot, int* iters, double* sums, double* T64);
 int track_eval(Context* ctx, int slot, int L, const float* pose16, double* sums);
 int track_eval_static(Context* ctx, int slot, int L, const float* pose16, double* sums);

@@ -39,6 +39,79 @@ void pipeline_free(Context* ctx) {
   ctx->graphs = nullptr;
 }
 
+// A batched frame with objects, in two branches of one graph.  The main
+// stream (highest priority) runs the critical path: the pyramid, the camera's
+// outlier mask and GN, the objects' GN, allocation, integration and raycast
+// marches, and the composite's fold.  The side stream (lowest priority) runs
+// what does not wait for it: first the tracking setup that needs no live
+// frame and no tracked pose (the camera's and the objects' problems from the
+// previous poses, their rendered references) and the integration masks while
+// the pyramid is built; then, once the camera is tracked, the background's
+// allocation, integration (own visit list, overlap_ctas CTAs or the launch
+// shape's own grid) and raycast marches while the objects are tracked.
+// Nothing one branch reads is written by the other before the event that
+// orders them, so the frame equals the in-order frame bit for bit (pool
+// slots are handed out in another order).  Every event is recorded and
+// waited on whatever happens, so that a stream capture always ends joined.
+static int frame_overlapped(Context* ctx, bool gen, const IdList& all, const IdList& objs,
+                            uint32_t moving) {
+  IdList bg;
+  bg.n = 1;
+  bg.v[0] = 0;
+  const bool phased = raycast_is_phased(ctx);
+  cudaStream_t main = ctx->stream, side = ctx->side;
+  int rc = MF_OK;
+  cudaError_t e = cudaSuccess;
+  auto ok = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
+  ctx->visit_side_used = true;
+  // side: the pose-independent tracking setup, then the masks
+  ok(cudaEventRecord(ctx->ev_start, main));
+  ok(cudaStreamWaitEvent(side, ctx->ev_start, 0));
+  ctx->stream = side;
+  rc = track_camera_pre(ctx, 0);
+  if (!rc) rc = track_objects_pre(ctx, objs);
+  ok(cudaEventRecord(ctx->ev_pre, side));
+  if (!rc && gen) rc = launch_generalize(ctx);
+  ok(cudaEventRecord(ctx->ev_gen, side));
+  ctx->stream = main;
+  // main: the pyramid, the camera's outlier mask, the camera's GN
+  if (!rc) rc = track_preprocess(ctx);
+  if (!rc) rc = track_camera_mask(ctx, moving);
+  ok(cudaStreamWaitEvent(main, ctx->ev_pre, 0));
+  if (!rc) rc = track_camera_gn(ctx);
+  ok(cudaEventRecord(ctx->ev_fork, main));
+  // side: the background, at the tracked camera pose
+  ok(cudaStreamWaitEvent(side, ctx->ev_fork, 0));
+  ctx->stream = side;
+  std::swap(ctx->d_visit, ctx->d_visit_side);
+  std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
+  if (!rc) rc = stage_prepare(ctx, bg);
+  if (!rc) rc = stage_alloc(ctx, bg);
+  if (!rc) rc = stage_integrate(ctx, bg, ctx->overlap_ctas > 0 ? ctx->overlap_ctas : 0);
+  if (!rc && phased) rc = stage_raycast_hits(ctx, bg, 0, ctx->ray_epsilon);
+  ok(cudaEventRecord(ctx->ev_join, side));
+  std::swap(ctx->d_visit, ctx->d_visit_side);
+  std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
+  ctx->stream = main;
+  // main: the objects
+  if (!rc) rc = track_objects_gn(ctx, objs);
+  ok(cudaStreamWaitEvent(main, ctx->ev_gen, 0));
+  if (!rc) rc = stage_prepare(ctx, objs);
+  if (!rc) rc = stage_alloc(ctx, objs);
+  if (!rc) rc = stage_integrate(ctx, objs);
+  if (!rc && phased) rc = stage_raycast_hits(ctx, objs, 1, ctx->ray_epsilon);
+  ok(cudaStreamWaitEvent(main, ctx->ev_join, 0));
+  if (rc) return rc;
+  if (e != cudaSuccess) {
+    ctx->last_error = std::string("overlapped frame: ") + cudaGetErrorString(e);
+    return MF_E_CUDA;
+  }
+  if (int rc2 = phased ? stage_raycast_fold(ctx, all, ctx->ray_epsilon)
+                       : stage_raycast(ctx, all, ctx->ray_epsilon))
+    return rc2;
+  return track_set_ref(ctx);
+}
+
 // Everything of one frame after the inputs are on the device.
 static int frame_body(Context* ctx, bool track, bool labels) {
   const int n = (int)ctx->inst.size();
@@ -54,81 +127,14 @@ static int frame_body(Context* ctx, bool track, bool labels) {
       if (ctx->inst[i].label >= 0 && ctx->inst[i].label < 32) moving |= 1u << ctx->inst[i].label;
     }
   }
-  const bool overlap = track && objs.n && ctx->cfg.batched && ctx->overlap_ctas != 0;
   const bool gen = labels && n > 0;
-  if (gen && overlap) {
-    // the integration masks are needed only by allocation and integration:
-    // generalised on the side stream while the pyramid and the camera are
-    // tracked (the main stream waits for them before the objects' allocation)
-    MF_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
-    MF_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_start, 0));
-    cudaStream_t main = ctx->stream;
-    ctx->stream = ctx->side;
-    const int rc = launch_generalize(ctx);
-    const cudaError_t e = cudaEventRecord(ctx->ev_gen, ctx->side);
-    ctx->stream = main;
-    if (rc || e != cudaSuccess) {
-      cudaStreamWaitEvent(ctx->stream, ctx->ev_gen, 0);  // joins the side stream
-      if (!rc) ctx->last_error = "overlapped mask generalisation: event record failed";
-      return rc ? rc : MF_E_CUDA;
-    }
-  } else if (gen) {
+  if (track && objs.n && ctx->cfg.batched && ctx->overlap_ctas != 0)
+    return frame_overlapped(ctx, gen, all, objs, moving);
+  if (gen)
     if (int rc = launch_generalize(ctx)) return rc;
-  }
   if (int rc = track_preprocess(ctx)) return rc;
   if (track) {
     if (int rc = track_camera(ctx, moving)) return rc;
-    if (overlap) {
-      // The background's allocation, integration and (with the phased
-      // raycast) its marches need the camera pose and the frame only, and
-      // object tracking reads neither the volumes nor that scratch: the
-      // background runs on the side stream (lowest priority; overlap_ctas
-      // integration CTAs, or the launch shape's own grid, and a visit list of
-      // its own) while the objects are tracked, allocated and integrated on
-      // the main stream; the composite's fold follows the join.  The values
-      // are those of the in-order frame (pool slots are handed out in another
-      // order).
-      IdList bg;
-      bg.n = 1;
-      bg.v[0] = 0;
-      const bool phased = raycast_is_phased(ctx);
-      ctx->visit_side_used = true;
-      MF_CUDA(cudaEventRecord(ctx->ev_fork, ctx->stream));
-      MF_CUDA(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
-      cudaStream_t main = ctx->stream;
-      ctx->stream = ctx->side;
-      std::swap(ctx->d_visit, ctx->d_visit_side);
-      std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
-      int rc = stage_prepare(ctx, bg);
-      if (!rc) rc = stage_alloc(ctx, bg);
-      if (!rc) rc = stage_integrate(ctx, bg, ctx->overlap_ctas > 0 ? ctx->overlap_ctas : 0);
-      if (!rc && phased) rc = stage_raycast_hits(ctx, bg, 0, ctx->ray_epsilon);
-      const cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->side);
-      std::swap(ctx->d_visit, ctx->d_visit_side);
-      std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
-      ctx->stream = main;
-      if (!rc) rc = track_objects(ctx, objs);
-      if (!rc && gen && cudaStreamWaitEvent(ctx->stream, ctx->ev_gen, 0) != cudaSuccess) {
-        ctx->last_error = "overlapped mask generalisation: stream wait failed";
-        rc = MF_E_CUDA;
-      }
-      if (!rc) rc = stage_prepare(ctx, objs);
-      if (!rc) rc = stage_alloc(ctx, objs);
-      if (!rc) rc = stage_integrate(ctx, objs);
-      if (!rc && phased) rc = stage_raycast_hits(ctx, objs, 1, ctx->ray_epsilon);
-      // the side stream joins the main stream before any return, so that a
-      // stream capture ends cleanly
-      const cudaError_t j = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
-      if (rc) return rc;
-      if (e != cudaSuccess || j != cudaSuccess) {
-        ctx->last_error = "overlapped background integration: stream fork / join failed";
-        return MF_E_CUDA;
-      }
-      if (int rc2 = phased ? stage_raycast_fold(ctx, all, ctx->ray_epsilon)
-                           : stage_raycast(ctx, all, ctx->ray_epsilon))
-        return rc2;
-      return track_set_ref(ctx);
-    }
     if (objs.n)
       if (int rc = track_objects(ctx, objs)) return rc;
   }

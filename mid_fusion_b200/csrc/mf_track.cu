@@ -349,25 +349,23 @@ __global__ void setup_camera_kernel(GNState* st, const float* __restrict__ Twc,
 
 // trackEachObject setup, tracking.cpp:586-593: T_c1_o1 = inverse(T_w_c1) T_wo1,
 // T_c2_o2 = inverse(T_w_c2) T_wo1 with T_w_c2 the freshly tracked camera.
-__global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __restrict__ Twc2,
-                                     const float* __restrict__ Twc1, const float* __restrict__ Two,
-                                     const int* __restrict__ inst_label) {
-  const int t = threadIdx.x;
-  if (t >= slots.n) return;
-  const int s = slots.v[t];
-  GNState& S = st[s];
-  const M4 T_w_c2 = load_m4(Twc2), T_w_c1 = load_m4(Twc1), T_wo1 = load_m4(Two + 16 * s);
-  S.kind = 1; S.inst = s; S.label = inst_label[s]; S.done = 0; S.ticket = 0; S.fallback = 0;
+// The part that does not need T_w_c2 (the previous camera pose, the object's
+// last pose, the rendered reference's label box) and the part that does.
+__device__ void setup_object_pre(GNState& S, int s, const M4& T_w_c1, const M4& T_wo1,
+                                 int label) {
+  S.kind = 1; S.inst = s; S.label = label; S.done = 0; S.ticket = 0; S.fallback = 0;
   for (int l = 0; l < MAX_PYR; ++l) S.iters[l] = 0;
   S.box[0] = S.box[1] = INT_MAX;
   S.box[2] = S.box[3] = -1;
-  S.T_w_c2 = T_w_c2;
   S.inv_T_w_r = inverse(T_w_c1);
   S.T_c1_o1 = mul(S.inv_T_w_r, T_wo1);
   S.inv_T_c1_o1 = inverse(S.T_c1_o1);
   S.inv_T_w_o1 = inverse(T_wo1);
   S.T_w_o1 = T_wo1;
-  const M4 T0 = mul(inverse(T_w_c2), T_wo1);
+}
+__device__ void setup_object_post(GNState& S, const M4& T_w_c2) {
+  S.T_w_c2 = T_w_c2;
+  const M4 T0 = mul(inverse(T_w_c2), S.T_w_o1);
   for (int i = 0; i < 16; ++i) {
     S.T[i] = (double)m_at(T0, i / 4, i % 4);
     S.prevT[i] = S.T[i];
@@ -375,6 +373,29 @@ __global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __r
   S.Tf = T0;
   S.invTf = inverse(T0);
   S.evalTf = T0;
+}
+
+__global__ void setup_objects_kernel(GNState* st, IdList slots, const float* __restrict__ Twc2,
+                                     const float* __restrict__ Twc1, const float* __restrict__ Two,
+                                     const int* __restrict__ inst_label) {
+  const int t = threadIdx.x;
+  if (t >= slots.n) return;
+  const int s = slots.v[t];
+  setup_object_pre(st[s], s, load_m4(Twc1), load_m4(Two + 16 * s), inst_label[s]);
+  setup_object_post(st[s], load_m4(Twc2));
+}
+__global__ void setup_objects_pre_kernel(GNState* st, IdList slots, const float* __restrict__ Twc1,
+                                         const float* __restrict__ Two,
+                                         const int* __restrict__ inst_label) {
+  const int t = threadIdx.x;
+  if (t >= slots.n) return;
+  const int s = slots.v[t];
+  setup_object_pre(st[s], s, load_m4(Twc1), load_m4(Two + 16 * s), inst_label[s]);
+}
+__global__ void setup_objects_post_kernel(GNState* st, IdList slots, const float* __restrict__ Twc2) {
+  const int t = threadIdx.x;
+  if (t >= slots.n) return;
+  setup_object_post(st[slots.v[t]], load_m4(Twc2));
 }
 
 __global__ void finalize_camera_kernel(const GNState* st, float* __restrict__ Twc) {
@@ -1673,7 +1694,10 @@ static int gn_host(Context* ctx, int slot) {
 // Tracking::trackLiveFrame with the current model maps; the camera pose is read
 // from and written back to the device.  `moving` (bit per label) selects the
 // pixels excluded from ICP (trackLiveFrame(..., mask)); 0 = no mask.
-int track_camera(Context* ctx, uint32_t moving, int retrack) {
+// The parts of trackLiveFrame before its GN that read neither the live
+// pyramid nor the ICP outlier mask: the problem's setup from the current
+// (pre-tracking) camera pose and the rendered reference of the model maps.
+int track_camera_pre(Context* ctx, int retrack) {
   if (int rc = track_init(ctx)) return rc;
   TrackState& T = *ctx->track;
   const mf_config& c = ctx->cfg;
@@ -1686,16 +1710,28 @@ int track_camera(Context* ctx, uint32_t moving, int retrack) {
   setup_camera_kernel<<<1, 1, 0, ctx->stream>>>(T.d_state, ctx->d_Twc, T.d_Twc_prev,
                                                 F4{c.k[0], c.k[1], c.k[2], c.k[3]}, retrack);
   MF_CUDA(cudaGetLastError());
-  if (moving) {
-    label_mask_kernel<<<div_up((long long)ctx->W * ctx->H, 256), 256, 0, ctx->stream>>>(
-        ctx->d_label, moving, T.d_mask0, ctx->W * ctx->H);
-    if (int rc = track_set_mask(ctx, T.d_mask0)) return rc;
-  }
   IdList cam;
   cam.n = 1;
   cam.v[0] = 0;
-  if (int rc = render_reference(ctx, cam)) return rc;
-  if (c.batched) {
+  return render_reference(ctx, cam);
+}
+
+// The ICP outlier mask of the moving objects' pixels (after the pyramid,
+// whose normals kernel clears the mask planes).
+int track_camera_mask(Context* ctx, uint32_t moving) {
+  if (!moving) return MF_OK;
+  TrackState& T = *ctx->track;
+  label_mask_kernel<<<div_up((long long)ctx->W * ctx->H, 256), 256, 0, ctx->stream>>>(
+      ctx->d_label, moving, T.d_mask0, ctx->W * ctx->H);
+  return track_set_mask(ctx, T.d_mask0);
+}
+
+int track_camera_gn(Context* ctx) {
+  TrackState& T = *ctx->track;
+  IdList cam;
+  cam.n = 1;
+  cam.v[0] = 0;
+  if (ctx->cfg.batched) {
     if (int rc = gn_device(ctx, cam, 0)) return rc;
   } else {
     if (int rc = gn_host(ctx, 0)) return rc;
@@ -1705,9 +1741,42 @@ int track_camera(Context* ctx, uint32_t moving, int retrack) {
   return MF_OK;
 }
 
+int track_camera(Context* ctx, uint32_t moving, int retrack) {
+  if (int rc = track_camera_pre(ctx, retrack)) return rc;
+  if (int rc = track_camera_mask(ctx, moving)) return rc;
+  return track_camera_gn(ctx);
+}
+
 // Tracking::trackEachObject for every id (instance ids >= 1), against the
 // model maps of the last raycast, from the previous camera pose (saved by
 // track_camera) to the current one.
+static int track_objects_run(Context* ctx, const IdList& ids);
+
+// The parts of trackEachObject before its GN that need neither the freshly
+// tracked camera pose nor the live pyramid: the problems' setup from the
+// previous camera pose (saved by track_camera_pre) and the objects' last
+// poses, and their rendered references.
+int track_objects_pre(Context* ctx, const IdList& ids) {
+  if (int rc = track_init(ctx)) return rc;
+  if (ids.n == 0) return MF_OK;
+  TrackState& T = *ctx->track;
+  for (int i = 0; i < ids.n; ++i) T.slot_kind[ids.v[i]] = 1;
+  setup_objects_pre_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, ids, T.d_Twc_prev, ctx->d_Two,
+                                                      ctx->d_inst_label);
+  MF_CUDA(cudaGetLastError());
+  return render_reference(ctx, ids);
+}
+
+// After track_objects_pre: the rest of the setup with the tracked camera pose,
+// then the GN.
+int track_objects_gn(Context* ctx, const IdList& ids) {
+  if (ids.n == 0) return MF_OK;
+  TrackState& T = *ctx->track;
+  setup_objects_post_kernel<<<1, 32, 0, ctx->stream>>>(T.d_state, ids, ctx->d_Twc);
+  MF_CUDA(cudaGetLastError());
+  return track_objects_run(ctx, ids);
+}
+
 int track_objects(Context* ctx, const IdList& ids) {
   if (int rc = track_init(ctx)) return rc;
   if (ids.n == 0) return MF_OK;
@@ -1717,6 +1786,12 @@ int track_objects(Context* ctx, const IdList& ids) {
                                                   ctx->d_Two, ctx->d_inst_label);
   MF_CUDA(cudaGetLastError());
   if (int rc = render_reference(ctx, ids)) return rc;
+  return track_objects_run(ctx, ids);
+}
+
+// The objects' GN once their problems are set up and their references rendered.
+static int track_objects_run(Context* ctx, const IdList& ids) {
+  TrackState& T = *ctx->track;
   if (int rc = tile_depth_range(ctx)) return rc;
   if (ctx->cfg.batched) {
     if (int rc = gn_device(ctx, ids, 1)) return rc;
