@@ -166,7 +166,9 @@ int interp_points(Context* ctx, int id, const float* pos, int n, int field, floa
 int root_children(Context* ctx, int id, uint8_t* mask);
 int track_init(Context* ctx);
 void track_free(Context* ctx);
-int track_preprocess(Context* ctx);
+// clear_mask false: the ICP outlier mask planes are left to track_camera_mask,
+// which writes them whole
+int track_preprocess(Context* ctx, bool clear_mask = true);
 int track_set_ref(Context* ctx);
 int track_camera(Context* ctx, uint32_t moving, int retrack = 0);
 int track_objects(Context* ctx, const IdList& ids);

@@ -45,8 +45,9 @@ void pipeline_free(Context* ctx) {
 // marches, and the composite's fold.  The side stream (lowest priority) runs
 // what does not wait for it: first the tracking setup that needs no live
 // frame and no tracked pose (the camera's and the objects' problems from the
-// previous poses, their rendered references) and the integration masks while
-// the pyramid is built; then, once the camera is tracked, the background's
+// previous poses, their rendered references, the camera's outlier mask of the
+// moving objects' pixels) and the integration masks while the pyramid is
+// built; then, once the camera is tracked, the background's
 // allocation, integration (own visit list, overlap_ctas CTAs or the launch
 // shape's own grid) and raycast marches while the objects are tracked.
 // Nothing one branch reads is written by the other before the event that
@@ -70,13 +71,15 @@ static int frame_overlapped(Context* ctx, bool gen, const IdList& all, const IdL
   ctx->stream = side;
   rc = track_camera_pre(ctx, 0);
   if (!rc) rc = track_objects_pre(ctx, objs);
+  // the moving objects' pixels, written whole into every level of the
+  // camera's outlier mask (the pyramid then leaves the mask planes alone)
+  if (!rc) rc = track_camera_mask(ctx, moving);
   ok(cudaEventRecord(ctx->ev_pre, side));
   if (!rc && gen) rc = launch_generalize(ctx);
   ok(cudaEventRecord(ctx->ev_gen, side));
   ctx->stream = main;
-  // main: the pyramid, the camera's outlier mask, the camera's GN
-  if (!rc) rc = track_preprocess(ctx);
-  if (!rc) rc = track_camera_mask(ctx, moving);
+  // main: the pyramid, then the camera's GN
+  if (!rc) rc = track_preprocess(ctx, /*clear_mask=*/moving == 0);
   ok(cudaStreamWaitEvent(main, ctx->ev_pre, 0));
   if (!rc) rc = track_camera_gn(ctx);
   ok(cudaEventRecord(ctx->ev_fork, main));

@@ -241,14 +241,15 @@ __device__ __forceinline__ void normal_grad_cov_px(const F3* __restrict__ V,
 }
 
 // normal_grad_cov_px on every level; it also clears the level's ICP outlier
-// mask (no pixel is masked until the camera track sets one).
+// mask (no pixel is masked until the camera track sets one) unless MASK is
+// null (the mask is then written whole by the camera's mask kernel).
 __global__ void normal_grad_cov_levels_kernel(LevelMaps m) {
   const int l = blockIdx.y;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= m.w[l] * m.h[l]) return;
   normal_grad_cov_px(m.V[l], m.I[l], m.D[l], m.N[l], m.GX[l], m.GY[l], m.COV[l], m.w[l],
                      m.h[l], m.focal[l], p);
-  m.MASK[l][p] = 0;
+  if (m.MASK[l]) m.MASK[l][p] = 0;
 }
 
 struct SlotPtrs {
@@ -1395,7 +1396,7 @@ static F4 kdiv(const mf_config& c, int l) {
 }
 
 // Tracking::set_params_frame, tracking.cpp:142-171 (buildPyramid :776-818).
-int track_preprocess(Context* ctx) {
+int track_preprocess(Context* ctx, bool clear_mask) {
   if (int rc = track_init(ctx)) return rc;
   TrackState& T = *ctx->track;
   PyrPtrs& P = T.pyr;
@@ -1423,7 +1424,7 @@ int track_preprocess(Context* ctx) {
     m.GX[l] = P.GX[l];
     m.GY[l] = P.GY[l];
     m.COV[l] = P.COV[l];
-    m.MASK[l] = P.MASK[l];
+    m.MASK[l] = clear_mask ? P.MASK[l] : nullptr;
     m.w[l] = P.w[l];
     m.h[l] = P.h[l];
     m.invK[l] = inverse_camera_matrix(kl);
