@@ -133,6 +133,7 @@ int mf_create(const mf_config* cfg, mf_context** out) {
   if (cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_start, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_pre, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_obj, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_gen, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess)
@@ -222,6 +223,7 @@ int mf_destroy(mf_context* ctx) {
   if (ctx->side) cudaStreamDestroy(ctx->side);
   if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
   if (ctx->ev_pre) cudaEventDestroy(ctx->ev_pre);
+  if (ctx->ev_obj) cudaEventDestroy(ctx->ev_obj);
   if (ctx->ev_gen) cudaEventDestroy(ctx->ev_gen);
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);

@@ -124,8 +124,8 @@ struct Context {
   // 0 = in order on the main stream)
   int overlap_ctas = -1;
   cudaStream_t side = nullptr;
-  cudaEvent_t ev_start = nullptr, ev_pre = nullptr, ev_gen = nullptr, ev_fork = nullptr,
-              ev_join = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_pre = nullptr, ev_obj = nullptr, ev_gen = nullptr,
+              ev_fork = nullptr, ev_join = nullptr;
   TrackState* track = nullptr;
   Tune tune;                        // autotuned launch shapes
   // mf_process_frame_motion: frames it has processed, and two planes of

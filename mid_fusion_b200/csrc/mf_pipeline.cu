@@ -69,12 +69,14 @@ static int frame_overlapped(Context* ctx, bool gen, const IdList& all, const IdL
   ok(cudaEventRecord(ctx->ev_start, main));
   ok(cudaStreamWaitEvent(side, ctx->ev_start, 0));
   ctx->stream = side;
+  // the camera's first (it is needed first): its problem, its rendered
+  // reference, and the moving objects' pixels written whole into every level
+  // of its outlier mask (the pyramid then leaves the mask planes alone)
   rc = track_camera_pre(ctx, 0);
-  if (!rc) rc = track_objects_pre(ctx, objs);
-  // the moving objects' pixels, written whole into every level of the
-  // camera's outlier mask (the pyramid then leaves the mask planes alone)
   if (!rc) rc = track_camera_mask(ctx, moving);
   ok(cudaEventRecord(ctx->ev_pre, side));
+  if (!rc) rc = track_objects_pre(ctx, objs);
+  ok(cudaEventRecord(ctx->ev_obj, side));
   if (!rc && gen) rc = launch_generalize(ctx);
   ok(cudaEventRecord(ctx->ev_gen, side));
   ctx->stream = main;
@@ -97,6 +99,7 @@ static int frame_overlapped(Context* ctx, bool gen, const IdList& all, const IdL
   std::swap(ctx->d_visit_count, ctx->d_visit_count_side);
   ctx->stream = main;
   // main: the objects
+  ok(cudaStreamWaitEvent(main, ctx->ev_obj, 0));
   if (!rc) rc = track_objects_gn(ctx, objs);
   ok(cudaStreamWaitEvent(main, ctx->ev_gen, 0));
   if (!rc) rc = stage_prepare(ctx, objs);
