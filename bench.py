@@ -419,6 +419,15 @@ def run_ours(args, rank, world, local_rank):
                          f"arm's first timed frames) after {first} untimed frames, full "
                          f"640x480 frames, OpenMP on every host thread, the reference's "
                          f"Release flags (-g -O1)"}
+        if uneven is not None:  # the 12-object workload's reference, a short sample
+            su = scene_for(rank, n_uneven, "uneven")
+            sec_u, kind_u = CB.time_frames(su, rendered["uneven"], 3, 2, use_reference=True)
+            uneven["cpu_baseline"] = {
+                "value": round(1.0 / sec_u, 4), "unit": "frames/s", "cores": CB.threads(),
+                "kind": kind_u,
+                "sample": "frames 3..4 of the 200-frame sequence after 3 untimed frames, "
+                          "13 instances, OpenMP on every host thread, the reference's "
+                          "Release flags (-g -O1)"}
         # device poses and model maps frame by frame (untimed), then each frame
         # re-tracked on the CPU from the device's previous pose and maps
         ctx_c = make_ctx(True)
