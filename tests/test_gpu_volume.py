@@ -4,7 +4,7 @@ Bit-exact: block and node key sets, corner coordinates, children masks, active
 flags, every voxel field (tsdf, weight, rgb, colour count, foreground
 probability, foreground count) of every block and internal node, and the
 composite raycast maps (vertex, normal, label).  The oracle itself is pinned to
-the reference compiled from its own sources (tests/test_oracle_ref.py).
+the reference compiled from its own sources (tests/test_oracle_reference.py).
 """
 import numpy as np
 import pytest
