@@ -463,6 +463,26 @@ int mf_process_frame(mf_context* ctx, const float* depth, const uint8_t* rgb,
 /* Same with device pointers. */
 int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t* d_rgb,
                             const uint16_t* d_labels);
+/* No counterpart in the reference, which reads each frame on the host before
+ * processing it.  A stream of frames with its uploads overlapped:
+ * mf_frame_stage copies a frame's inputs (as mf_process_frame takes them;
+ * labels may be NULL) from host memory into input slot `slot` (0 or 1) on
+ * the context's upload stream and returns without waiting; mf_process_staged
+ * then processes the frame in that slot exactly as mf_process_frame would.
+ * Staging frame f + 1 into the other slot before mf_get_poses of frame f lets
+ * its copy run while frame f is processed.  An upload into a slot waits, on
+ * the device, until the frame processed from it has copied it out.  The host
+ * buffers must be pinned for the copy to overlap, and must stay unchanged
+ * until the frame has been processed (mf_get_poses after mf_process_staged).
+ * MF_E_STATE: staging into a slot whose frame has not been processed, or
+ * processing an empty slot.  The slots (2 x W*H*9 bytes) and the stream are
+ * created by the first call. */
+int mf_frame_stage(mf_context* ctx, int slot, const float* depth, const uint8_t* rgb,
+                   const uint16_t* labels);
+int mf_process_staged(mf_context* ctx, int slot);
+/* The upload stream of mf_frame_stage (created on first use), as a
+ * cudaStream_t, for callers that order their own work with it. */
+int mf_upload_stream(mf_context* ctx, void** stream);
 /* Kfusion::tracking with motion segmentation (apps/kfusion/src/cpp/
  * kfusion.cpp:265-466) and the integration that follows (:606-630), for one
  * frame from host buffers (labels required).  Host-driven (it synchronises

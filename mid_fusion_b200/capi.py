@@ -45,7 +45,8 @@ EXPORTS = [
     "mf_mesh", "mf_write_vtk_mesh", "mf_dump_mesh", "mf_tune_candidates", "mf_tune_describe",
     "mf_autotune", "mf_tune_get", "mf_tune_set", "mf_process_frame_motion",
     "mf_set_gn_persistent", "mf_object_residuals", "mf_mesh_set_triangle_table",
-    "mf_raycast_records", "mf_raycast_fold",
+    "mf_raycast_records", "mf_raycast_fold", "mf_frame_stage", "mf_process_staged",
+    "mf_upload_stream",
 ]
 
 TUNE_RAYCAST, TUNE_INTEGRATE, TUNE_MAX_VARIANTS = 0, 1, 16
@@ -292,6 +293,22 @@ class Context:
         s = C.c_void_p()
         self._check(self.lib.mf_get_stream(self.h, C.byref(s)))
         return s.value
+
+    def upload_stream(self):
+        s = C.c_void_p()
+        self._check(self.lib.mf_upload_stream(self.h, C.byref(s)))
+        return s.value
+
+    def frame_stage(self, slot, depth, rgb, labels=None):
+        """Upload a frame into input slot 0 or 1 (mf_frame_stage).  The arrays
+        are borrowed: keep them alive and unchanged until the frame has been
+        processed and mf_get_poses has returned."""
+        lab = None if labels is None else labels.ctypes.data_as(C.c_void_p)
+        self._check(self.lib.mf_frame_stage(self.h, int(slot), depth.ctypes.data_as(C.c_void_p),
+                                            rgb.ctypes.data_as(C.c_void_p), lab))
+
+    def process_staged(self, slot):
+        self._check(self.lib.mf_process_staged(self.h, int(slot)))
 
     # ---------------------------------------------------------------- tracking
     def preprocess(self):

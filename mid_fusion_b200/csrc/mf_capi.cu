@@ -207,6 +207,17 @@ int mf_create(const mf_config* cfg, mf_context** out) {
 int mf_destroy(mf_context* ctx) {
   if (!ctx) return MF_E_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->upload) {
+    cudaStreamSynchronize(ctx->upload);
+    for (int s = 0; s < 2; ++s) {
+      if (ctx->stg_depth[s]) cudaFree(ctx->stg_depth[s]);
+      if (ctx->stg_rgb8[s]) cudaFree(ctx->stg_rgb8[s]);
+      if (ctx->stg_labels[s]) cudaFree(ctx->stg_labels[s]);
+      if (ctx->ev_staged[s]) cudaEventDestroy(ctx->ev_staged[s]);
+      if (ctx->ev_consumed[s]) cudaEventDestroy(ctx->ev_consumed[s]);
+    }
+    cudaStreamDestroy(ctx->upload);
+  }
   pipeline_free(ctx);
   track_free(ctx);
   for (auto& in : ctx->inst) volume_free(in);
@@ -526,6 +537,77 @@ int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t
     MF_CUDA(cudaMemcpyAsync(ctx->d_labels, d_labels, 2 * WH, cudaMemcpyDeviceToDevice,
                             ctx->stream));
   return process_frame(ctx, d_labels != nullptr);
+}
+
+// The upload stream, the two input slots and their events, on first use.
+static int staging_init(Context* ctx) {
+  if (ctx->upload) return MF_OK;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  cudaStream_t st = nullptr;
+  MF_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  ctx->upload = st;  // mf_destroy frees whatever of the rest was made
+  for (int s = 0; s < 2; ++s) {
+    MF_CUDA(cudaMalloc(&ctx->stg_depth[s], 4 * WH));
+    MF_CUDA(cudaMalloc(&ctx->stg_rgb8[s], 3 * WH));
+    MF_CUDA(cudaMalloc(&ctx->stg_labels[s], 2 * WH));
+    MF_CUDA(cudaEventCreateWithFlags(&ctx->ev_staged[s], cudaEventDisableTiming));
+    MF_CUDA(cudaEventCreateWithFlags(&ctx->ev_consumed[s], cudaEventDisableTiming));
+  }
+  return MF_OK;
+}
+
+int mf_frame_stage(mf_context* ctx, int slot, const float* depth, const uint8_t* rgb,
+                   const uint16_t* labels) {
+  if (check(ctx) || slot < 0 || slot > 1 || !depth || !rgb) return MF_E_ARG;
+  if (ctx->stg_pending[slot]) {
+    ctx->last_error = "mf_frame_stage: slot " + std::to_string(slot) +
+                      " holds a frame that mf_process_staged has not taken yet";
+    return MF_E_STATE;
+  }
+  if (int rc = staging_init(ctx)) return rc;
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  // the frame last processed from this slot has copied it out (an event never
+  // recorded is complete)
+  MF_CUDA(cudaStreamWaitEvent(ctx->upload, ctx->ev_consumed[slot], 0));
+  MF_CUDA(cudaMemcpyAsync(ctx->stg_depth[slot], depth, 4 * WH, cudaMemcpyHostToDevice,
+                          ctx->upload));
+  MF_CUDA(cudaMemcpyAsync(ctx->stg_rgb8[slot], rgb, 3 * WH, cudaMemcpyHostToDevice, ctx->upload));
+  if (labels)
+    MF_CUDA(cudaMemcpyAsync(ctx->stg_labels[slot], labels, 2 * WH, cudaMemcpyHostToDevice,
+                            ctx->upload));
+  MF_CUDA(cudaEventRecord(ctx->ev_staged[slot], ctx->upload));
+  ctx->stg_labels_set[slot] = labels != nullptr;
+  ctx->stg_pending[slot] = true;
+  return MF_OK;
+}
+
+int mf_process_staged(mf_context* ctx, int slot) {
+  if (check(ctx) || slot < 0 || slot > 1) return MF_E_ARG;
+  if (!ctx->stg_pending[slot]) {
+    ctx->last_error = "mf_process_staged: nothing staged in slot " + std::to_string(slot);
+    return MF_E_STATE;
+  }
+  const size_t WH = (size_t)ctx->W * ctx->H;
+  MF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->ev_staged[slot], 0));
+  MF_CUDA(cudaMemcpyAsync(ctx->d_depth, ctx->stg_depth[slot], 4 * WH, cudaMemcpyDeviceToDevice,
+                          ctx->stream));
+  rgb_convert_kernel<<<(unsigned)((WH + 255) / 256), 256, 0, ctx->stream>>>(
+      ctx->stg_rgb8[slot], ctx->d_rgb, ctx->d_grey, (int)WH);
+  MF_CUDA(cudaGetLastError());
+  const bool labels = ctx->stg_labels_set[slot];
+  if (labels)
+    MF_CUDA(cudaMemcpyAsync(ctx->d_labels, ctx->stg_labels[slot], 2 * WH,
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+  MF_CUDA(cudaEventRecord(ctx->ev_consumed[slot], ctx->stream));
+  ctx->stg_pending[slot] = false;
+  return process_frame(ctx, labels);
+}
+
+int mf_upload_stream(mf_context* ctx, void** stream) {
+  if (check(ctx) || !stream) return MF_E_ARG;
+  if (int rc = staging_init(ctx)) return rc;
+  *stream = (void*)ctx->upload;
+  return MF_OK;
 }
 
 int mf_get_poses(mf_context* ctx, float* T_w_c, float* T_w_o) {

@@ -132,6 +132,17 @@ struct Context {
   // result rows (2 x W*H int8 each) for the mask refinement
   int motion_frames = 0;
   int8_t* d_motion_rows = nullptr;
+  // mf_frame_stage / mf_process_staged: two device slots of frame inputs,
+  // uploaded on their own stream (all created with the first staged frame);
+  // ev_staged[s]: slot s's upload is done; ev_consumed[s]: the frame processed
+  // from slot s has copied it out (the next upload into s may start)
+  cudaStream_t upload = nullptr;
+  float* stg_depth[2] = {};
+  uint8_t* stg_rgb8[2] = {};
+  uint16_t* stg_labels[2] = {};
+  bool stg_labels_set[2] = {};
+  bool stg_pending[2] = {};
+  cudaEvent_t ev_staged[2] = {}, ev_consumed[2] = {};
   uint8_t* d_render = nullptr;      // W*H*4 render scratch for host destinations
   void* d_render_small = nullptr;   // colour / pointer tables of a render
   size_t render_small_bytes = 0;
