@@ -178,6 +178,10 @@ void ref_raycast_objects(void** vols, const float* Two, const int* labels, int n
   float3* normal = (float3*)normal_out;
   const float4 k = make_float4(k4[0], k4[1], k4[2], k4[3]);
   const Matrix4 view = load_m4(Twc) * getInverseCameraMatrix(k);
+  // the reference's pixel loop is an OpenMP loop over rows (rendering.cpp:18);
+  // every pixel writes only its own outputs.  The serial parity build ignores
+  // the pragma.
+#pragma omp parallel for
   for (int y = 0; y < H; y++)
     for (int x = 0; x < W; x++) {
       float nearest_hit_t = 1.0e3;
