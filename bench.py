@@ -466,7 +466,7 @@ def run_ours(args, rank, world, local_rank):
         first = 1 + args.warmup                 # the GPU arm's first timed frame
         n_cpu = min(CPU_SAMPLE_FRAMES, n_frames - first)
         sec, kind = CB.time_frames(s, frames, first, n_cpu, use_reference=True)
-        cpu = {"value": round(1.0 / sec, 4), "unit": "frames/s", "cores": CB.threads(),
+        cpu = {"value": round(1.0 / sec, 4), "unit": "frames/s", "cores": CB.threads(), "cpu": CB.cpu_model(),
                "kind": kind,
                "sample": f"frames {first}..{first + n_cpu - 1} of the same sequence (the GPU "
                          f"arm's first timed frames) after {first} untimed frames, full "
@@ -476,7 +476,7 @@ def run_ours(args, rank, world, local_rank):
             su = scene_for(rank, n_uneven, "uneven")
             sec_u, kind_u = CB.time_frames(su, rendered["uneven"], 3, 2, use_reference=True)
             uneven["cpu_baseline"] = {
-                "value": round(1.0 / sec_u, 4), "unit": "frames/s", "cores": CB.threads(),
+                "value": round(1.0 / sec_u, 4), "unit": "frames/s", "cores": CB.threads(), "cpu": CB.cpu_model(),
                 "kind": kind_u,
                 "sample": "frames 3..4 of the 200-frame sequence after 3 untimed frames, "
                           "13 instances, OpenMP on every host thread, the reference's "
@@ -650,7 +650,7 @@ def run_reference(args):
         "ms_per_step": round(1e3 * total / n, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "frame": [W, H], "instances": 4},
-        "cpu_baseline": {"value": round(value, 4), "unit": "frames/s", "cores": CB.threads(),
+        "cpu_baseline": {"value": round(value, 4), "unit": "frames/s", "cores": CB.threads(), "cpu": CB.cpu_model(),
                          "kind": kind,
                          "sample": f"{n} frames after {1 + args.warmup} untimed, full "
                                    "640x480 frames, OpenMP on every host thread, the "

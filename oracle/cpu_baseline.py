@@ -114,6 +114,19 @@ def threads():
     return int(n) if n else (os.cpu_count() or 1)
 
 
+def cpu_model():
+    """The host CPU's model name (the first `model name` of /proc/cpuinfo), or
+    None where it cannot be read."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def time_frames(scene, frames, n_first, n_timed, use_reference=True, build="stock"):
     """Runs frames [0, n_first + n_timed); times the last n_timed.  Returns
     (seconds per frame, kind)."""
