@@ -1,5 +1,6 @@
 """TEST INFRASTRUCTURE ONLY: precision study of the mixed-precision pipeline
-(a study script run on a GPU host, not a test).
+over a long sequence (300 frames of the 640x480 three-object workload against
+an all-FP64 oracle run; a study script run on a GPU host, not a test).
 
 The bench's scene (640x480, background 512^3 @ 1 cm + 3 objects 256^3 @ 2 mm,
 each with its own twist) for many frames through the device pipeline
