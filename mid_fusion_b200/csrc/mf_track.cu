@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 #include "mf_internal.h"
+#include "mf_robust.cuh"
 #include "mf_solve.cuh"
 
 namespace mf {
@@ -853,40 +854,6 @@ __device__ void rgb_row(const GNArgs& a, const GNState& S, const F3* rV, int L, 
   r.J[3] = ic * Jr.x; r.J[4] = ic * Jr.y; r.J[5] = ic * Jr.z;
   r.e = ic * residual;
   r.result = 1;
-}
-
-// calc_robust_weight / calc_robust_residual, tracking.cpp:1474-1532: evaluated
-// in double, used as float.
-__device__ __forceinline__ void robust(float e, int kind, float& w, float& loss) {
-  const double r = e;
-  double wd = 1.0, l;
-  switch (kind) {
-    case 1: {
-      const double a = fabs(r);
-      if (a <= 1.345) { wd = 1.0; l = 0.5 * r * r; }
-      else { wd = 1.345 / a; l = 1.345 * (a - 0.5 * 1.345); }
-      break;
-    }
-    case 2: {
-      const double b = 4.6851, a = fabs(r);
-      if (a <= b) {
-        const double u = 1.0 - r * r / (b * b);
-        wd = u * u;
-        const double v = 1.0 - (r / b) * (r / b);
-        l = b * b / 6.0 * (1.0 - v * v * v);
-      } else { wd = 0; l = b * b / 6.0; }
-      break;
-    }
-    case 3: {
-      const double q = (r / 2.3849) * (r / 2.3849);
-      wd = 1 / (1 + q);
-      l = 0.5 * 2.3849 * 2.3849 * log(1.0 + q);
-      break;
-    }
-    default: l = 0.5 * r * r;
-  }
-  w = (float)wd;
-  loss = (float)l;
 }
 
 // Index of J_i J_j (i <= j) among the 21 upper-triangle terms, row-major

@@ -78,13 +78,35 @@ void se3_exp(const double xi[6], double T[4][4]) {
 }
 
 // ----------------------------------------------------------------- helpers
+// The reference squares through math_utils.h:92 `float sq(float)`: its Tukey
+// and Cauchy terms round r / b (a double) and 1 - r^2 / b^2 to float and
+// square them in float.  The FP32 oracle (T = float) keeps those roundings;
+// the FP64 oracle squares in double.
+template <typename T> static double sq_ref(double x) {
+  if (sizeof(T) == sizeof(float)) { const float f = (float)x; return (double)(f * f); }
+  return x * x;
+}
 template <typename T> static T robust_weight(T e, int kind) {  // tracking.cpp:1504-1532
   double w = 1.0;
   const double r = e;
   switch (kind) {
     case 1: w = std::fabs(r) <= 1.345 ? 1.0 : 1.345 / std::fabs(r); break;
-    case 2: w = std::fabs(r) <= 4.6851 ? (1.0 - r * r / (4.6851 * 4.6851)) * (1.0 - r * r / (4.6851 * 4.6851)) : 0.0; break;
-    case 3: w = 1 / (1 + (r / 2.3849) * (r / 2.3849)); break;
+    case 2:
+      if (std::fabs(r) <= 4.6851) {
+        // sq(1.0 - sq(residual) / sq(tukey_b)): float quotient of float squares
+        const double q = sizeof(T) == sizeof(float)
+                             ? (double)((float)sq_ref<T>(r) / (float)sq_ref<T>(4.6851))
+                             : r * r / (4.6851 * 4.6851);
+        w = sq_ref<T>(1.0 - q);
+      } else {
+        w = 0.0;
+      }
+      break;
+    case 3:
+      // 1 / (1 + sq(residual / cauchy_k)): int + float and the quotient in float
+      w = sizeof(T) == sizeof(float) ? (double)(1.f / (1.f + (float)sq_ref<T>(r / 2.3849)))
+                                     : 1 / (1 + sq_ref<T>(r / 2.3849));
+      break;
     default: break;
   }
   return (T)w;
@@ -96,10 +118,10 @@ template <typename T> static T robust_loss(T e, int kind) {  // tracking.cpp:147
     case 1: l = std::fabs(r) <= 1.345 ? 0.5 * r * r : 1.345 * (std::fabs(r) - 0.5 * 1.345); break;
     case 2: {
       const double b = 4.6851;
-      l = std::fabs(r) <= b ? b * b / 6.0 * (1.0 - std::pow(1.0 - (r / b) * (r / b), 3)) : b * b / 6.0;
+      l = std::fabs(r) <= b ? b * b / 6.0 * (1.0 - std::pow(1.0 - sq_ref<T>(r / b), 3)) : b * b / 6.0;
       break;
     }
-    case 3: l = 0.5 * 2.3849 * 2.3849 * std::log(1.0 + (r / 2.3849) * (r / 2.3849)); break;
+    case 3: l = 0.5 * 2.3849 * 2.3849 * std::log(1.0 + sq_ref<T>(r / 2.3849)); break;
     default: l = 0.5 * r * r;
   }
   return (T)l;

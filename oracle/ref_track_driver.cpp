@@ -114,6 +114,17 @@ void* rt_create(int W, int H, int levels, const int* iters, int robust, int use_
 }
 void rt_destroy(void* h) { delete (Tracking*)h; }
 
+// Tracking::calc_robust_weight / calc_robust_residual (tracking.cpp:1474-1532)
+// of n residuals; robust in RobustW order.
+void rt_robust(void* h, int robust, const float* e, int n, float* w, float* loss) {
+  Tracking* t = (Tracking*)h;
+  const RobustW k = static_cast<RobustW>(robust);
+  for (int i = 0; i < n; ++i) {
+    w[i] = t->calc_robust_weight(e[i], k);
+    loss[i] = t->calc_robust_residual(e[i], k);
+  }
+}
+
 // preprocessing.cpp:73-102: grey intensity and float RGB of an 8-bit frame (ratio 1).
 void rt_rgb2intensity(const unsigned char* rgb, int W, int H, float* grey, float* rgb3) {
   rgb2intensity(grey, (float3*)rgb3, make_uint2(W, H), (const uchar3*)rgb, make_uint2(W, H));

@@ -426,6 +426,7 @@ def reference_tracking(path=REF_TRACK_SO):
         fn("rt_set_ref_from_current", None, P)
         fn("rt_track_live", C.c_int, P, FP, FP, FP, FP, FP, V)
         fn("rt_reduction", None, P, C.c_int, FP)
+        fn("rt_robust", None, P, C.c_int, FP, C.c_int, FP, FP)
         fn("rt_get_level", C.c_int, P, C.c_int, C.c_int, FP)
         fn("rt_track_data", None, P, C.c_int, I32, FP, FP)
         fn("rt_compute_residuals", None, P, FP, FP, FP, FP, FP, C.c_int, C.c_int, C.c_float)
@@ -518,6 +519,15 @@ class RefTracker:
         out = np.zeros(32, np.float32)
         self.lib.rt_reduction(self.h, level, out)
         return out
+
+    def robust(self, kind, e):
+        """calc_robust_weight / calc_robust_residual of float32 residuals e:
+        (weights, losses)."""
+        e = np.ascontiguousarray(e, np.float32)
+        w = np.zeros_like(e)
+        loss = np.zeros_like(e)
+        self.lib.rt_robust(self.h, int(kind), e, e.size, w, loss)
+        return w, loss
 
     def level(self, l, which):
         w, h = self.W >> l, self.H >> l

@@ -260,3 +260,88 @@ def test_bench_pose_check_is_zero_on_the_reference_itself():
     # "device" (here the reference) against FP64 are the same numbers
     assert chk["device_vs_fp64_oracle"] == chk["reference_vs_fp64_oracle"]
     assert 0.0 < chk["reference_vs_fp64_oracle"]["camera_m"] < 1e-3
+
+
+def _product_robust(tmp_path_factory):
+    """The device's robust() (mid_fusion_b200/csrc/mf_robust.cuh) compiled for
+    the host, as the GN kernels compile it for the device: plain IEEE float and
+    double operations, no contraction into fused multiply-adds."""
+    import ctypes as C
+    import os
+    import subprocess
+    d = tmp_path_factory.mktemp("robust")
+    src = d / "robust_host.cpp"
+    src.write_text('#include "mf_robust.cuh"\n'
+                   'extern "C" void robust_host(int kind, const float* e, int n, float* w, '
+                   'float* l) { for (int i = 0; i < n; ++i) mf::robust(e[i], kind, w[i], l[i]); }\n')
+    csrc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                        "mid_fusion_b200", "csrc")
+    so = d / "librobust_host.so"
+    subprocess.run(["g++", "-O2", "-std=c++14", "-ffp-contract=off", "-fPIC", "-shared",
+                    "-I", csrc, "-o", str(so), str(src)], check=True)
+    lib = C.CDLL(str(so))
+    FP = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    lib.robust_host.argtypes = [C.c_int, FP, C.c_int, FP, FP]
+    lib.robust_host.restype = None
+
+    def run(kind, e):
+        w = np.zeros_like(e)
+        loss = np.zeros_like(e)
+        lib.robust_host(kind, e, e.size, w, loss)
+        return w, loss
+    return run
+
+
+def test_robust_weights_match_reference(tmp_path_factory):
+    """Tracking::calc_robust_weight / calc_robust_residual (tracking.cpp:
+    1474-1532) against the device's robust() on residuals across each
+    kernel's range (thresholds, signs, zeros, tiny and large values): none and
+    Huber (the parity mode) bit for bit; Tukey and Cauchy, which the device
+    squares in double where the reference squares in float, within one float
+    ulp of 1 for the weight and 4 ulps for the loss."""
+    rng = np.random.default_rng(3)
+    e = np.concatenate([
+        rng.normal(scale=0.5, size=50000), rng.normal(scale=3.0, size=50000),
+        rng.normal(scale=20.0, size=20000), rng.uniform(-6, 6, size=50000),
+        np.array([0.0, -0.0, 1e-30, -1e-30, 1e-8, 1.345, -1.345, 4.6851, -4.6851, 2.3849,
+                  -2.3849, 1e6, -1e6]),
+        np.nextafter(np.float32(1.345), np.float32(0)).reshape(1),
+        np.nextafter(np.float32(4.6851), np.float32(10)).reshape(1)]).astype(np.float32)
+    R = O.RefTracker(32, 24, np.array([20, 20, 16, 12], np.float32))
+    dev = _product_robust(tmp_path_factory)
+    for kind in range(4):
+        wr, lr = R.robust(kind, e)
+        wd, ld = dev(kind, e)
+        if kind < 2:
+            assert np.array_equal(wr, wd), (kind, np.flatnonzero(wr != wd)[:5])
+            assert np.array_equal(lr, ld), (kind, np.flatnonzero(lr != ld)[:5])
+        else:
+            assert np.abs(wd - wr).max() <= np.float32(2.0 ** -23), kind
+            ulps = np.abs(ld.view(np.int32).astype(np.int64) - lr.view(np.int32).astype(np.int64))
+            assert ulps.max() <= 4, kind
+
+
+@pytest.mark.parametrize("robust", [0, 1, 2, 3])
+@pytest.mark.parametrize("use_icp,use_rgb", [(1, 1), (1, 0), (0, 1)])
+def test_camera_tracking_every_robust_kernel_matches_reference(robust, use_icp, use_rgb):
+    """trackLiveFrame with each robust kernel (none, Huber, Tukey, Cauchy: the
+    reference's default) and with ICP rows only, photometric rows only, or
+    both (Tracking(using_ICP, using_RGB)): the FP32 oracle's pose and every
+    level's sums equal the reference's."""
+    W, H = 320, 240
+    s = make_scene("room", W, H, n_frames=2, seed=5, bg_size=256, bg_dim=2.56)
+    _, _, T0, _, vm, nm, _ = _model(s, W, H)
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    R = O.RefTracker(W, H, s.k, robust=robust, use_icp=bool(use_icp), use_rgb=bool(use_rgb))
+    F = O.Tracker(W, H, s.k, robust=robust, fp64=False, use_icp=bool(use_icp),
+                  use_rgb=bool(use_rgb))
+    for t in (R, F):
+        t.set_frame(rgb0, d0)
+        t.set_ref()
+        t.set_frame(rgb1, d1)
+    Tr = R.track_camera(T0, T0, vm, nm)
+    Tf = F.track_camera(T0, T0, vm, nm).astype(np.float32)
+    assert np.array_equal(Tr, Tf)
+    for level in range(3):
+        assert np.array_equal(R.reduction(level), _sums(F, level)), level
