@@ -345,3 +345,27 @@ def test_camera_tracking_every_robust_kernel_matches_reference(robust, use_icp, 
     assert np.array_equal(Tr, Tf)
     for level in range(3):
         assert np.array_equal(R.reduction(level), _sums(F, level)), level
+
+
+@pytest.mark.parametrize("iters", [(10,), (10, 5), (2, 2, 2), (4, 3, 1)])
+def test_camera_tracking_pyramid_depths_match_reference(iters):
+    """trackLiveFrame with one, two and three pyramid levels and other
+    iteration counts: the FP32 oracle's pose and sums equal the reference's.
+    (Four levels have no reference behaviour to match: its per-level
+    photometric thresholds hold three entries, tracking.h:347-351, and a
+    fourth level reads past them.)"""
+    W, H = 320, 240
+    s = make_scene("room", W, H, n_frames=2, seed=5, bg_size=256, bg_dim=2.56)
+    _, _, T0, _, vm, nm, _ = _model(s, W, H)
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    R = O.RefTracker(W, H, s.k, iters=iters)
+    F = O.Tracker(W, H, s.k, iters=iters, robust=1, fp64=False)
+    for t in (R, F):
+        t.set_frame(rgb0, d0)
+        t.set_ref()
+        t.set_frame(rgb1, d1)
+    assert np.array_equal(R.track_camera(T0, T0, vm, nm),
+                          F.track_camera(T0, T0, vm, nm).astype(np.float32))
+    for level in range(len(iters)):
+        assert np.array_equal(R.reduction(level), _sums(F, level)), level
