@@ -369,3 +369,32 @@ def test_camera_tracking_pyramid_depths_match_reference(iters):
                           F.track_camera(T0, T0, vm, nm).astype(np.float32))
     for level in range(len(iters)):
         assert np.array_equal(R.reduction(level), _sums(F, level)), level
+
+
+@pytest.mark.parametrize("robust", [0, 2, 3])
+@pytest.mark.parametrize("use_icp,use_rgb", [(1, 1), (1, 0), (0, 1)])
+def test_object_tracking_every_robust_kernel_matches_reference(robust, use_icp, use_rgb):
+    """trackEachObject (tracking.cpp:580-708) with the other robust kernels
+    (Huber: test_object_tracking_matches_reference) and each row set: every
+    object's pose and sums equal the reference's."""
+    W, H = 320, 240
+    s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=256, obj_size=128, n_objects=3)
+    _, labels, T0, P0, vm, nm, lm = _model(s, W, H)
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    R = O.RefTracker(W, H, s.k, robust=robust, use_icp=bool(use_icp), use_rgb=bool(use_rgb))
+    F = O.Tracker(W, H, s.k, robust=robust, fp64=False, use_icp=bool(use_icp),
+                  use_rgb=bool(use_rgb))
+    for t in (R, F):
+        t.set_frame(rgb0, d0)
+        t.set_ref()
+        t.set_frame(rgb1, d1)
+    Tc = R.track_camera(T0, T0, vm, nm)
+    assert np.array_equal(Tc, F.track_camera(T0, T0, vm, nm).astype(np.float32))
+    for i, label in enumerate(labels[1:], 1):
+        mv, mn = _object_maps(vm, nm, lm, label)
+        To_r, _ = R.track_object(R.object(P0[i], mv, mn), Tc, T0)
+        To_f = F.track_object(P0[i], Tc, T0, vm, nm, lm, label).astype(np.float32)
+        assert np.array_equal(To_r, To_f), label
+        for level in range(3):
+            assert np.array_equal(R.reduction(level), _sums(F, level)), (label, level)
