@@ -96,3 +96,38 @@ def test_interp_and_grad_match_reference():
         for field in range(5):  # tsdf, fg, r, g, b
             assert a.interp(p, field) == b.interp(p, field), field
         assert np.array_equal(a.grad(p), b.grad(p))
+
+
+@pytest.mark.parametrize("mu", [0.02, 0.05, 0.2])
+def test_oracle_matches_reference_other_truncation(mu):
+    """Integration (every block and node field) and the composite raycast with
+    truncation distances other than the default 0.1: oracle == reference."""
+    W, H = 128, 96
+    s = make_scene("multi", W, H, n_frames=3, seed=3, bg_size=128, obj_size=64, n_objects=2)
+    orc = O.oracle()
+    labels = [i.label for i in s.instances]
+    vo = [orc.volume(i.size, i.dim) for i in s.instances]
+    vr = [ref.volume(i.size, i.dim) for i in s.instances]
+    for f in range(3):
+        d, rgb, lab = s.render(f)
+        masks = generalize_masks(lab, labels)
+        poses = s.volume_poses(f)
+        T = s.cam_poses[f].astype(np.float32)
+        rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+        for i in range(len(labels)):
+            assert (vo[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, mu) ==
+                    vr[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, mu))
+            ko, _, ao, xo = vo[i].blocks()
+            kr, _, ar, xr = vr[i].blocks()
+            assert np.array_equal(ko, kr) and np.array_equal(ao, ar)
+            assert xo.tobytes() == xr.tobytes()
+            assert vo[i].nodes()[3].tobytes() == vr[i].nodes()[3].tobytes()
+        bo = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+        br = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+        orc.raycast_objects(vo, poses, labels, T, s.k, W, H, eps_size=EPS_SIZE, mu=mu,
+                            vertex=bo[0], normal=bo[1], label_img=bo[2])
+        ref.raycast_objects(vr, poses, labels, T, s.k, W, H, mu=mu, vertex=br[0], normal=br[1],
+                            label_img=br[2])
+        oob = orc.raycast_oob_mask(vo, poses, T, s.k, W, H, eps_size=EPS_SIZE)
+        bad = np.any(bo[0] != br[0], axis=-1) | np.any(bo[1] != br[1], axis=-1) | (bo[2] != br[2])
+        assert not np.any(bad & ~oob), np.argwhere(bad & ~oob)[:10]
