@@ -93,7 +93,7 @@ def test_pyramid_matches_reference():
             assert np.array_equal(a, b), (level, which)
 
 
-@pytest.mark.parametrize("W,H,seed", [(320, 240, 5), (320, 240, 9), (160, 120, 2)])
+@pytest.mark.parametrize("W,H,seed", [(320, 240, 5), (320, 240, 9), (160, 120, 2), (640, 480, 4)])
 def test_camera_tracking_matches_reference(W, H, seed):
     s = make_scene("room", W, H, n_frames=2, seed=seed, bg_size=256, bg_dim=2.56)
     _, _, T0, _, vm, nm, _ = _model(s, W, H)
@@ -130,13 +130,17 @@ def test_masked_camera_tracking_matches_reference():
         assert np.array_equal(R.reduction(level), _sums(F, level)), level
 
 
-@pytest.mark.parametrize("preset", ["multi", "uneven"])
+@pytest.mark.parametrize("preset", ["multi", "uneven", "headline"])
 def test_object_tracking_matches_reference(preset):
     W, H = 320, 240
     if preset == "multi":
         s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=256, obj_size=128, n_objects=3)
-    else:  # 12 objects, octrees 32^3 .. 256^3 at 2-5 mm
+    elif preset == "uneven":  # 12 objects, octrees 32^3 .. 256^3 at 2-5 mm
         s = make_scene("uneven", W, H, n_frames=2, seed=23, n_objects=12)
+    else:  # the bench workload: 640x480, background 512^3 @ 1 cm + 3 objects 256^3 @ 2 mm
+        W, H = 640, 480
+        s = make_scene("multi", W, H, n_frames=2, seed=11, n_objects=3, bg_size=512,
+                       bg_dim=5.12, obj_size=256, obj_dim=0.512)
     _, labels, T0, P0, vm, nm, lm = _model(s, W, H)
     R, F = _pair(s, W, H)
     Tc = R.track_camera(T0, T0, vm, nm)
