@@ -402,3 +402,34 @@ def test_object_tracking_every_robust_kernel_matches_reference(robust, use_icp, 
         assert np.array_equal(To_r, To_f), label
         for level in range(3):
             assert np.array_equal(R.reduction(level), _sums(F, level)), (label, level)
+
+
+@pytest.mark.parametrize("threshold", [0.5, 3.0])
+@pytest.mark.parametrize("use_icp,use_rgb", [(1, 1), (1, 0), (0, 1)])
+def test_motion_residuals_other_thresholds_and_rows_match_reference(threshold, use_icp, use_rgb):
+    """compute_residuals (tracking.cpp:1535-1747) with other residual
+    thresholds than the reference's 1.5 and with each row set: every row code
+    and every valid row's error equal the reference's."""
+    W, H = 320, 240
+    s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=256, obj_size=128, n_objects=3)
+    vols, labels, T0, P0, vm, nm, _ = _model(s, W, H)
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    R = O.RefTracker(W, H, s.k, use_icp=bool(use_icp), use_rgb=bool(use_rgb))
+    F = O.Tracker(W, H, s.k, robust=1, fp64=False, use_icp=bool(use_icp), use_rgb=bool(use_rgb))
+    for t in (R, F):
+        t.set_frame(rgb0, d0)
+        t.set_ref()
+        t.set_frame(rgb1, d1)
+    Tc = R.track_camera(T0, T0, vm, nm)
+    assert np.array_equal(Tc, F.track_camera(T0, T0, vm, nm).astype(np.float32))
+    lv = np.zeros((H, W, 3), np.float32)
+    O.oracle().raycast_objects(vols, P0, labels, Tc, s.k, W, H, eps_size=s.instances[0].size,
+                               vertex=lv, normal=np.zeros((H, W, 3), np.float32),
+                               label_img=np.zeros((H, W), np.int32))
+    res_r, err_r, _ = R.compute_residuals(Tc, T0, vm, nm, lv, use_icp=bool(use_icp),
+                                          use_rgb=bool(use_rgb), threshold=threshold)
+    res_f, err_f = F.motion_residuals(Tc, T0, vm, nm, lv, threshold=threshold)
+    assert np.array_equal(res_r.astype(np.int8), res_f)
+    ok = res_r == 1
+    assert ok.sum() > 1000 and np.array_equal(err_r[ok], err_f[ok])
