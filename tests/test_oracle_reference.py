@@ -131,3 +131,33 @@ def test_oracle_matches_reference_other_truncation(mu):
         oob = orc.raycast_oob_mask(vo, poses, T, s.k, W, H, eps_size=EPS_SIZE)
         bad = np.any(bo[0] != br[0], axis=-1) | np.any(bo[1] != br[1], axis=-1) | (bo[2] != br[2])
         assert not np.any(bad & ~oob), np.argwhere(bad & ~oob)[:10]
+
+
+@pytest.mark.parametrize("near,far", [(0.4, 4.0), (0.1, 1.2), (0.5, 1.5), (1.0, 8.0)])
+def test_raycast_other_near_far_match_reference(near, far):
+    """The composite raycast with near / far planes other than 0.1 / 4.0 (the
+    ray iterator's range and the march's bound): oracle == reference."""
+    W, H = 128, 96
+    s = make_scene("multi", W, H, n_frames=1, seed=8, bg_size=128, obj_size=64, n_objects=2)
+    orc = O.oracle()
+    labels = [i.label for i in s.instances]
+    vo = [orc.volume(i.size, i.dim) for i in s.instances]
+    vr = [ref.volume(i.size, i.dim) for i in s.instances]
+    d, rgb, lab = s.render(0)
+    masks = generalize_masks(lab, labels)
+    poses = s.volume_poses(0)
+    T = s.cam_poses[0].astype(np.float32)
+    rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+    for i in range(len(labels)):
+        vo[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, 0.1)
+        vr[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, 0.1)
+    bo = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+    br = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+    orc.raycast_objects(vo, poses, labels, T, s.k, W, H, near=near, far=far, eps_size=EPS_SIZE,
+                        vertex=bo[0], normal=bo[1], label_img=bo[2])
+    ref.raycast_objects(vr, poses, labels, T, s.k, W, H, near=near, far=far, vertex=br[0],
+                        normal=br[1], label_img=br[2])
+    oob = orc.raycast_oob_mask(vo, poses, T, s.k, W, H, near=near, far=far, eps_size=EPS_SIZE)
+    bad = np.any(bo[0] != br[0], axis=-1) | np.any(bo[1] != br[1], axis=-1) | (bo[2] != br[2])
+    assert not np.any(bad & ~oob), np.argwhere(bad & ~oob)[:10]
+    assert (bo[2] >= 0).sum() > 500
