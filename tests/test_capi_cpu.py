@@ -81,3 +81,22 @@ def test_tune_candidate_tables(lib):
     assert lib.mf_tune_get(None, 0, C.byref(n)) == -1
     assert lib.mf_tune_set(None, 0, 0) == -1
     assert lib.mf_autotune(None, 3, None, None) == -1
+
+
+def test_config_struct_layout_matches_header(tmp_path):
+    """The ctypes mf_config (capi.MfConfig) has the header's field offsets and
+    size, as a C compiler lays the struct out."""
+    import subprocess
+    fields = [f[0] for f in capi.MfConfig._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "midfusion_b200.h"\n'
+                   "int main(void) {\n"
+                   + "".join(f'  printf("%zu\\n", offsetof(mf_config, {f}));\n' for f in fields)
+                   + '  printf("%zu\\n", sizeof(mf_config));\n  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", str(exe),
+                    str(src)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    want = [getattr(capi.MfConfig, f).offset for f in fields] + [C.sizeof(capi.MfConfig)]
+    assert got == want
