@@ -100,3 +100,19 @@ def test_config_struct_layout_matches_header(tmp_path):
                                           text=True).stdout.split()]
     want = [getattr(capi.MfConfig, f).offset for f in fields] + [C.sizeof(capi.MfConfig)]
     assert got == want
+
+
+def test_ray_record_sizes_match_header(tmp_path):
+    """The byte sizes the sharded exchange allocates per pixel and instance
+    (mid_fusion_b200.shard) equal the header's mf_ray_record / mf_ray_origin."""
+    import subprocess
+    from mid_fusion_b200 import shard
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stdio.h>\n#include "midfusion_b200.h"\n'
+                   'int main(void) { printf("%zu %zu\\n", sizeof(mf_ray_record), '
+                   'sizeof(mf_ray_origin)); return 0; }\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), "-o", str(exe),
+                    str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert [int(x) for x in out] == [shard.RECORD_BYTES, shard.ORIGIN_BYTES]
