@@ -206,15 +206,19 @@ static void depth2vertex(std::vector<V3<T>>& v, const std::vector<T>& d, int W, 
       v[x + y * W] = dd > 0 ? dd * rotate(invK, v3<T>((T)x, (T)y, T(1))) : v3<T>(0, 0, 0);
     }
 }
-// preprocessing.h:39-81 (NegY = false, SDF field): only .x is set on invalid
-// pixels; the others keep the previous frame's values in the reference buffer.
+// preprocessing.h:39-81 (SDF field): only .x is set on invalid pixels; the
+// others keep the previous frame's values in the reference buffer.  NegY (a
+// negative fy, the ICL-NUIM convention, tracking.cpp:805-810) swaps the rows
+// taken as up and down.
 template <typename T>
-static void vertex2normal(std::vector<V3<T>>& out, const std::vector<V3<T>>& in, int W, int H) {
+static void vertex2normal(std::vector<V3<T>>& out, const std::vector<V3<T>>& in, int W, int H,
+                          bool negy) {
   if (out.size() != (size_t)W * H) out.assign((size_t)W * H, v3<T>(0, 0, 0));
   for (int y = 0; y < H; ++y)
     for (int x = 0; x < W; ++x) {
       const V3<T> left = in[std::max(x - 1, 0) + W * y], right = in[std::min(x + 1, W - 1) + W * y];
-      const V3<T> down = in[x + W * std::max(y - 1, 0)], up = in[x + W * std::min(y + 1, H - 1)];
+      const int ylo = std::max(y - 1, 0), yhi = std::min(y + 1, H - 1);
+      const V3<T> down = in[x + W * (negy ? yhi : ylo)], up = in[x + W * (negy ? ylo : yhi)];
       if (left.z == 0 || right.z == 0 || up.z == 0 || down.z == 0) {
         out[x + y * W].x = INVALID;
         continue;
@@ -282,7 +286,7 @@ template <typename T> void Tracker<T>::set_frame(const uint8_t* rgb, const float
     const T d = T(1 << l);
     const M4<T> invK = inverse_camera_matrix<T>(T(p.k[0]) / d, T(p.k[1]) / d, T(p.k[2]) / d, T(p.k[3]) / d);
     depth2vertex(l_vertex[l], l_D[l], lw[l], lh[l], invK);
-    vertex2normal(l_normal[l], l_vertex[l], lw[l], lh[l]);
+    vertex2normal(l_normal[l], l_vertex[l], lw[l], lh[l], p.k[1] < 0);
     gradients(gx[l], gy[l], l_I[l], lw[l], lh[l]);
     // calc_icp_cov, tracking.cpp:845-871 (sigma_xy = sigma_disp = 1, baseline 0.075)
     const T focal = T(p.k[0]) / d, baseline = T(0.075f);

@@ -145,6 +145,7 @@ int ot_get_level(void* hh, int level, int which, float* out) {
       default: {
         const auto& v = which == 2 ? t.l_vertex[level] : which == 3 ? t.l_normal[level]
                         : which == 6 ? t.cov[level] : t.r_vertex_render[level];
+        if (v.size() < n) return -1;  // not computed yet (the rendered reference: a track)
         for (size_t i = 0; i < n; ++i) {
           out[3 * i] = (float)v[i].x; out[3 * i + 1] = (float)v[i].y; out[3 * i + 2] = (float)v[i].z;
         }

@@ -798,7 +798,8 @@ class Tracker:
     def level(self, l, which):
         n = (self.W >> l) * (self.H >> l)
         out = np.zeros(n * 3, np.float32)
-        self.lib.ot_get_level(self.h, l, which, out)
+        if self.lib.ot_get_level(self.h, l, which, out) < 0:
+            raise ValueError(f"pyramid plane {which} of level {l} is not computed yet")
         if which in (2, 3, 6, 7):
             return out.reshape(self.H >> l, self.W >> l, 3)
         return out[:n].reshape(self.H >> l, self.W >> l)

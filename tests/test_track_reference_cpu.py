@@ -433,3 +433,38 @@ def test_motion_residuals_other_thresholds_and_rows_match_reference(threshold, u
     assert np.array_equal(res_r.astype(np.int8), res_f)
     ok = res_r == 1
     assert ok.sum() > 1000 and np.array_equal(err_r[ok], err_f[ok])
+
+
+def test_camera_tracking_negative_fy_matches_reference():
+    """A negative fy (the ICL-NUIM convention): the reference takes the rows
+    above and below in the other order for the normals (vertex2normalKernel
+    with NegY, tracking.cpp:805-810).  Frames rendered with fy > 0 and flipped
+    upside down are the same scene seen through (fx, -fy, cx, H - 1 - cy);
+    the FP32 oracle's pyramid, sums and pose equal the reference's."""
+    W, H = 320, 240
+    s = make_scene("room", W, H, n_frames=2, seed=5, bg_size=256, bg_dim=2.56)
+    _, _, T0, _, vm, nm, _ = _model(s, W, H)
+    k = np.asarray(s.k, np.float32)
+    kneg = np.array([k[0], -k[1], k[2], H - 1 - k[3]], np.float32)
+
+    def flip(a):
+        return np.ascontiguousarray(a[::-1])
+
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    R = O.RefTracker(W, H, kneg)
+    F = O.Tracker(W, H, kneg, robust=1, fp64=False)
+    for t in (R, F):
+        t.set_frame(flip(rgb0), flip(d0))
+        t.set_ref()
+        t.set_frame(flip(rgb1), flip(d1))
+    for level in range(3):
+        for which in range(7):  # depth, intensity, vertex, normal, gradients, ICP covariance
+            assert np.array_equal(R.level(level, which), F.level(level, which)), (level, which)
+    Tr = R.track_camera(T0, T0, flip(vm), flip(nm))
+    assert np.array_equal(Tr, F.track_camera(T0, T0, flip(vm), flip(nm)).astype(np.float32))
+    for level in range(3):
+        assert np.array_equal(R.level(level, 7), F.level(level, 7)), level  # rendered reference
+        sums = R.reduction(level)
+        assert np.array_equal(sums, _sums(F, level)), level
+        assert sums[28] > 100, level
