@@ -202,6 +202,7 @@ struct LevelMaps {
   int w[MAX_PYR], h[MAX_PYR];
   M4 invK[MAX_PYR];
   float focal[MAX_PYR];
+  int negy;             // fy < 0 (the ICL-NUIM convention): up and down swap
 };
 
 __global__ void depth2vertex_levels_kernel(LevelMaps m) {
@@ -211,18 +212,21 @@ __global__ void depth2vertex_levels_kernel(LevelMaps m) {
   depth2vertex_px(m.D[l], m.V[l], m.w[l], p, m.invK[l]);
 }
 
-// vertex2normalKernel<SDF, false> (preprocessing.h:39-81), gradientsKernel
-// (preprocessing.cpp:235-246, borders untouched) and calc_icp_cov
-// (tracking.cpp:845-871, sigma_xy = sigma_disp = 1, baseline 0.075).
+// vertex2normalKernel<SDF, NegY> (preprocessing.h:39-81; NegY when fy < 0,
+// tracking.cpp:805-810), gradientsKernel (preprocessing.cpp:235-246, borders
+// untouched) and calc_icp_cov (tracking.cpp:845-871, sigma_xy = sigma_disp = 1,
+// baseline 0.075).
 __device__ __forceinline__ void normal_grad_cov_px(const F3* __restrict__ V,
                                                    const float* __restrict__ I,
                                                    const float* __restrict__ D,
                                                    F3* __restrict__ N, float* __restrict__ GX,
                                                    float* __restrict__ GY, F3* __restrict__ COV,
-                                                   int w, int h, float focal, int p) {
+                                                   int w, int h, float focal, int negy,
+                                                   int p) {
   const int x = p % w, y = p / w;
   const F3 left = V[imx(x - 1, 0) + w * y], right = V[imn(x + 1, w - 1) + w * y];
-  const F3 down = V[x + w * imx(y - 1, 0)], up = V[x + w * imn(y + 1, h - 1)];
+  const int ylo = imx(y - 1, 0), yhi = imn(y + 1, h - 1);
+  const F3 down = V[x + w * (negy ? yhi : ylo)], up = V[x + w * (negy ? ylo : yhi)];
   if (left.z == 0 || right.z == 0 || up.z == 0 || down.z == 0) {
     N[p].x = INVALIDF;  // the other components keep their previous values
   } else {
@@ -249,7 +253,7 @@ __global__ void normal_grad_cov_levels_kernel(LevelMaps m) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= m.w[l] * m.h[l]) return;
   normal_grad_cov_px(m.V[l], m.I[l], m.D[l], m.N[l], m.GX[l], m.GY[l], m.COV[l], m.w[l],
-                     m.h[l], m.focal[l], p);
+                     m.h[l], m.focal[l], m.negy, p);
   if (m.MASK[l]) m.MASK[l][p] = 0;
 }
 
@@ -1397,6 +1401,7 @@ int track_preprocess(Context* ctx, bool clear_mask) {
     m.invK[l] = inverse_camera_matrix(kl);
     m.focal[l] = kl.x;
   }
+  m.negy = ctx->cfg.k[1] < 0.f;
   const dim3 grid(div_up((long long)P.w[0] * P.h[0], 256), T.levels);
   depth2vertex_levels_kernel<<<grid, 256, 0, ctx->stream>>>(m);
   normal_grad_cov_levels_kernel<<<grid, 256, 0, ctx->stream>>>(m);
