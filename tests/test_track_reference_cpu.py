@@ -468,3 +468,32 @@ def test_camera_tracking_negative_fy_matches_reference():
         sums = R.reduction(level)
         assert np.array_equal(sums, _sums(F, level)), level
         assert sums[28] > 100, level
+
+
+def test_camera_tracking_with_nan_and_negative_depths_matches_reference():
+    """Depth frames with NaN and negative values (sensor erasures other than
+    the zero dropouts the scenes have): the FP32 oracle's pyramid, sums and
+    pose equal the reference's, NaNs in the same places."""
+    W, H = 320, 240
+    s = make_scene("room", W, H, n_frames=2, seed=5, bg_size=256, bg_dim=2.56)
+    _, _, T0, _, vm, nm, _ = _model(s, W, H)
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    rng = np.random.default_rng(1)
+    d1 = d1.copy()
+    d1[rng.random(d1.shape) < 0.005] = np.nan
+    d1[rng.random(d1.shape) < 0.002] = -1.0
+    R = O.RefTracker(W, H, s.k)
+    F = O.Tracker(W, H, s.k, robust=1, fp64=False)
+    for t in (R, F):
+        t.set_frame(rgb0, d0)
+        t.set_ref()
+        t.set_frame(rgb1, d1)
+    for level in range(3):
+        for which in range(7):
+            assert np.array_equal(R.level(level, which), F.level(level, which), equal_nan=True), \
+                (level, which)
+    assert np.array_equal(R.track_camera(T0, T0, vm, nm),
+                          F.track_camera(T0, T0, vm, nm).astype(np.float32))
+    for level in range(3):
+        assert np.array_equal(R.reduction(level), _sums(F, level)), level
