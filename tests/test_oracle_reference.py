@@ -161,3 +161,33 @@ def test_raycast_other_near_far_match_reference(near, far):
     bad = np.any(bo[0] != br[0], axis=-1) | np.any(bo[1] != br[1], axis=-1) | (bo[2] != br[2])
     assert not np.any(bad & ~oob), np.argwhere(bad & ~oob)[:10]
     assert (bo[2] >= 0).sum() > 500
+
+
+def test_integration_with_nan_negative_and_infinite_depths_matches_reference():
+    """Allocation and integration from depth frames with NaN, negative and
+    infinite values: every block, voxel and node value equal the reference's."""
+    W, H = 128, 96
+    s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=128, obj_size=64, n_objects=2)
+    orc = O.oracle()
+    labels = [i.label for i in s.instances]
+    vo = [orc.volume(i.size, i.dim) for i in s.instances]
+    vr = [ref.volume(i.size, i.dim) for i in s.instances]
+    rng = np.random.default_rng(2)
+    for f in range(2):
+        d, rgb, lab = s.render(f)
+        d = d.copy()
+        d[rng.random(d.shape) < 0.01] = np.nan
+        d[rng.random(d.shape) < 0.005] = -0.5
+        d[rng.random(d.shape) < 0.002] = np.inf
+        masks = generalize_masks(lab, labels)
+        poses = s.volume_poses(f)
+        T = s.cam_poses[f].astype(np.float32)
+        rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+        for i in range(len(labels)):
+            assert (vo[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, 0.1) ==
+                    vr[i].integrate(d, rgb3, masks[i], T, poses[i], s.k, 0.1))
+            ko, _, ao, xo = vo[i].blocks()
+            kr, _, ar, xr = vr[i].blocks()
+            assert np.array_equal(ko, kr) and np.array_equal(ao, ar) and len(ko) > 0
+            assert xo.tobytes() == xr.tobytes()
+            assert vo[i].nodes()[3].tobytes() == vr[i].nodes()[3].tobytes()
