@@ -497,3 +497,35 @@ def test_camera_tracking_with_nan_and_negative_depths_matches_reference():
                           F.track_camera(T0, T0, vm, nm).astype(np.float32))
     for level in range(3):
         assert np.array_equal(R.reduction(level), _sums(F, level)), level
+
+
+def test_object_tracking_negative_fy_matches_reference():
+    """trackEachObject with a negative fy on flipped frames and flipped model
+    maps: every object's pose and sums equal the reference's."""
+    W, H = 320, 240
+    s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=256, obj_size=128, n_objects=3)
+    _, labels, T0, P0, vm, nm, lm = _model(s, W, H)
+    k = np.asarray(s.k, np.float32)
+    kneg = np.array([k[0], -k[1], k[2], H - 1 - k[3]], np.float32)
+
+    def flip(a):
+        return np.ascontiguousarray(a[::-1])
+
+    d0, rgb0, _ = s.render(0)
+    d1, rgb1, _ = s.render(1)
+    R = O.RefTracker(W, H, kneg)
+    F = O.Tracker(W, H, kneg, robust=1, fp64=False)
+    for t in (R, F):
+        t.set_frame(flip(rgb0), flip(d0))
+        t.set_ref()
+        t.set_frame(flip(rgb1), flip(d1))
+    vm, nm, lm = flip(vm), flip(nm), flip(lm)
+    Tc = R.track_camera(T0, T0, vm, nm)
+    assert np.array_equal(Tc, F.track_camera(T0, T0, vm, nm).astype(np.float32))
+    for i, label in enumerate(labels[1:], 1):
+        mv, mn = _object_maps(vm, nm, lm, label)
+        To_r, _ = R.track_object(R.object(P0[i], mv, mn), Tc, T0)
+        To_f = F.track_object(P0[i], Tc, T0, vm, nm, lm, label).astype(np.float32)
+        assert np.array_equal(To_r, To_f), label
+        for level in range(3):
+            assert np.array_equal(R.reduction(level), _sums(F, level)), (label, level)
