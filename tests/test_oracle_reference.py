@@ -191,3 +191,42 @@ def test_integration_with_nan_negative_and_infinite_depths_matches_reference():
             assert np.array_equal(ko, kr) and np.array_equal(ao, ar) and len(ko) > 0
             assert xo.tobytes() == xr.tobytes()
             assert vo[i].nodes()[3].tobytes() == vr[i].nodes()[3].tobytes()
+
+
+def test_volume_path_negative_fy_matches_reference():
+    """Allocation, integration and the composite raycast with a negative fy
+    (the ICL-NUIM convention) on flipped frames: oracle == reference."""
+    W, H = 128, 96
+    s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=128, obj_size=64, n_objects=2)
+    k = np.asarray(s.k, np.float32)
+    kneg = np.array([k[0], -k[1], k[2], H - 1 - k[3]], np.float32)
+
+    def flip(a):
+        return np.ascontiguousarray(a[::-1])
+
+    orc = O.oracle()
+    labels = [i.label for i in s.instances]
+    vo = [orc.volume(i.size, i.dim) for i in s.instances]
+    vr = [ref.volume(i.size, i.dim) for i in s.instances]
+    for f in range(2):
+        d, rgb, lab = (flip(a) for a in s.render(f))
+        masks = generalize_masks(lab, labels)
+        poses = s.volume_poses(f)
+        T = s.cam_poses[f].astype(np.float32)
+        rgb3 = rgb.astype(np.float32) / np.float32(255.0)
+        for i in range(len(labels)):
+            assert (vo[i].integrate(d, rgb3, masks[i], T, poses[i], kneg, 0.1) ==
+                    vr[i].integrate(d, rgb3, masks[i], T, poses[i], kneg, 0.1))
+            ko, _, _, xo = vo[i].blocks()
+            kr, _, _, xr = vr[i].blocks()
+            assert np.array_equal(ko, kr) and xo.tobytes() == xr.tobytes()
+            assert vo[i].nodes()[3].tobytes() == vr[i].nodes()[3].tobytes()
+        bo = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+        br = [np.zeros((H, W, 3), np.float32) for _ in range(2)] + [np.zeros((H, W), np.int32)]
+        orc.raycast_objects(vo, poses, labels, T, kneg, W, H, eps_size=EPS_SIZE, vertex=bo[0],
+                            normal=bo[1], label_img=bo[2])
+        ref.raycast_objects(vr, poses, labels, T, kneg, W, H, vertex=br[0], normal=br[1],
+                            label_img=br[2])
+        oob = orc.raycast_oob_mask(vo, poses, T, kneg, W, H, eps_size=EPS_SIZE)
+        bad = np.any(bo[0] != br[0], axis=-1) | np.any(bo[1] != br[1], axis=-1) | (bo[2] != br[2])
+        assert not np.any(bad & ~oob) and (bo[2] >= 0).sum() > 5000
