@@ -207,17 +207,15 @@ int mf_create(const mf_config* cfg, mf_context** out) {
 int mf_destroy(mf_context* ctx) {
   if (!ctx) return MF_E_ARG;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  if (ctx->upload) {
-    cudaStreamSynchronize(ctx->upload);
-    for (int s = 0; s < 2; ++s) {
-      if (ctx->stg_depth[s]) cudaFree(ctx->stg_depth[s]);
-      if (ctx->stg_rgb8[s]) cudaFree(ctx->stg_rgb8[s]);
-      if (ctx->stg_labels[s]) cudaFree(ctx->stg_labels[s]);
-      if (ctx->ev_staged[s]) cudaEventDestroy(ctx->ev_staged[s]);
-      if (ctx->ev_consumed[s]) cudaEventDestroy(ctx->ev_consumed[s]);
-    }
-    cudaStreamDestroy(ctx->upload);
+  if (ctx->upload) cudaStreamSynchronize(ctx->upload);
+  for (int s = 0; s < 2; ++s) {
+    if (ctx->stg_depth[s]) cudaFree(ctx->stg_depth[s]);
+    if (ctx->stg_rgb8[s]) cudaFree(ctx->stg_rgb8[s]);
+    if (ctx->stg_labels[s]) cudaFree(ctx->stg_labels[s]);
+    if (ctx->ev_staged[s]) cudaEventDestroy(ctx->ev_staged[s]);
+    if (ctx->ev_consumed[s]) cudaEventDestroy(ctx->ev_consumed[s]);
   }
+  if (ctx->upload) cudaStreamDestroy(ctx->upload);
   pipeline_free(ctx);
   track_free(ctx);
   for (auto& in : ctx->inst) volume_free(in);
@@ -539,19 +537,21 @@ int mf_process_frame_device(mf_context* ctx, const float* d_depth, const uint8_t
   return process_frame(ctx, d_labels != nullptr);
 }
 
-// The upload stream, the two input slots and their events, on first use.
+// The upload stream, the two input slots and their events, on first use.  A
+// call that failed part way leaves what it made (mf_destroy frees it) and the
+// next call makes the rest; ev_consumed[1], made last, marks the set whole.
 static int staging_init(Context* ctx) {
-  if (ctx->upload) return MF_OK;
+  if (ctx->ev_consumed[1]) return MF_OK;
   const size_t WH = (size_t)ctx->W * ctx->H;
-  cudaStream_t st = nullptr;
-  MF_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-  ctx->upload = st;  // mf_destroy frees whatever of the rest was made
+  if (!ctx->upload) MF_CUDA(cudaStreamCreateWithFlags(&ctx->upload, cudaStreamNonBlocking));
   for (int s = 0; s < 2; ++s) {
-    MF_CUDA(cudaMalloc(&ctx->stg_depth[s], 4 * WH));
-    MF_CUDA(cudaMalloc(&ctx->stg_rgb8[s], 3 * WH));
-    MF_CUDA(cudaMalloc(&ctx->stg_labels[s], 2 * WH));
-    MF_CUDA(cudaEventCreateWithFlags(&ctx->ev_staged[s], cudaEventDisableTiming));
-    MF_CUDA(cudaEventCreateWithFlags(&ctx->ev_consumed[s], cudaEventDisableTiming));
+    if (!ctx->stg_depth[s]) MF_CUDA(cudaMalloc(&ctx->stg_depth[s], 4 * WH));
+    if (!ctx->stg_rgb8[s]) MF_CUDA(cudaMalloc(&ctx->stg_rgb8[s], 3 * WH));
+    if (!ctx->stg_labels[s]) MF_CUDA(cudaMalloc(&ctx->stg_labels[s], 2 * WH));
+    if (!ctx->ev_staged[s])
+      MF_CUDA(cudaEventCreateWithFlags(&ctx->ev_staged[s], cudaEventDisableTiming));
+    if (!ctx->ev_consumed[s])
+      MF_CUDA(cudaEventCreateWithFlags(&ctx->ev_consumed[s], cudaEventDisableTiming));
   }
   return MF_OK;
 }
