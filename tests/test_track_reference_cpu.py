@@ -529,3 +529,21 @@ def test_object_tracking_negative_fy_matches_reference():
         assert np.array_equal(To_r, To_f), label
         for level in range(3):
             assert np.array_equal(R.reduction(level), _sums(F, level)), (label, level)
+
+
+@pytest.mark.parametrize("W,H", [(322, 242), (321, 241)])
+def test_camera_tracking_ragged_frame_sizes_match_reference(W, H):
+    """Frame sizes that 4 does not divide, and odd ones: the pyramid's
+    truncated level sizes (localImgSize_ = size >> level), the half-samples
+    that drop the last row / column, the pose and the sums equal the
+    reference's."""
+    s = make_scene("room", W, H, n_frames=2, seed=5, bg_size=256, bg_dim=2.56)
+    _, _, T0, _, vm, nm, _ = _model(s, W, H)
+    R, F = _pair(s, W, H)
+    for level in range(3):
+        for which in range(7):
+            assert np.array_equal(R.level(level, which), F.level(level, which)), (level, which)
+    assert np.array_equal(R.track_camera(T0, T0, vm, nm),
+                          F.track_camera(T0, T0, vm, nm).astype(np.float32))
+    for level in range(3):
+        assert np.array_equal(R.reduction(level), _sums(F, level)), level
