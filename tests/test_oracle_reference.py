@@ -193,10 +193,11 @@ def test_integration_with_nan_negative_and_infinite_depths_matches_reference():
             assert vo[i].nodes()[3].tobytes() == vr[i].nodes()[3].tobytes()
 
 
-def test_volume_path_negative_fy_matches_reference():
+@pytest.mark.parametrize("W,H", [(128, 96), (129, 97)])
+def test_volume_path_negative_fy_matches_reference(W, H):
     """Allocation, integration and the composite raycast with a negative fy
-    (the ICL-NUIM convention) on flipped frames: oracle == reference."""
-    W, H = 128, 96
+    (the ICL-NUIM convention) on flipped frames, at an even and an odd frame
+    size: oracle == reference."""
     s = make_scene("multi", W, H, n_frames=2, seed=3, bg_size=128, obj_size=64, n_objects=2)
     k = np.asarray(s.k, np.float32)
     kneg = np.array([k[0], -k[1], k[2], H - 1 - k[3]], np.float32)
